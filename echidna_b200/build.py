@@ -1,0 +1,78 @@
+"""Builds the engine's shared library in-tree: ``echidna_b200/libechidna_b200.so``.
+
+Every CUDA translation unit is compiled for sm_100a only
+(``-gencode arch=compute_100a,code=sm_100a``) with ``-fmad=false`` so that
+``a*b+c`` rounds like the reference's CPU sweeps, then linked with the host
+lowering (plan.cpp) into one library that exports the C ABI of
+``include/echidna_b200.h``.  Compilation is incremental on file timestamps.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libechidna_b200.so")
+
+NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+           "--expt-relaxed-constexpr", "-I", CSRC, "-I", os.path.join(ROOT, "include")]
+CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-ffp-contract=off", "-I", CSRC]
+
+CU_SOURCES = ["abi.cu", "k_plain.cu", "k_dual.cu", "k_jet.cu", "stde.cu"]
+CXX_SOURCES = ["plan.cpp"]
+HEADERS = ["ech_types.h", "device_math.cuh", "interp.cuh", "launch.h", "plan.h", "k_common.cuh"]
+
+
+def _newer(src: str, obj: str, deps) -> bool:
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(p) > t for p in [src, *deps] if os.path.exists(p))
+
+
+def _compile(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("compile failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+    return r.stdout + r.stderr
+
+
+def build(verbose: bool = False, jobs: int | None = None) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    deps = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "echidna_b200.h")]
+    cmds, objs = [], []
+    for s in CU_SOURCES:
+        src = os.path.join(CSRC, s)
+        obj = os.path.join(BUILD, s + ".o")
+        objs.append(obj)
+        if _newer(src, obj, deps):
+            cmds.append([NVCC, *ARCH, *NVFLAGS, "-c", src, "-o", obj])
+    for s in CXX_SOURCES:
+        src = os.path.join(CSRC, s)
+        obj = os.path.join(BUILD, s + ".o")
+        objs.append(obj)
+        if _newer(src, obj, deps):
+            cmds.append(["g++", *CXXFLAGS, "-c", src, "-o", obj])
+    if cmds:
+        with cf.ThreadPoolExecutor(max_workers=jobs or min(8, os.cpu_count() or 4)) as ex:
+            for out in ex.map(_compile, cmds):
+                if verbose and out.strip():
+                    print(out)
+    if cmds or not os.path.exists(LIB):
+        tmp = LIB + ".tmp"
+        _compile([NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lpthread"])
+        os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose="-v" in sys.argv)
+    print(LIB)

@@ -1,0 +1,890 @@
+// C ABI of the engine: context, tape upload, per-kind programs and dispatch.
+//
+// Reference boundary: echidna's CudaContext (src/gpu/cuda_backend.rs) and the
+// GpuBackend trait (src/gpu/mod.rs:92-225); the declarations and the per-call
+// reference citations are in include/echidna_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/echidna_b200.h"
+#include "interp.cuh"
+#include "launch.h"
+#include "plan.h"
+
+using namespace ech;
+
+// ───────────────────────────── errors ───────────────────────────────────────
+static thread_local std::string g_last_error;
+
+static ech_status fail(ech_status st, const std::string& msg) {
+  g_last_error = msg;
+  return st;
+}
+static ech_status cuda_fail(cudaError_t e, const char* what) {
+  if (e == cudaErrorMemoryAllocation) return fail(ECH_ERR_OUT_OF_MEMORY, "GPU out of memory");
+  return fail(ECH_ERR_OTHER, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CU(call)                                           \
+  do {                                                     \
+    cudaError_t e_ = (call);                               \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);    \
+  } while (0)
+
+extern "C" ECH_API const char* ech_last_error(void) { return g_last_error.c_str(); }
+extern "C" ECH_API const char* ech_version(void) { return "echidna_b200 0.1.0 (sm_100a)"; }
+
+// ───────────────────────────── device buffers ───────────────────────────────
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() { if (p) cudaFree(p); }
+  cudaError_t ensure(size_t n) {
+    if (n <= bytes) return cudaSuccess;
+    if (p) { cudaFree(p); p = nullptr; bytes = 0; }
+    size_t want = std::max<size_t>(n, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) bytes = want;
+    return e;
+  }
+};
+
+struct DevPlan {
+  Plan host;
+  Ins* d_fwd = nullptr;
+  RIns* d_rev = nullptr;
+  double* d_pool = nullptr;
+  ~DevPlan() {
+    if (d_fwd) cudaFree(d_fwd);
+    if (d_rev) cudaFree(d_rev);
+    if (d_pool) cudaFree(d_pool);
+  }
+};
+
+struct ech_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sm_count = 0;
+  size_t smem_optin = 0;
+  std::mutex mu;
+  DevBuf scratch, io_in, io_in2, io_out, io_out2, io_out3, stde_tmp;
+  uint32_t* d_err = nullptr;
+  // launch overrides (0 = automatic)
+  uint32_t ov_threads = 0, ov_ppt = 0, ov_cap = 0;
+};
+
+struct ech_tape {
+  ech_ctx* ctx = nullptr;
+  bool f64 = true;
+  HostTape host;
+  std::mutex mu;
+  std::map<std::tuple<int, int, uint32_t>, std::unique_ptr<DevPlan>> plans;  // (kind, K, cap)
+};
+
+// ───────────────────────────── context ──────────────────────────────────────
+extern "C" ECH_API ech_status ech_ctx_create(int device, ech_ctx** out) {
+  if (!out) return fail(ECH_ERR_INVALID_ARG, "out is null");
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= device || device < 0)
+    return fail(ECH_ERR_NO_DEVICE, "no suitable GPU device found");
+  std::unique_ptr<ech_ctx> c(new ech_ctx());
+  c->device = device;
+  CU(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  CU(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10) return fail(ECH_ERR_NO_DEVICE, "no suitable GPU device found (sm_100a required)");
+  c->sm_count = prop.multiProcessorCount;
+  c->smem_optin = prop.sharedMemPerBlockOptin;
+  CU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CU(cudaMalloc(&c->d_err, sizeof(uint32_t)));
+  CU(cudaMemset(c->d_err, 0, sizeof(uint32_t)));
+  *out = c.release();
+  return ECH_OK;
+}
+
+extern "C" ECH_API void ech_ctx_destroy(ech_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->d_err) cudaFree(ctx->d_err);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+extern "C" ECH_API ech_status ech_ctx_set_launch(ech_ctx* ctx, uint32_t threads, uint32_t ppt, uint32_t cap) {
+  if (!ctx) return fail(ECH_ERR_INVALID_ARG, "ctx is null");
+  if (threads && (threads % 32 || threads > 256)) return fail(ECH_ERR_INVALID_ARG, "threads must be a multiple of 32, <= 256");
+  if (ppt && ppt != 1 && ppt != 2) return fail(ECH_ERR_INVALID_ARG, "points_per_thread must be 1 or 2");
+  ctx->ov_threads = threads;
+  ctx->ov_ppt = ppt;
+  ctx->ov_cap = cap;
+  return ECH_OK;
+}
+
+// ───────────────────────────── validation ───────────────────────────────────
+extern "C" ECH_API ech_status ech_validate_bytecode_tape(const uint32_t* op, const uint32_t* a0, const uint32_t* a1,
+                                                         uint32_t nv, uint32_t ni, uint32_t output_index,
+                                                         const uint32_t* outs, uint32_t nouts, int has_custom) {
+  if ((nv && (!op || !a0 || !a1)) || (nouts && !outs)) return fail(ECH_ERR_INVALID_ARG, "null tape array");
+  std::string m = validate_bytecode_tape(op, a0, a1, nv, ni, output_index, outs, nouts, has_custom != 0);
+  if (!m.empty()) return fail(ECH_ERR_OTHER, "invalid bytecode tape: " + m);
+  return ECH_OK;
+}
+
+extern "C" ECH_API ech_status ech_validate_gpu_tape_data(const uint32_t* op, uint32_t n_op, const uint32_t* a0,
+                                                         uint32_t n_a0, const uint32_t* a1, uint32_t n_a1,
+                                                         uint32_t n_const, uint32_t num_ops, uint32_t num_inputs,
+                                                         uint32_t num_variables, uint32_t output_index,
+                                                         const uint32_t* outs, uint32_t nouts) {
+  if ((n_op && !op) || (n_a0 && !a0) || (n_a1 && !a1) || (nouts && !outs))
+    return fail(ECH_ERR_INVALID_ARG, "null tape array");
+  std::string m = validate_gpu_tape_data(op, a0, a1, n_op, n_a0, n_a1, n_const, num_ops, num_inputs, num_variables,
+                                         output_index, outs, nouts);
+  if (!m.empty()) return fail(ECH_ERR_OTHER, "GPU error: invalid GpuTapeData: " + m);
+  return ECH_OK;
+}
+
+// ───────────────────────────── upload ───────────────────────────────────────
+static ech_status make_tape(ech_ctx* ctx, bool f64, HostTape&& h, ech_tape** out) {
+  std::unique_ptr<ech_tape> t(new ech_tape());
+  t->ctx = ctx;
+  t->f64 = f64;
+  t->host = std::move(h);
+  *out = t.release();
+  return ECH_OK;
+}
+
+extern "C" ECH_API ech_status ech_upload_tape_f32(ech_ctx* ctx, const uint32_t* op, uint32_t n_op, const uint32_t* a0,
+                                                  uint32_t n_a0, const uint32_t* a1, uint32_t n_a1,
+                                                  const float* consts, uint32_t n_const, uint32_t num_ops,
+                                                  uint32_t num_inputs, uint32_t num_variables, uint32_t output_index,
+                                                  const uint32_t* outs, uint32_t nouts, ech_tape** out) {
+  if (!ctx || !out) return fail(ECH_ERR_INVALID_ARG, "ctx/out is null");
+  *out = nullptr;
+  if ((n_const && !consts)) return fail(ECH_ERR_INVALID_ARG, "null constants");
+  ech_status st = ech_validate_gpu_tape_data(op, n_op, a0, n_a0, a1, n_a1, n_const, num_ops, num_inputs, num_variables,
+                                             output_index, outs, nouts);
+  if (st != ECH_OK) return fail(ECH_ERR_OTHER, "refusing to upload invalid GpuTapeData: " + g_last_error);
+  HostTape h;
+  h.nv = num_variables;
+  h.ni = num_inputs;
+  h.out_index = output_index;
+  h.op.assign(op, op + n_op);
+  h.a0.assign(a0, a0 + n_a0);
+  h.a1.assign(a1, a1 + n_a1);
+  h.vals.resize(n_const);
+  for (uint32_t i = 0; i < n_const; ++i) h.vals[i] = (double)consts[i];
+  // empty output_indices -> [output_index] (src/gpu/cuda_backend.rs:632-648)
+  if (nouts == 0) h.outs.assign(1, output_index);
+  else h.outs.assign(outs, outs + nouts);
+  return make_tape(ctx, false, std::move(h), out);
+}
+
+extern "C" ECH_API ech_status ech_upload_tape_f64(ech_ctx* ctx, const uint32_t* op, const uint32_t* a0,
+                                                  const uint32_t* a1, const double* values, uint32_t nv, uint32_t ni,
+                                                  uint32_t output_index, const uint32_t* outs, uint32_t nouts,
+                                                  int has_custom, ech_tape** out) {
+  if (!ctx || !out) return fail(ECH_ERR_INVALID_ARG, "ctx/out is null");
+  *out = nullptr;
+  if (has_custom) return fail(ECH_ERR_CUSTOM_OPS_NOT_SUPPORTED, "tape contains custom ops which cannot run on GPU");
+  if (nv && !values) return fail(ECH_ERR_INVALID_ARG, "null values");
+  ech_status st = ech_validate_bytecode_tape(op, a0, a1, nv, ni, output_index, outs, nouts, 0);
+  if (st != ECH_OK) return fail(ECH_ERR_OTHER, "GPU error: refusing to upload invalid tape: " + g_last_error);
+  for (uint32_t i = 0; i < nv; ++i)
+    if (op[i] == OP_CUSTOM) return fail(ECH_ERR_CUSTOM_OPS_NOT_SUPPORTED, "tape contains custom ops which cannot run on GPU");
+  HostTape h;
+  h.nv = nv;
+  h.ni = ni;
+  h.out_index = output_index;
+  h.op.assign(op, op + nv);
+  h.a0.assign(a0, a0 + nv);
+  h.a1.assign(a1, a1 + nv);
+  h.vals.assign(values, values + nv);
+  if (nouts == 0) h.outs.assign(1, output_index);
+  else h.outs.assign(outs, outs + nouts);
+  return make_tape(ctx, true, std::move(h), out);
+}
+
+extern "C" ECH_API void ech_tape_destroy(ech_tape* t) { delete t; }
+extern "C" ECH_API uint32_t ech_tape_num_outputs(const ech_tape* t) { return t ? (uint32_t)t->host.outs.size() : 0; }
+extern "C" ECH_API uint32_t ech_tape_num_inputs(const ech_tape* t) { return t ? t->host.ni : 0; }
+extern "C" ECH_API uint32_t ech_tape_num_variables(const ech_tape* t) { return t ? t->host.nv : 0; }
+
+// ───────────────────────────── plans and launch configuration ───────────────
+static const int kRingBytes = kStages * kChunk * 32;
+
+struct LaunchCfg {
+  LaunchReq req;
+  int threads = 128;
+  uint32_t tile = 128;
+  uint32_t cap = 0;
+  size_t smem = 0;
+  size_t vbytes = 0;
+};
+
+static Kind kind_of(int k) {
+  switch (k) {
+    case 0: return Kind::Forward;
+    case 1: return Kind::Gradient;
+    case 2: return Kind::Hvp;
+    case 3: return Kind::Jvp;
+    default: return Kind::Taylor;
+  }
+}
+
+// Shared-register budget: the ring plus `cap` registers of `tile` values must
+// fit, aiming at two CTAs per SM when the live set allows it.
+static LaunchCfg choose_cfg(ech_ctx* ctx, const ech_tape* t, int kind, int K) {
+  LaunchCfg c;
+  c.req.f64 = t->f64;
+  c.req.K = K;
+  c.req.vk = (kind == 2 || kind == 3) ? VKind::Dual : (kind == 4 ? VKind::Jet : VKind::Plain);
+  c.req.rev = (kind == 1 || kind == 2);
+  c.req.P = ctx->ov_ppt ? (int)ctx->ov_ppt : 1;
+  c.threads = ctx->ov_threads ? (int)ctx->ov_threads : 128;
+  c.tile = (uint32_t)(c.threads * c.req.P);
+  c.vbytes = value_bytes(c.req);
+  const size_t budget_total = std::min<size_t>(ctx->smem_optin, 227 * 1024) - 1024;
+  const size_t per_cta = ctx->ov_cap ? budget_total : budget_total / 2;
+  size_t cap = (per_cta - kRingBytes) / (c.tile * c.vbytes);
+  if (ctx->ov_cap) cap = std::min<size_t>(cap, ctx->ov_cap);
+  c.cap = (uint32_t)std::max<size_t>(cap, 1);
+  return c;
+}
+
+static ech_status get_plan(ech_tape* t, int kind, int K, uint32_t cap, DevPlan** out) {
+  std::lock_guard<std::mutex> lk(t->mu);
+  auto key = std::make_tuple(kind, K, cap);
+  auto it = t->plans.find(key);
+  if (it != t->plans.end()) {
+    *out = it->second.get();
+    return ECH_OK;
+  }
+  std::unique_ptr<DevPlan> dp(new DevPlan());
+  dp->host = build_plan(t->host, kind_of(kind), cap);
+  const Plan& p = dp->host;
+  CU(cudaMalloc(&dp->d_fwd, std::max<size_t>(p.fwd.size(), 1) * sizeof(Ins)));
+  if (!p.fwd.empty()) CU(cudaMemcpy(dp->d_fwd, p.fwd.data(), p.fwd.size() * sizeof(Ins), cudaMemcpyHostToDevice));
+  CU(cudaMalloc(&dp->d_rev, std::max<size_t>(p.rev.size(), 1) * sizeof(RIns)));
+  if (!p.rev.empty()) CU(cudaMemcpy(dp->d_rev, p.rev.data(), p.rev.size() * sizeof(RIns), cudaMemcpyHostToDevice));
+  CU(cudaMalloc(&dp->d_pool, p.pool.size() * sizeof(double)));
+  CU(cudaMemcpy(dp->d_pool, p.pool.data(), p.pool.size() * sizeof(double), cudaMemcpyHostToDevice));
+  *out = dp.get();
+  t->plans[key] = std::move(dp);
+  return ECH_OK;
+}
+
+// Enqueues one sweep.  All pointers are device pointers.
+struct SweepIO {
+  const void* x = nullptr;
+  const void* v = nullptr;
+  int x_bcast = 0;
+  void* out = nullptr;
+  void* out2 = nullptr;
+  void* out3 = nullptr;
+  uint32_t S = 0;
+  int dir_mode = 0;
+  uint64_t seed = 0;
+};
+
+static ech_status enqueue(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n_units, const SweepIO& io,
+                          cudaStream_t st) {
+  LaunchCfg c = choose_cfg(ctx, t, kind, K);
+  DevPlan* dp = nullptr;
+  ech_status s = get_plan(t, kind, K, c.cap, &dp);
+  if (s != ECH_OK) return s;
+  const Plan& p = dp->host;
+  const uint32_t regs = std::max<uint32_t>(p.smem_regs, 1);
+  c.smem = kRingBytes + (size_t)regs * c.tile * c.vbytes;
+  KParams kp{};
+  kp.fwd = dp->d_fwd;
+  kp.n_fwd = (uint32_t)p.fwd.size();
+  kp.rev = dp->d_rev;
+  kp.n_rev = c.req.rev ? (uint32_t)p.rev.size() : 0u;
+  kp.pool = dp->d_pool;
+  kp.far_slots = p.far_slots;
+  kp.smem_regs = regs;
+  kp.tile = c.tile;
+  kp.n_units = n_units;
+  kp.ni = t->host.ni;
+  kp.no = (uint32_t)t->host.outs.size();
+  kp.x = io.x;
+  kp.v = io.v;
+  kp.x_bcast = io.x_bcast;
+  kp.out = io.out;
+  kp.out2 = io.out2;
+  kp.out3 = io.out3;
+  kp.err = ctx->d_err;
+  kp.S = io.S;
+  kp.dir_mode = io.dir_mode;
+  kp.seed = io.seed;
+  int bps = 0;
+  cudaError_t e = launch_sweep(c.req, kp, 0, c.threads, c.smem, st, &bps);
+  if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+  if (bps <= 0) return fail(ECH_ERR_OTHER, "tape live set does not fit the shared-memory slot file");
+  const uint64_t ntiles = (n_units + c.tile - 1) / c.tile;
+  const uint64_t grid = std::min<uint64_t>(ntiles, (uint64_t)bps * ctx->sm_count);
+  const uint64_t slots = (uint64_t)p.far_slots + p.traj_slots;
+  uint64_t stride = slots * c.tile * c.vbytes;
+  stride = (stride + 255) & ~(uint64_t)255;
+  CU(ctx->scratch.ensure(std::max<uint64_t>(stride * grid, 256)));
+  kp.scratch = ctx->scratch.p;
+  kp.scratch_stride_bytes = stride;
+  if (grid == 0) return ECH_OK;
+  e = launch_sweep(c.req, kp, (int)grid, c.threads, c.smem, st, &bps);
+  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  return ECH_OK;
+}
+
+static ech_status check_err_word(ech_ctx* ctx) {
+  uint32_t h = 0;
+  CU(cudaMemcpy(&h, ctx->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (h) {
+    CU(cudaMemset(ctx->d_err, 0, sizeof(uint32_t)));
+    if (h & KERR_TIMEOUT) return fail(ECH_ERR_TIMEOUT, "device-side wait timed out");
+    return fail(ECH_ERR_OTHER, "device reported a malformed instruction");
+  }
+  return ECH_OK;
+}
+
+// validate_batch_args (src/gpu/mod.rs:572-582)
+static ech_status batch_args(const ech_tape* t, uint64_t batch) {
+  if (batch == 0) return fail(ECH_ERR_OTHER, "batch_size must be non-zero");
+  if (t->host.ni == 0)
+    return fail(ECH_ERR_OTHER, "tape has no inputs (constant function); evaluate it on the CPU instead");
+  return ECH_OK;
+}
+
+static ech_status common_checks(ech_ctx* ctx, const ech_tape* t, bool f64) {
+  if (!ctx || !t) return fail(ECH_ERR_INVALID_ARG, "ctx/tape is null");
+  if (t->ctx != ctx) return fail(ECH_ERR_INVALID_ARG, "tape was uploaded on a different context");
+  if (t->f64 != f64)
+    return fail(ECH_ERR_INVALID_ARG, f64 ? "tape was uploaded with f32 constants" : "tape was uploaded with f64 constants");
+  return ECH_OK;
+}
+
+#define CHECK(x)                      \
+  do {                                \
+    ech_status s_ = (x);              \
+    if (s_ != ECH_OK) return s_;      \
+  } while (0)
+
+static ech_status len_check(size_t got, uint64_t want, const char* what) {
+  if (got != want) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "%s length mismatch: got %zu, expected %llu", what, got, (unsigned long long)want);
+    return fail(ECH_ERR_INVALID_ARG, buf);
+  }
+  return ECH_OK;
+}
+
+// ───────────────────────────── host-buffer entry points ─────────────────────
+template <class T>
+static ech_status do_forward(ech_ctx* ctx, const ech_tape* tc, const T* in, size_t n_in, uint32_t B, T* out,
+                             size_t n_out) {
+  const bool f64 = sizeof(T) == 8;
+  CHECK(common_checks(ctx, tc, f64));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(batch_args(t, B));
+  const uint64_t ni = t->host.ni, no = t->host.outs.size();
+  CHECK(len_check(n_in, (uint64_t)B * ni, "inputs"));
+  CHECK(len_check(n_out, (uint64_t)B * no, "outputs"));
+  if (!in || !out) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  CU(ctx->io_in.ensure(n_in * sizeof(T)));
+  CU(ctx->io_out.ensure(n_out * sizeof(T)));
+  CU(cudaMemcpyAsync(ctx->io_in.p, in, n_in * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  SweepIO io;
+  io.x = ctx->io_in.p;
+  io.out = ctx->io_out.p;
+  CHECK(enqueue(ctx, t, 0, 0, B, io, ctx->stream));
+  CU(cudaMemcpyAsync(out, ctx->io_out.p, n_out * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return check_err_word(ctx);
+}
+
+template <class T>
+static ech_status do_gradient(ech_ctx* ctx, const ech_tape* tc, const T* in, size_t n_in, uint32_t B, T* out,
+                              size_t n_out, T* grads, size_t n_grads) {
+  const bool f64 = sizeof(T) == 8;
+  CHECK(common_checks(ctx, tc, f64));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(batch_args(t, B));
+  const uint64_t ni = t->host.ni, no = t->host.outs.size();
+  CHECK(len_check(n_in, (uint64_t)B * ni, "inputs"));
+  CHECK(len_check(n_out, (uint64_t)B * no, "outputs"));
+  CHECK(len_check(n_grads, (uint64_t)B * ni, "grads"));
+  if (!in || !out || !grads) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  CU(ctx->io_in.ensure(n_in * sizeof(T)));
+  CU(ctx->io_out.ensure(n_out * sizeof(T)));
+  CU(ctx->io_out2.ensure(n_grads * sizeof(T)));
+  CU(cudaMemcpyAsync(ctx->io_in.p, in, n_in * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  SweepIO io;
+  io.x = ctx->io_in.p;
+  io.out = ctx->io_out.p;
+  io.out2 = ctx->io_out2.p;
+  CHECK(enqueue(ctx, t, 1, 0, B, io, ctx->stream));
+  CU(cudaMemcpyAsync(out, ctx->io_out.p, n_out * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaMemcpyAsync(grads, ctx->io_out2.p, n_grads * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return check_err_word(ctx);
+}
+
+template <class T>
+static ech_status do_hvp(ech_ctx* ctx, const ech_tape* tc, const T* x, size_t n_x, bool per_point, const T* dirs,
+                         size_t n_dirs, uint32_t B, T* grads, size_t n_grads, T* hvps, size_t n_hvps) {
+  const bool f64 = sizeof(T) == 8;
+  CHECK(common_checks(ctx, tc, f64));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(batch_args(t, B));
+  const uint64_t ni = t->host.ni;
+  CHECK(len_check(n_x, per_point ? (uint64_t)B * ni : ni, "x"));
+  CHECK(len_check(n_dirs, (uint64_t)B * ni, "tangent_dirs"));
+  CHECK(len_check(n_grads, (uint64_t)B * ni, "grads"));
+  CHECK(len_check(n_hvps, (uint64_t)B * ni, "hvps"));
+  if (!x || !dirs || !grads || !hvps) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  CU(ctx->io_in.ensure(n_x * sizeof(T)));
+  CU(ctx->io_in2.ensure(n_dirs * sizeof(T)));
+  CU(ctx->io_out2.ensure(n_grads * sizeof(T)));
+  CU(ctx->io_out3.ensure(n_hvps * sizeof(T)));
+  CU(cudaMemcpyAsync(ctx->io_in.p, x, n_x * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(ctx->io_in2.p, dirs, n_dirs * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  SweepIO io;
+  io.x = ctx->io_in.p;
+  io.v = ctx->io_in2.p;
+  io.x_bcast = per_point ? 0 : 1;
+  io.out2 = ctx->io_out2.p;
+  io.out3 = ctx->io_out3.p;
+  CHECK(enqueue(ctx, t, 2, 0, B, io, ctx->stream));
+  CU(cudaMemcpyAsync(grads, ctx->io_out2.p, n_grads * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaMemcpyAsync(hvps, ctx->io_out3.p, n_hvps * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return check_err_word(ctx);
+}
+
+template <class T>
+static ech_status do_tangent(ech_ctx* ctx, const ech_tape* tc, const T* x, size_t n_x, const T* seeds, size_t n_seeds,
+                             uint32_t B, T* vals, T* tans, size_t n_out) {
+  const bool f64 = sizeof(T) == 8;
+  CHECK(common_checks(ctx, tc, f64));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(batch_args(t, B));
+  const uint64_t ni = t->host.ni, no = t->host.outs.size();
+  CHECK(len_check(n_x, (uint64_t)B * ni, "primal_inputs"));
+  CHECK(len_check(n_seeds, (uint64_t)B * ni, "tangent_seeds"));
+  CHECK(len_check(n_out, (uint64_t)B * no, "outputs"));
+  if (!x || !seeds || !tans) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  CU(ctx->io_in.ensure(n_x * sizeof(T)));
+  CU(ctx->io_in2.ensure(n_seeds * sizeof(T)));
+  CU(ctx->io_out.ensure(n_out * sizeof(T)));
+  CU(ctx->io_out2.ensure(n_out * sizeof(T)));
+  CU(cudaMemcpyAsync(ctx->io_in.p, x, n_x * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(ctx->io_in2.p, seeds, n_seeds * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  SweepIO io;
+  io.x = ctx->io_in.p;
+  io.v = ctx->io_in2.p;
+  io.out = ctx->io_out.p;
+  io.out2 = ctx->io_out2.p;
+  CHECK(enqueue(ctx, t, 3, 0, B, io, ctx->stream));
+  if (vals) CU(cudaMemcpyAsync(vals, ctx->io_out.p, n_out * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaMemcpyAsync(tans, ctx->io_out2.p, n_out * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return check_err_word(ctx);
+}
+
+template <class T>
+static ech_status do_taylor(ech_ctx* ctx, const ech_tape* tc, const T* P, size_t n_p, const T* S, size_t n_s,
+                            uint32_t B, uint32_t order, T* coeffs, size_t n_c) {
+  const bool f64 = sizeof(T) == 8;
+  CHECK(common_checks(ctx, tc, f64));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  if (order < 1 || order > 5) {
+    char buf[96];
+    snprintf(buf, sizeof buf, "unsupported Taylor order %u, must be 1..=5", order);
+    return fail(ECH_ERR_OTHER, buf);
+  }
+  CHECK(batch_args(t, B));
+  const uint64_t ni = t->host.ni, no = t->host.outs.size();
+  CHECK(len_check(n_p, (uint64_t)B * ni, "primal_inputs"));
+  CHECK(len_check(n_s, (uint64_t)B * ni, "direction_seeds"));
+  CHECK(len_check(n_c, (uint64_t)order * B * no, "coefficients"));
+  if (!P || !S || !coeffs) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  CU(ctx->io_in.ensure(n_p * sizeof(T)));
+  CU(ctx->io_in2.ensure(n_s * sizeof(T)));
+  CU(ctx->io_out.ensure(n_c * sizeof(T)));
+  CU(cudaMemcpyAsync(ctx->io_in.p, P, n_p * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(ctx->io_in2.p, S, n_s * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  SweepIO io;
+  io.x = ctx->io_in.p;
+  io.v = ctx->io_in2.p;
+  io.out = ctx->io_out.p;
+  CHECK(enqueue(ctx, t, 4, (int)order, B, io, ctx->stream));
+  CU(cudaMemcpyAsync(coeffs, ctx->io_out.p, n_c * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return check_err_word(ctx);
+}
+
+extern "C" {
+
+ECH_API ech_status ech_forward_batch_f32(ech_ctx* c, const ech_tape* t, const float* in, size_t n_in, uint32_t B,
+                                         float* out, size_t n_out) {
+  return do_forward<float>(c, t, in, n_in, B, out, n_out);
+}
+ECH_API ech_status ech_forward_batch_f64(ech_ctx* c, const ech_tape* t, const double* in, size_t n_in, uint32_t B,
+                                         double* out, size_t n_out) {
+  return do_forward<double>(c, t, in, n_in, B, out, n_out);
+}
+ECH_API ech_status ech_gradient_batch_f32(ech_ctx* c, const ech_tape* t, const float* in, size_t n_in, uint32_t B,
+                                          float* out, size_t n_out, float* g, size_t n_g) {
+  return do_gradient<float>(c, t, in, n_in, B, out, n_out, g, n_g);
+}
+ECH_API ech_status ech_gradient_batch_f64(ech_ctx* c, const ech_tape* t, const double* in, size_t n_in, uint32_t B,
+                                          double* out, size_t n_out, double* g, size_t n_g) {
+  return do_gradient<double>(c, t, in, n_in, B, out, n_out, g, n_g);
+}
+ECH_API ech_status ech_hvp_batch_f32(ech_ctx* c, const ech_tape* t, const float* x, size_t n_x, const float* d,
+                                     size_t n_d, uint32_t B, float* g, size_t n_g, float* h, size_t n_h) {
+  return do_hvp<float>(c, t, x, n_x, false, d, n_d, B, g, n_g, h, n_h);
+}
+ECH_API ech_status ech_hvp_batch_f64(ech_ctx* c, const ech_tape* t, const double* x, size_t n_x, const double* d,
+                                     size_t n_d, uint32_t B, double* g, size_t n_g, double* h, size_t n_h) {
+  return do_hvp<double>(c, t, x, n_x, false, d, n_d, B, g, n_g, h, n_h);
+}
+ECH_API ech_status ech_hvp_batch_points_f32(ech_ctx* c, const ech_tape* t, const float* x, size_t n_x, const float* d,
+                                            size_t n_d, uint32_t B, float* g, size_t n_g, float* h, size_t n_h) {
+  return do_hvp<float>(c, t, x, n_x, true, d, n_d, B, g, n_g, h, n_h);
+}
+ECH_API ech_status ech_hvp_batch_points_f64(ech_ctx* c, const ech_tape* t, const double* x, size_t n_x,
+                                            const double* d, size_t n_d, uint32_t B, double* g, size_t n_g, double* h,
+                                            size_t n_h) {
+  return do_hvp<double>(c, t, x, n_x, true, d, n_d, B, g, n_g, h, n_h);
+}
+ECH_API ech_status ech_tangent_forward_batch_f32(ech_ctx* c, const ech_tape* t, const float* x, size_t n_x,
+                                                 const float* s, size_t n_s, uint32_t B, float* v, float* tn,
+                                                 size_t n_o) {
+  return do_tangent<float>(c, t, x, n_x, s, n_s, B, v, tn, n_o);
+}
+ECH_API ech_status ech_tangent_forward_batch_f64(ech_ctx* c, const ech_tape* t, const double* x, size_t n_x,
+                                                 const double* s, size_t n_s, uint32_t B, double* v, double* tn,
+                                                 size_t n_o) {
+  return do_tangent<double>(c, t, x, n_x, s, n_s, B, v, tn, n_o);
+}
+ECH_API ech_status ech_taylor_forward_kth_batch_f32(ech_ctx* c, const ech_tape* t, const float* p, size_t n_p,
+                                                    const float* s, size_t n_s, uint32_t B, uint32_t order,
+                                                    float* co, size_t n_co) {
+  return do_taylor<float>(c, t, p, n_p, s, n_s, B, order, co, n_co);
+}
+ECH_API ech_status ech_taylor_forward_kth_batch_f64(ech_ctx* c, const ech_tape* t, const double* p, size_t n_p,
+                                                    const double* s, size_t n_s, uint32_t B, uint32_t order,
+                                                    double* co, size_t n_co) {
+  return do_taylor<double>(c, t, p, n_p, s, n_s, B, order, co, n_co);
+}
+
+// ── device-pointer variants ──
+ECH_API ech_status ech_forward_batch_device(ech_ctx* ctx, const ech_tape* t, int f64, const void* in, uint32_t B,
+                                            void* out, void* stream) {
+  CHECK(common_checks(ctx, t, f64 != 0));
+  CHECK(batch_args(t, B));
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  SweepIO io;
+  io.x = in;
+  io.out = out;
+  return enqueue(ctx, const_cast<ech_tape*>(t), 0, 0, B, io, stream ? (cudaStream_t)stream : ctx->stream);
+}
+ECH_API ech_status ech_gradient_batch_device(ech_ctx* ctx, const ech_tape* t, int f64, const void* in, uint32_t B,
+                                             void* out, void* grads, void* stream) {
+  CHECK(common_checks(ctx, t, f64 != 0));
+  CHECK(batch_args(t, B));
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  SweepIO io;
+  io.x = in;
+  io.out = out;
+  io.out2 = grads;
+  return enqueue(ctx, const_cast<ech_tape*>(t), 1, 0, B, io, stream ? (cudaStream_t)stream : ctx->stream);
+}
+ECH_API ech_status ech_hvp_batch_device(ech_ctx* ctx, const ech_tape* t, int f64, const void* xs, int x_per_point,
+                                        const void* dirs, uint32_t B, void* grads, void* hvps, void* stream) {
+  CHECK(common_checks(ctx, t, f64 != 0));
+  CHECK(batch_args(t, B));
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  SweepIO io;
+  io.x = xs;
+  io.v = dirs;
+  io.x_bcast = x_per_point ? 0 : 1;
+  io.out2 = grads;
+  io.out3 = hvps;
+  return enqueue(ctx, const_cast<ech_tape*>(t), 2, 0, B, io, stream ? (cudaStream_t)stream : ctx->stream);
+}
+ECH_API ech_status ech_taylor_batch_device(ech_ctx* ctx, const ech_tape* t, int f64, const void* p, const void* s,
+                                           uint32_t B, uint32_t order, void* coeffs, void* stream) {
+  CHECK(common_checks(ctx, t, f64 != 0));
+  if (order < 1 || order > 5) return fail(ECH_ERR_OTHER, "unsupported Taylor order, must be 1..=5");
+  CHECK(batch_args(t, B));
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  SweepIO io;
+  io.x = p;
+  io.v = s;
+  io.out = coeffs;
+  return enqueue(ctx, const_cast<ech_tape*>(t), 4, (int)order, B, io, stream ? (cudaStream_t)stream : ctx->stream);
+}
+}  // extern "C"
+
+// ── STDE (src/gpu/stde_gpu.rs) ──
+// require_scalar_output / require_nonempty_x (src/gpu/stde_gpu.rs:16-40)
+static ech_status stde_checks(const ech_tape* t, size_t n, const char* caller, const char* quantity) {
+  if (t->host.outs.size() != 1) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "%s requires a scalar-output tape; got %zu outputs", caller, t->host.outs.size());
+    return fail(ECH_ERR_OTHER, buf);
+  }
+  if (n == 0) {
+    return fail(ECH_ERR_OTHER, std::string(caller) + " requires a non-empty x (a zero-input tape has no " + quantity +
+                                   "); zero-sized GPU buffers would panic");
+  }
+  if (n != t->host.ni) return fail(ECH_ERR_INVALID_ARG, "x length must match the tape's num_inputs");
+  return ECH_OK;
+}
+
+// Taylor K=3 over npoints*S units, then the per-point Welford reduction.
+// dir_mode: 0 dirs per unit, 1 shared [S][n], 2 device Rademacher, 3 basis e_s.
+template <class T>
+static ech_status stde_run(ech_ctx* ctx, ech_tape* t, const T* d_x, bool x_bcast, uint64_t npoints, uint32_t S,
+                           const T* d_dirs, int dir_mode, uint64_t seed, bool acc64, const T* d_cv, double trace,
+                           int control, ech_estimator_result* d_res, T* d_c0_out, T* d_c2_out) {
+  const uint64_t units = npoints * S;
+  CU(ctx->stde_tmp.ensure(units * 3 * sizeof(T)));
+  SweepIO io;
+  io.x = d_x;
+  io.x_bcast = x_bcast ? 1 : 0;
+  io.v = d_dirs;
+  io.out = ctx->stde_tmp.p;
+  io.S = S;
+  io.dir_mode = dir_mode;
+  io.seed = seed;
+  CHECK(enqueue(ctx, t, 4, 3, units, io, ctx->stream));
+  const T* c0 = (const T*)ctx->stde_tmp.p;
+  const T* c2 = c0 + 2 * units;
+  if (d_res) {
+    CU(launch_stde_reduce_t(sizeof(T) == 8, acc64, c0, c2, npoints, S, d_cv, trace, control, d_res, ctx->stream));
+  }
+  if (d_c0_out) CU(cudaMemcpyAsync(d_c0_out, c0, units * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
+  if (d_c2_out) CU(cudaMemcpyAsync(d_c2_out, c2, units * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
+  return ECH_OK;
+}
+
+ECH_API ech_status ech_laplacian_gpu_f32(ech_ctx* ctx, const ech_tape* tc, const float* x, size_t n,
+                                         const float* dirs, uint32_t S, ech_estimator_result* out) {
+  CHECK(common_checks(ctx, tc, false));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(stde_checks(t, n, "laplacian_gpu", "Laplacian"));
+  if (S == 0) return fail(ECH_ERR_OTHER, "no directions provided");
+  if (!x || !dirs || !out) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  CU(ctx->io_in.ensure(n * sizeof(float)));
+  CU(ctx->io_in2.ensure((size_t)S * n * sizeof(float)));
+  CU(ctx->io_out3.ensure(sizeof(ech_estimator_result)));
+  CU(cudaMemcpyAsync(ctx->io_in.p, x, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(ctx->io_in2.p, dirs, (size_t)S * n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  CHECK(stde_run<float>(ctx, t, (const float*)ctx->io_in.p, true, 1, S, (const float*)ctx->io_in2.p, 0, 0, false,
+                        nullptr, 0.0, 0, (ech_estimator_result*)ctx->io_out3.p, nullptr, nullptr));
+  CU(cudaMemcpyAsync(out, ctx->io_out3.p, sizeof(ech_estimator_result), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return check_err_word(ctx);
+}
+
+ECH_API ech_status ech_hessian_diagonal_gpu_f32(ech_ctx* ctx, const ech_tape* tc, const float* x, size_t n,
+                                                float* value, float* diag) {
+  CHECK(common_checks(ctx, tc, false));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(stde_checks(t, n, "hessian_diagonal_gpu", "Hessian diagonal"));
+  if (!x || !value || !diag) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  CU(ctx->io_in.ensure(n * sizeof(float)));
+  CU(ctx->io_out.ensure(n * sizeof(float)));
+  CU(ctx->io_out2.ensure(n * sizeof(float)));
+  CU(cudaMemcpyAsync(ctx->io_in.p, x, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  CHECK(stde_run<float>(ctx, t, (const float*)ctx->io_in.p, true, 1, (uint32_t)n, nullptr, 3, 0, false, nullptr, 0.0,
+                        0, nullptr, (float*)ctx->io_out.p, (float*)ctx->io_out2.p));
+  std::vector<float> c0(n), c2(n);
+  CU(cudaMemcpyAsync(c0.data(), ctx->io_out.p, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaMemcpyAsync(c2.data(), ctx->io_out2.p, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  CHECK(check_err_word(ctx));
+  *value = c0[0];
+  for (size_t j = 0; j < n; ++j) diag[j] = 2.0f * c2[j];
+  return ECH_OK;
+}
+
+ECH_API ech_status ech_laplacian_with_control_gpu_f32(ech_ctx* ctx, const ech_tape* tc, const float* x, size_t n,
+                                                      const float* dirs, uint32_t S, const float* control,
+                                                      ech_estimator_result* out) {
+  CHECK(common_checks(ctx, tc, false));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(stde_checks(t, n, "laplacian_with_control_gpu", "Laplacian"));
+  if (S == 0) return fail(ECH_ERR_OTHER, "no directions provided");
+  if (!x || !dirs || !control || !out) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  float trace = 0.0f;
+  for (size_t j = 0; j < n; ++j) trace = trace + control[j];
+  CU(ctx->io_in.ensure(n * sizeof(float)));
+  CU(ctx->io_in2.ensure((size_t)S * n * sizeof(float)));
+  CU(ctx->io_out.ensure(n * sizeof(float) + S * sizeof(float)));
+  CU(ctx->io_out3.ensure(sizeof(ech_estimator_result)));
+  float* d_diag = (float*)ctx->io_out.p;
+  float* d_cv = d_diag + n;
+  CU(cudaMemcpyAsync(ctx->io_in.p, x, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(ctx->io_in2.p, dirs, (size_t)S * n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(d_diag, control, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  CU(launch_control_term(false, ctx->io_in2.p, d_diag, S, (uint32_t)n, d_cv, ctx->stream));
+  CHECK(stde_run<float>(ctx, t, (const float*)ctx->io_in.p, true, 1, S, (const float*)ctx->io_in2.p, 0, 0, false,
+                        d_cv, (double)trace, 1, (ech_estimator_result*)ctx->io_out3.p, nullptr, nullptr));
+  CU(cudaMemcpyAsync(out, ctx->io_out3.p, sizeof(ech_estimator_result), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return check_err_word(ctx);
+}
+
+template <class T>
+static ech_status do_laplacian_batch(ech_ctx* ctx, const ech_tape* tc, const T* xs, size_t n_xs, uint32_t B,
+                                     const T* dirs, size_t n_dirs, uint32_t S, int dir_mode, uint64_t seed,
+                                     ech_estimator_result* res) {
+  CHECK(common_checks(ctx, tc, sizeof(T) == 8));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(stde_checks(t, t->host.ni, "laplacian_batch", "Laplacian"));
+  CHECK(batch_args(t, B));
+  if (S == 0) return fail(ECH_ERR_OTHER, "no directions provided");
+  const uint64_t n = t->host.ni;
+  CHECK(len_check(n_xs, (uint64_t)B * n, "xs"));
+  if (dir_mode == 0) CHECK(len_check(n_dirs, (uint64_t)B * S * n, "directions"));
+  else if (dir_mode == 1) CHECK(len_check(n_dirs, (uint64_t)S * n, "directions"));
+  else if (dir_mode != 2) return fail(ECH_ERR_INVALID_ARG, "dir_mode must be 0, 1 or 2");
+  if (!xs || !res || (dir_mode != 2 && !dirs)) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  CU(ctx->io_in.ensure(n_xs * sizeof(T)));
+  CU(ctx->io_out3.ensure((size_t)B * sizeof(ech_estimator_result)));
+  CU(cudaMemcpyAsync(ctx->io_in.p, xs, n_xs * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  const T* d_dirs = nullptr;
+  if (dir_mode != 2) {
+    CU(ctx->io_in2.ensure(n_dirs * sizeof(T)));
+    CU(cudaMemcpyAsync(ctx->io_in2.p, dirs, n_dirs * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    d_dirs = (const T*)ctx->io_in2.p;
+  }
+  CHECK(stde_run<T>(ctx, t, (const T*)ctx->io_in.p, false, B, S, d_dirs, dir_mode, seed, true, nullptr, 0.0, 0,
+                    (ech_estimator_result*)ctx->io_out3.p, nullptr, nullptr));
+  CU(cudaMemcpyAsync(res, ctx->io_out3.p, (size_t)B * sizeof(ech_estimator_result), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return check_err_word(ctx);
+}
+
+ECH_API ech_status ech_laplacian_batch_f32(ech_ctx* ctx, const ech_tape* t, const float* xs, size_t n_xs, uint32_t B,
+                                           const float* dirs, size_t n_dirs, uint32_t S, int dir_mode, uint64_t seed,
+                                           ech_estimator_result* res) {
+  return do_laplacian_batch<float>(ctx, t, xs, n_xs, B, dirs, n_dirs, S, dir_mode, seed, res);
+}
+ECH_API ech_status ech_laplacian_batch_f64(ech_ctx* ctx, const ech_tape* t, const double* xs, size_t n_xs,
+                                           uint32_t B, const double* dirs, size_t n_dirs, uint32_t S, int dir_mode,
+                                           uint64_t seed, ech_estimator_result* res) {
+  return do_laplacian_batch<double>(ctx, t, xs, n_xs, B, dirs, n_dirs, S, dir_mode, seed, res);
+}
+
+extern "C" {
+
+ECH_API ech_status ech_ctx_synchronize(ech_ctx* ctx) {
+  if (!ctx) return fail(ECH_ERR_INVALID_ARG, "ctx is null");
+  CU(cudaSetDevice(ctx->device));
+  CU(cudaStreamSynchronize(ctx->stream));
+  CU(cudaDeviceSynchronize());
+  return check_err_word(ctx);
+}
+
+
+// Host-only: lowers a tape without a device and copies the programs out, so the
+// lowering can be checked on machines without a GPU.  counts[0..5] receive the
+// instruction, reverse-instruction and pool counts, shared registers, far slots
+// and trajectory slots; arrays are filled up to their capacities.
+ECH_API ech_status ech_plan_dump(const uint32_t* op, const uint32_t* a0, const uint32_t* a1, const double* values,
+                                 uint32_t nv, uint32_t ni, uint32_t output_index, const uint32_t* outs,
+                                 uint32_t nouts, int kind, uint32_t cap, void* fwd, size_t fwd_cap, void* rev,
+                                 size_t rev_cap, double* pool, size_t pool_cap, uint64_t* counts) {
+  if (!op || !a0 || !a1 || !values || !counts) return fail(ECH_ERR_INVALID_ARG, "null argument");
+  std::string m = validate_bytecode_tape(op, a0, a1, nv, ni, output_index, outs, nouts, false);
+  if (!m.empty()) return fail(ECH_ERR_OTHER, "invalid bytecode tape: " + m);
+  if (kind < 0 || kind > 4) return fail(ECH_ERR_INVALID_ARG, "kind must be 0..4");
+  HostTape h;
+  h.nv = nv;
+  h.ni = ni;
+  h.out_index = output_index;
+  h.op.assign(op, op + nv);
+  h.a0.assign(a0, a0 + nv);
+  h.a1.assign(a1, a1 + nv);
+  h.vals.assign(values, values + nv);
+  if (nouts == 0) h.outs.assign(1, output_index);
+  else h.outs.assign(outs, outs + nouts);
+  Plan p = build_plan(h, kind_of(kind), cap);
+  counts[0] = p.fwd.size();
+  counts[1] = p.rev.size();
+  counts[2] = p.pool.size();
+  counts[3] = p.smem_regs;
+  counts[4] = p.far_slots;
+  counts[5] = p.traj_slots;
+  if (fwd) memcpy(fwd, p.fwd.data(), std::min(fwd_cap, p.fwd.size()) * sizeof(Ins));
+  if (rev) memcpy(rev, p.rev.data(), std::min(rev_cap, p.rev.size()) * sizeof(RIns));
+  if (pool) memcpy(pool, p.pool.data(), std::min(pool_cap, p.pool.size()) * sizeof(double));
+  return ECH_OK;
+}
+
+ECH_API ech_status ech_tape_plan_stats(ech_ctx* ctx, const ech_tape* tc, int kind, uint32_t order, int f64,
+                                       uint64_t* stats) {
+  if (!ctx || !tc || !stats) return fail(ECH_ERR_INVALID_ARG, "null argument");
+  if (kind < 0 || kind > 4) return fail(ECH_ERR_INVALID_ARG, "kind must be 0..4");
+  (void)f64;
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  LaunchCfg c = choose_cfg(ctx, t, kind, (int)order);
+  Plan p = build_plan(t->host, kind_of(kind), c.cap);
+  const PlanStats& s = p.stats;
+  uint64_t v[12] = {s.fwd_ops, s.rev_ops, s.max_live_fwd, s.max_live_rev, s.traj_values, s.flops_fwd, s.flops_rev,
+                    s.specials_fwd, s.specials_rev, p.smem_regs, p.far_slots, p.fwd.size() + p.rev.size()};
+  memcpy(stats, v, sizeof v);
+  return ECH_OK;
+}
+
+}  // extern "C"
+
+namespace ech {
+size_t value_bytes(const LaunchReq& r) {
+  const size_t s = r.f64 ? 8 : 4;
+  switch (r.vk) {
+    case VKind::Plain: return s;
+    case VKind::Dual: return 2 * s;
+    case VKind::Jet: return (size_t)r.K * s;
+  }
+  return s;
+}
+}  // namespace ech

@@ -1,0 +1,37 @@
+// Shared launcher body for the sweep-kernel instantiation units.
+#pragma once
+#include "interp.cuh"
+#include "launch.h"
+
+namespace ech {
+
+template <class V, int P, bool REV>
+cudaError_t launch_one(const KParams& kp, int grid, int block, size_t smem, cudaStream_t st, int* blocks_per_sm) {
+  auto fn = sweep_kernel<V, P, REV>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (grid == 0) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, block, smem);
+  }
+  fn<<<grid, block, smem, st>>>(kp);
+  return cudaGetLastError();
+}
+
+template <class V>
+cudaError_t launch_by_p(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
+                        int* bps) {
+  if (r.rev) {
+    switch (r.P) {
+      case 1: return launch_one<V, 1, true>(kp, grid, block, smem, st, bps);
+      case 2: return launch_one<V, 2, true>(kp, grid, block, smem, st, bps);
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  switch (r.P) {
+    case 1: return launch_one<V, 1, false>(kp, grid, block, smem, st, bps);
+    case 2: return launch_one<V, 2, false>(kp, grid, block, smem, st, bps);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace ech

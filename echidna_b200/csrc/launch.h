@@ -1,0 +1,48 @@
+// Kernel registry: maps a value kind / precision / points-per-thread to the
+// template instantiation of the sweep kernel and launches it.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include "ech_types.h"
+
+namespace ech {
+struct KParams;
+
+enum class VKind { Plain, Dual, Jet };
+
+struct LaunchReq {
+  VKind vk = VKind::Plain;
+  bool f64 = true;
+  int K = 0;      // jet order (Jet kind)
+  int P = 1;      // points per thread
+  bool rev = false;
+};
+
+size_t value_bytes(const LaunchReq& r);
+// Each returns cudaErrorInvalidValue for an unsupported combination.
+cudaError_t launch_plain(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
+                         int* blocks_per_sm);
+cudaError_t launch_dual(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
+                        int* blocks_per_sm);
+cudaError_t launch_jet(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
+                       int* blocks_per_sm);
+
+// Launch (grid > 0) or query occupancy (grid == 0, result in *blocks_per_sm).
+inline cudaError_t launch_sweep(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem,
+                                cudaStream_t st, int* blocks_per_sm) {
+  switch (r.vk) {
+    case VKind::Plain: return launch_plain(r, kp, grid, block, smem, st, blocks_per_sm);
+    case VKind::Dual: return launch_dual(r, kp, grid, block, smem, st, blocks_per_sm);
+    case VKind::Jet: return launch_jet(r, kp, grid, block, smem, st, blocks_per_sm);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// STDE per-point reduction of 2*c2 samples (Welford in direction order);
+// acc64 selects a double accumulator for f32 samples.
+cudaError_t launch_stde_reduce_t(bool f64, bool acc64, const void* c0, const void* c2, uint64_t npoints, uint32_t S,
+                                 const void* cv, double trace, int control, void* results, cudaStream_t st);
+cudaError_t launch_control_term(bool f64, const void* dirs, const void* diag, uint32_t S, uint32_t n, void* cv,
+                                cudaStream_t st);
+
+}  // namespace ech

@@ -1,0 +1,599 @@
+// Host-side lowering: tape -> forward / reverse interpreter programs.
+//
+// 1. Liveness.  Ops that reach no requested output are dropped (their values are
+//    unobservable, and in the reverse sweep their adjoints are exactly zero, so
+//    skipping them matches reverse_sweep_core's zero-adjoint skip bit for bit).
+// 2. The reverse program visits the surviving ops in decreasing tape order, so
+//    every adjoint receives its contributions in the same order as the CPU
+//    sweep (src/bytecode_tape/reverse.rs:32-105).
+// 3. Virtual registers (slot values forward, adjoints reverse) get live
+//    intervals over instruction positions and are assigned by linear scan
+//    (Poletto & Sarkar 1999): up to `smem_cap` shared-memory registers, the
+//    intervals ending furthest away spill to L2-resident global slots.
+// 4. Values that a reverse partial reads are written once to a trajectory slot
+//    by the forward program.
+#include "plan.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <set>
+#include <sstream>
+#include <stdexcept>
+
+namespace ech {
+
+bool is_binary(uint32_t op) { return op >= OP_ADD && op <= OP_MIN; }
+
+static const char* kOpNames[] = {
+    "Input", "Const", "Add", "Sub", "Mul", "Div", "Rem", "Powf", "Atan2", "Hypot", "Max", "Min",
+    "Neg", "Recip", "Sqrt", "Cbrt", "Powi", "Exp", "Exp2", "ExpM1", "Ln", "Log2", "Log10", "Ln1p",
+    "Sin", "Cos", "Tan", "Asin", "Acos", "Atan", "Sinh", "Cosh", "Tanh", "Asinh", "Acosh", "Atanh",
+    "Abs", "Signum", "Floor", "Ceil", "Round", "Trunc", "Fract", "Custom"};
+
+static std::string arg_pair(uint32_t a, uint32_t b) {
+  std::ostringstream o;
+  o << "[" << a << ", " << b << "]";
+  return o.str();
+}
+
+// src/bytecode_tape/mod.rs:575-705
+std::string validate_bytecode_tape(const uint32_t* op, const uint32_t* a0, const uint32_t* a1, uint32_t nv,
+                                   uint32_t ni, uint32_t output_index, const uint32_t* outs, uint32_t nouts,
+                                   bool has_custom_ops) {
+  std::ostringstream e;
+  if (ni > nv) {
+    e << "num_inputs (" << ni << ") > tape length (" << nv << ")";
+    return e.str();
+  }
+  for (uint32_t i = 0; i < nv; ++i) {
+    if (op[i] > OP_CUSTOM) {
+      e << "opcodes[" << i << "] (" << op[i] << ") is not a valid opcode";
+      return e.str();
+    }
+    if ((op[i] == OP_INPUT) != (i < ni)) {
+      if (i < ni) e << "opcodes[" << i << "] should be Input but is " << kOpNames[op[i]];
+      else e << "opcodes[" << i << "] is Input, but only the first " << ni << " entries may be inputs";
+      return e.str();
+    }
+    if (i < ni && (a0[i] != kUnused || a1[i] != kUnused)) {
+      e << "arg_indices[" << i << "] must be [UNUSED, UNUSED] for an Input entry, found " << arg_pair(a0[i], a1[i]);
+      return e.str();
+    }
+  }
+  if (output_index >= nv) {
+    e << "output_index (" << output_index << ") >= tape length (" << nv << ")";
+    return e.str();
+  }
+  for (uint32_t j = 0; j < nouts; ++j) {
+    if (outs[j] >= nv) {
+      e << "output_indices[" << j << "] (" << outs[j] << ") >= tape length (" << nv << ")";
+      return e.str();
+    }
+  }
+  for (uint32_t i = ni; i < nv; ++i) {
+    const uint32_t o = op[i];
+    if (o == OP_CONST) {
+      if (a0[i] != kUnused || a1[i] != kUnused) {
+        e << "arg_indices[" << i << "] must be [UNUSED, UNUSED] for a Const entry, found " << arg_pair(a0[i], a1[i]);
+        return e.str();
+      }
+      continue;
+    }
+    if (a0[i] >= i) {
+      e << "arg_indices[" << i << "][0] (" << a0[i] << ") must reference an earlier slot";
+      return e.str();
+    }
+    if (o == OP_POWI) continue;
+    if (o == OP_CUSTOM) {
+      if (!has_custom_ops) {
+        e << "arg_indices[" << i << "][1] (" << a1[i] << ") is not a registered custom-op callback";
+        return e.str();
+      }
+      continue;
+    }
+    if (is_binary(o)) {
+      if (a1[i] >= i) {
+        e << "arg_indices[" << i << "][1] (" << a1[i] << ") must reference an earlier slot";
+        return e.str();
+      }
+    } else if (a1[i] != kUnused) {
+      e << "arg_indices[" << i << "][1] (" << a1[i] << ") should be UNUSED for unary op " << kOpNames[o];
+      return e.str();
+    }
+  }
+  return std::string();
+}
+
+// src/gpu/mod.rs:397-564
+std::string validate_gpu_tape_data(const uint32_t* op, const uint32_t* a0, const uint32_t* a1, uint32_t n_op,
+                                   uint32_t n_a0, uint32_t n_a1, uint32_t n_const, uint32_t num_ops,
+                                   uint32_t num_inputs, uint32_t num_variables, uint32_t output_index,
+                                   const uint32_t* outs, uint32_t nouts) {
+  std::ostringstream e;
+  const uint32_t n = num_ops;
+  if (n_op != n) { e << "opcodes.len() (" << n_op << ") != num_ops (" << n << ")"; return e.str(); }
+  if (n_a0 != n) { e << "arg0.len() (" << n_a0 << ") != num_ops (" << n << ")"; return e.str(); }
+  if (n_a1 != n) { e << "arg1.len() (" << n_a1 << ") != num_ops (" << n << ")"; return e.str(); }
+  if (num_ops != num_variables) {
+    e << "num_ops (" << num_ops << ") != num_variables (" << num_variables << ")";
+    return e.str();
+  }
+  if (n_const != num_variables) {
+    e << "constants.len() (" << n_const << ") != num_variables (" << num_variables << ")";
+    return e.str();
+  }
+  if (num_inputs > num_variables) {
+    e << "num_inputs (" << num_inputs << ") > num_variables (" << num_variables << ")";
+    return e.str();
+  }
+  const uint32_t ni = num_inputs;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (op[i] > OP_FRACT) { e << "opcodes[" << i << "] (" << op[i] << ") is not a GPU-executable opcode"; return e.str(); }
+    if ((op[i] == OP_INPUT) != (i < ni)) {
+      if (i < ni) e << "opcodes[" << i << "] (" << op[i] << ") should be Input";
+      else e << "opcodes[" << i << "] is Input, but only the first " << ni << " entries may be inputs";
+      return e.str();
+    }
+  }
+  for (uint32_t i = ni; i < n; ++i) {
+    const uint32_t o = op[i];
+    if (o == OP_CONST) continue;
+    if (a0[i] >= i) { e << "arg0[" << i << "] (" << a0[i] << ") must reference an earlier slot"; return e.str(); }
+    if (o == OP_POWI) continue;
+    if (is_binary(o)) {
+      if (a1[i] >= i) { e << "arg1[" << i << "] (" << a1[i] << ") must reference an earlier slot"; return e.str(); }
+    } else if (a1[i] != kUnused) {
+      e << "arg1[" << i << "] (" << a1[i] << ") should be the UNUSED sentinel for unary opcode " << o;
+      return e.str();
+    }
+  }
+  if (output_index >= num_variables) {
+    e << "output_index (" << output_index << ") >= num_variables (" << num_variables << ")";
+    return e.str();
+  }
+  for (uint32_t j = 0; j < nouts; ++j) {
+    if (outs[j] >= num_variables) {
+      e << "output_indices[" << j << "] (" << outs[j] << ") >= num_variables (" << num_variables << ")";
+      return e.str();
+    }
+  }
+  return std::string();
+}
+
+namespace {
+
+// Arithmetic/special op counts per tape opcode (forward); used for the
+// roofline's algorithmic-flops figure.  Specials are libm-class calls.
+void op_cost(uint32_t o, uint64_t& flops, uint64_t& specials) {
+  switch (o) {
+    case OP_ADD: case OP_SUB: case OP_MUL: case OP_DIV: case OP_NEG: flops += 1; break;
+    case OP_MAX: case OP_MIN: case OP_ABS: case OP_FRACT: flops += 1; break;
+    case OP_RECIP: case OP_SQRT: flops += 1; break;
+    case OP_POWI: flops += 2; break;
+    case OP_SIGNUM: case OP_FLOOR: case OP_CEIL: case OP_ROUND: case OP_TRUNC: break;
+    default: specials += 1; break;  // transcendental / libm
+  }
+}
+
+struct Loc {
+  uint8_t mode = M_NONE;
+  uint32_t idx = kNone;
+};
+
+// Linear-scan register assignment over intervals [start, end] (inclusive
+// instruction positions).  A register whose interval ends at position p may be
+// reused by an interval starting at p (instructions read before they write).
+struct LinearScan {
+  struct Iv {
+    int64_t start, end;
+    uint32_t id;
+  };
+  std::vector<Iv> ivs;
+  std::vector<Loc> loc;  // by id
+  uint32_t smem_used = 0, glob_used = 0;
+  uint64_t max_live = 0;
+
+  void run(uint32_t nids, uint32_t cap) {
+    loc.assign(nids, Loc{});
+    std::sort(ivs.begin(), ivs.end(), [](const Iv& x, const Iv& y) {
+      return x.start != y.start ? x.start < y.start : x.id < y.id;
+    });
+    // Pass 1: decide shared vs global (furthest-end spill).
+    std::vector<uint8_t> in_smem(nids, 0);
+    std::set<std::pair<int64_t, uint32_t>> active;  // (end, id) of smem-resident intervals
+    {
+      std::set<std::pair<int64_t, uint32_t>> all_active;
+      for (const Iv& iv : ivs) {
+        // An interval ending at iv.start is read by the instruction that writes
+        // iv (reads precede the write), so its register is free for iv.
+        while (!active.empty() && active.begin()->first <= iv.start) active.erase(active.begin());
+        while (!all_active.empty() && all_active.begin()->first < iv.start) all_active.erase(all_active.begin());
+        all_active.insert({iv.end, iv.id});
+        max_live = std::max<uint64_t>(max_live, all_active.size());
+        if (active.size() < cap) {
+          active.insert({iv.end, iv.id});
+          in_smem[iv.id] = 1;
+        } else if (cap > 0) {
+          auto last = std::prev(active.end());
+          if (last->first > iv.end) {
+            in_smem[last->second] = 0;
+            active.erase(last);
+            active.insert({iv.end, iv.id});
+            in_smem[iv.id] = 1;
+          }
+        }
+      }
+    }
+    // Pass 2: concrete indices, separately for each class.
+    for (int cls = 0; cls < 2; ++cls) {
+      std::set<std::pair<int64_t, uint32_t>> busy;  // (end, reg)
+      std::vector<uint32_t> free_regs;
+      uint32_t next = 0;
+      for (const Iv& iv : ivs) {
+        if ((in_smem[iv.id] != 0) != (cls == 0)) continue;
+        while (!busy.empty() && busy.begin()->first <= iv.start) {
+          free_regs.push_back(busy.begin()->second);
+          busy.erase(busy.begin());
+        }
+        uint32_t r;
+        if (!free_regs.empty()) {
+          r = free_regs.back();
+          free_regs.pop_back();
+        } else {
+          r = next++;
+        }
+        busy.insert({iv.end, r});
+        loc[iv.id] = Loc{cls == 0 ? (uint8_t)M_SMEM : (uint8_t)M_GLOB, r};
+      }
+      if (cls == 0) smem_used = next;
+      else glob_used = next;
+    }
+  }
+};
+
+}  // namespace
+
+Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
+  const uint32_t nv = t.nv, ni = t.ni;
+  const bool reverse = (kind == Kind::Gradient || kind == Kind::Hvp);
+  const bool emit_outputs = (kind != Kind::Hvp);
+  const uint32_t seed = t.outs.empty() ? t.out_index : t.outs[0];
+  Plan pl;
+
+  auto is_const = [&](uint32_t s) { return t.op[s] == OP_CONST; };
+  auto has_b = [&](uint32_t i) { return is_binary(t.op[i]); };
+
+  // ---------------- liveness of the forward program ----------------
+  std::vector<uint8_t> live(nv, 0);
+  if (emit_outputs)
+    for (uint32_t o : t.outs) live[o] = 1;
+  if (reverse) live[seed] = 1;
+  for (int64_t i = (int64_t)nv - 1; i >= (int64_t)ni; --i) {
+    if (!live[i] || is_const((uint32_t)i)) continue;
+    live[t.a0[i]] = 1;
+    if (has_b((uint32_t)i)) live[t.a1[i]] = 1;
+  }
+
+  // ---------------- reverse reachability and value needs ----------------
+  std::vector<uint8_t> reach(nv, 0);
+  std::vector<uint8_t> saved(nv, 0);
+  if (reverse) {
+    reach[seed] = 1;
+    for (int64_t i = seed; i >= (int64_t)ni; --i) {
+      if (!reach[i] || is_const((uint32_t)i)) continue;
+      reach[t.a0[i]] = 1;
+      if (has_b((uint32_t)i)) reach[t.a1[i]] = 1;
+    }
+  }
+  // which values each reverse op reads: bit0=a, bit1=b, bit2=r
+  auto rev_needs = [&](uint32_t i, bool needA, bool needB) -> uint32_t {
+    const uint32_t o = t.op[i];
+    switch (o) {
+      case OP_ADD: case OP_SUB: case OP_NEG: case OP_FRACT:
+      case OP_SIGNUM: case OP_FLOOR: case OP_CEIL: case OP_ROUND: case OP_TRUNC:
+        return 0;
+      case OP_MUL: return (needA ? 2u : 0u) | (needB ? 1u : 0u);
+      case OP_DIV: return (needA ? 2u : 0u) | (needB ? 6u : 0u);
+      case OP_REM: return needB ? 3u : 0u;
+      case OP_POWF: return 7u;
+      case OP_ATAN2: case OP_MAX: case OP_MIN: return 3u;
+      case OP_HYPOT: return (needA ? 5u : 0u) | (needB ? 6u : 0u);
+      case OP_POWI: return (t.a1[i] == 0x80000000u) ? 5u : 1u;
+      case OP_SQRT: case OP_CBRT: case OP_EXP: case OP_EXP2: case OP_EXPM1: return 4u;
+      default: return 1u;  // unary partial reads its argument
+    }
+  };
+  std::vector<uint32_t> needs(nv, 0);
+  if (reverse) {
+    for (uint32_t i = ni; i < nv; ++i) {
+      if (!reach[i] || is_const(i)) continue;
+      const bool needA = !is_const(t.a0[i]);
+      const bool needB = has_b(i) && !is_const(t.a1[i]);
+      if (!needA && !needB) continue;
+      needs[i] = rev_needs(i, needA, needB);
+      if ((needs[i] & 1u) && !is_const(t.a0[i])) saved[t.a0[i]] = 1;
+      if ((needs[i] & 2u) && !is_const(t.a1[i])) saved[t.a1[i]] = 1;
+      if (needs[i] & 4u) saved[i] = 1;
+    }
+  }
+  std::vector<uint32_t> traj(nv, kNone);
+  uint32_t ntraj = 0;
+  for (uint32_t s = 0; s < nv; ++s)
+    if (saved[s]) traj[s] = ntraj++;
+  pl.traj_slots = ntraj;
+  pl.stats.traj_values = ntraj;
+
+  // ---------------- forward program (symbolic) ----------------
+  struct FSym {
+    uint8_t opc;
+    int32_t aux;
+    int64_t d;       // vreg (slot) or -1
+    int64_t a, b;    // vreg or -1
+    bool a_imm, b_imm;
+    double a_val, b_val;
+    uint32_t save;
+  };
+  std::vector<FSym> fs;
+  fs.reserve(nv + t.outs.size());
+  std::vector<int64_t> def_pos(nv, -1), last_pos(nv, -1);
+  auto use = [&](uint32_t s, int64_t pos) { last_pos[s] = std::max(last_pos[s], pos); };
+  std::vector<std::vector<uint32_t>> outs_of;  // output ids per slot (sparse)
+  std::vector<std::pair<uint32_t, uint32_t>> out_pairs;  // (slot, j)
+  if (emit_outputs)
+    for (uint32_t j = 0; j < (uint32_t)t.outs.size(); ++j) out_pairs.push_back({t.outs[j], j});
+  std::sort(out_pairs.begin(), out_pairs.end());
+  size_t op_cursor = 0;
+  auto emit_outputs_for = [&](uint32_t s) {
+    while (op_cursor < out_pairs.size() && out_pairs[op_cursor].first < s) ++op_cursor;
+    size_t k = op_cursor;
+    while (k < out_pairs.size() && out_pairs[k].first == s) {
+      FSym f{};
+      f.opc = XI_STOUT;
+      f.aux = (int32_t)out_pairs[k].second;
+      f.d = -1;
+      f.b = -1;
+      f.save = kNone;
+      if (is_const(s)) {
+        f.a = -1; f.a_imm = true; f.a_val = t.vals[s];
+      } else {
+        f.a = s; f.a_imm = false;
+        use(s, (int64_t)fs.size());
+      }
+      fs.push_back(f);
+      ++k;
+    }
+  };
+  // constant outputs first
+  for (auto& pr : out_pairs) {
+    if (!is_const(pr.first)) continue;
+    FSym f{};
+    f.opc = XI_STOUT; f.aux = (int32_t)pr.second; f.d = -1; f.a = -1; f.b = -1;
+    f.a_imm = true; f.a_val = t.vals[pr.first]; f.save = kNone;
+    fs.push_back(f);
+  }
+  int64_t tmp_vreg = nv;  // extra vregs for materialised constants
+  std::vector<std::pair<int64_t, int64_t>> tmp_iv;  // (def, use) of temps
+  for (uint32_t i = 0; i < nv; ++i) {
+    if (!live[i] || is_const(i)) continue;
+    const uint32_t o = t.op[i];
+    FSym f{};
+    f.d = i;
+    f.save = traj[i];
+    f.b = -1;
+    if (o == OP_INPUT) {
+      f.opc = XI_LDIN; f.aux = (int32_t)i; f.a = -1;
+    } else {
+      f.opc = (uint8_t)o;
+      f.aux = (o == OP_POWI) ? (int32_t)t.a1[i] : 0;
+      const uint32_t sa = t.a0[i];
+      const bool bin = has_b(i);
+      const uint32_t sb = bin ? t.a1[i] : kUnused;
+      const bool ca = is_const(sa), cb = bin && is_const(sb);
+      if (ca && cb) {
+        // both operands constant (hand-built tapes): materialise a into a temp
+        FSym m{};
+        m.opc = XI_MOV; m.d = tmp_vreg; m.a = -1; m.b = -1; m.a_imm = true; m.a_val = t.vals[sa]; m.save = kNone;
+        const int64_t p = (int64_t)fs.size();
+        fs.push_back(m);
+        tmp_iv.push_back({p, p + 1});
+        f.a = tmp_vreg++;
+        f.a_imm = false;
+      } else if (ca) {
+        f.a = -1; f.a_imm = true; f.a_val = t.vals[sa];
+      } else {
+        f.a = sa; f.a_imm = false; use(sa, (int64_t)fs.size());
+      }
+      if (bin) {
+        if (cb) { f.b = -1; f.b_imm = true; f.b_val = t.vals[sb]; }
+        else { f.b = sb; f.b_imm = false; use(sb, (int64_t)fs.size()); }
+      }
+      op_cost(o, pl.stats.flops_fwd, pl.stats.specials_fwd);
+      pl.stats.fwd_ops++;
+    }
+    def_pos[i] = (int64_t)fs.size();
+    fs.push_back(f);
+    emit_outputs_for(i);
+  }
+  // forward intervals
+  LinearScan lsf;
+  for (uint32_t s = 0; s < nv; ++s) {
+    if (def_pos[s] < 0) continue;
+    int64_t e = std::max(last_pos[s], def_pos[s]);
+    lsf.ivs.push_back({def_pos[s], e, s});
+  }
+  for (size_t k = 0; k < tmp_iv.size(); ++k) lsf.ivs.push_back({tmp_iv[k].first, tmp_iv[k].second, (uint32_t)(nv + k)});
+  lsf.run((uint32_t)(nv + tmp_iv.size()), smem_cap);
+  pl.stats.max_live_fwd = lsf.max_live;
+  pl.fwd.reserve(fs.size());
+  for (const FSym& f : fs) {
+    Ins in{};
+    in.opc = f.opc;
+    in.aux = f.aux;
+    in.save = f.save;
+    in.imm = 0.0;
+    if (f.d >= 0) { in.md = lsf.loc[f.d].mode; in.d = lsf.loc[f.d].idx; }
+    else { in.md = M_NONE; in.d = kNone; }
+    if (f.a >= 0) { in.ma = lsf.loc[f.a].mode; in.a = lsf.loc[f.a].idx; }
+    else if (f.a_imm) { in.ma = M_IMM; in.a = 0; in.imm = f.a_val; }
+    else { in.ma = M_NONE; in.a = kNone; }
+    if (f.b >= 0) { in.mb = lsf.loc[f.b].mode; in.b = lsf.loc[f.b].idx; }
+    else if (f.b_imm) { in.mb = M_IMM; in.b = 0; in.imm = f.b_val; }
+    else { in.mb = M_NONE; in.b = kNone; }
+    pl.fwd.push_back(in);
+  }
+  uint32_t smem_used = lsf.smem_used, glob_used = lsf.glob_used;
+
+  // ---------------- reverse program ----------------
+  if (reverse) {
+    struct RSym {
+      uint8_t opc;
+      int32_t aux;
+      uint16_t flags;
+      int64_t r, a, b;   // adjoint vregs (slot ids), -1 none
+      uint32_t va, vb, vr;
+    };
+    std::vector<RSym> rs;
+    std::vector<int64_t> birth(nv, -1), death(nv, -1);
+    // minimum reachable consumer of every input (its gradient is final after it)
+    std::vector<int64_t> min_cons(ni, -1);
+    for (uint32_t i = ni; i < nv; ++i) {
+      if (!reach[i] || is_const(i)) continue;
+      const uint32_t sa = t.a0[i];
+      if (sa < ni && min_cons[sa] < 0) min_cons[sa] = i;
+      if (has_b(i)) {
+        const uint32_t sb = t.a1[i];
+        if (sb < ni && min_cons[sb] < 0) min_cons[sb] = i;
+      }
+    }
+    std::vector<std::vector<uint32_t>> grads_after;  // by op -> inputs whose gradient completes there
+    // zero gradients for inputs without reachable consumers
+    const bool seed_const = is_const(seed);
+    for (uint32_t k = 0; k < ni; ++k) {
+      const bool seeded = (!seed_const && k == seed);
+      if (min_cons[k] < 0 && !seeded) {
+        RSym g{};
+        g.opc = XI_STGRAD; g.aux = (int32_t)k; g.r = -1; g.a = -1; g.b = -1;
+        g.va = g.vb = g.vr = kNone;
+        rs.push_back(g);
+      }
+    }
+    if (!seed_const) {
+      RSym sd{};
+      sd.opc = XI_SEED; sd.r = seed; sd.a = -1; sd.b = -1; sd.va = sd.vb = sd.vr = kNone;
+      birth[seed] = (int64_t)rs.size();
+      rs.push_back(sd);
+      if (seed < ni && min_cons[seed] < 0) {
+        RSym g{};
+        g.opc = XI_STGRAD; g.aux = (int32_t)seed; g.r = seed; g.a = -1; g.b = -1;
+        g.va = g.vb = g.vr = kNone;
+        death[seed] = (int64_t)rs.size();
+        rs.push_back(g);
+      }
+    }
+    auto value_of = [&](uint32_t s, uint32_t& v, bool& imm) {
+      if (is_const(s)) {
+        v = (uint32_t)pl.pool.size();
+        pl.pool.push_back(t.vals[s]);
+        imm = true;
+      } else {
+        v = traj[s];
+        imm = false;
+      }
+    };
+    for (int64_t ii = (int64_t)nv - 1; ii >= (int64_t)ni && !seed_const; --ii) {
+      const uint32_t i = (uint32_t)ii;
+      if (!reach[i] || is_const(i)) continue;
+      const uint32_t o = t.op[i];
+      const uint32_t sa = t.a0[i];
+      const bool bin = has_b(i);
+      const uint32_t sb = bin ? t.a1[i] : kUnused;
+      const bool needA = !is_const(sa);
+      const bool needB = bin && !is_const(sb);
+      const int64_t pos = (int64_t)rs.size();
+      if (birth[i] >= 0) death[i] = pos;  // adj(i) read here
+      if (!needA && !needB) continue;
+      RSym r{};
+      r.opc = (uint8_t)o;
+      r.aux = (o == OP_POWI) ? (int32_t)t.a1[i] : 0;
+      r.r = i;
+      r.a = needA ? (int64_t)sa : -1;
+      r.b = needB ? (int64_t)sb : -1;
+      r.va = r.vb = r.vr = kNone;
+      uint16_t fl = 0;
+      if (needA) fl |= RF_HAS_A;
+      if (needB) fl |= RF_HAS_B;
+      if (needA && birth[sa] < 0) { birth[sa] = pos; fl |= RF_A_INIT; }
+      if (needB && birth[sb] < 0) { birth[sb] = pos; fl |= RF_B_INIT; }
+      const uint32_t nd = needs[i];
+      bool imm;
+      if (nd & 1u) { value_of(sa, r.va, imm); if (imm) fl |= RF_VA_IMM; }
+      if (nd & 2u) { value_of(sb, r.vb, imm); if (imm) fl |= RF_VB_IMM; }
+      if (nd & 4u) { r.vr = traj[i]; }
+      r.flags = fl;
+      rs.push_back(r);
+      op_cost(o, pl.stats.flops_rev, pl.stats.specials_rev);
+      pl.stats.flops_rev += 2 * ((needA ? 1 : 0) + (needB ? 1 : 0));
+      pl.stats.rev_ops++;
+      // gradients that complete at this op
+      for (int which = 0; which < 2; ++which) {
+        const uint32_t s = which == 0 ? sa : sb;
+        if ((which == 0 && !needA) || (which == 1 && !needB)) continue;
+        if (which == 1 && sb == sa) continue;
+        if (s < ni && min_cons[s] == (int64_t)i) {
+          RSym g{};
+          g.opc = XI_STGRAD; g.aux = (int32_t)s; g.r = s; g.a = -1; g.b = -1; g.va = g.vb = g.vr = kNone;
+          death[s] = (int64_t)rs.size();
+          rs.push_back(g);
+        }
+      }
+    }
+    // Every reachable op other than the seed has a reachable consumer, so its
+    // adjoint is born (first contribution, RF_*_INIT) before it is read.
+    LinearScan lsr;
+    for (uint32_t s = 0; s < nv; ++s) {
+      if (birth[s] < 0) continue;
+      int64_t e = std::max(death[s], birth[s]);
+      lsr.ivs.push_back({birth[s], e, s});
+    }
+    lsr.run(nv, smem_cap);
+    pl.stats.max_live_rev = lsr.max_live;
+    pl.rev.reserve(rs.size());
+    for (const RSym& r : rs) {
+      RIns in{};
+      in.opc = r.opc;
+      in.aux = r.aux;
+      uint16_t fl = r.flags;
+      if (r.r >= 0) {
+        in.r = lsr.loc[r.r].idx;
+        if (lsr.loc[r.r].mode == M_GLOB) fl |= RF_R_GLOB;
+      } else {
+        in.r = kNone;
+      }
+      if (r.a >= 0) {
+        in.a = lsr.loc[r.a].idx;
+        if (lsr.loc[r.a].mode == M_GLOB) fl |= RF_A_GLOB;
+      } else {
+        in.a = kNone;
+      }
+      if (r.b >= 0) {
+        in.b = lsr.loc[r.b].idx;
+        if (lsr.loc[r.b].mode == M_GLOB) fl |= RF_B_GLOB;
+      } else {
+        in.b = kNone;
+      }
+      in.va = r.va;
+      in.vb = r.vb;
+      in.vr = r.vr;
+      in.flags = fl;
+      pl.rev.push_back(in);
+    }
+    smem_used = std::max(smem_used, lsr.smem_used);
+    glob_used = std::max(glob_used, lsr.glob_used);
+  }
+  pl.smem_regs = smem_used;
+  pl.far_slots = glob_used;
+  if (pl.pool.empty()) pl.pool.push_back(0.0);
+  return pl;
+}
+
+}  // namespace ech

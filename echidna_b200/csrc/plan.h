@@ -1,0 +1,60 @@
+// Host-side lowering of a recorded tape into interpreter programs.
+#pragma once
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include "ech_types.h"
+
+namespace ech {
+
+// A validated tape in host memory.  `vals` holds the constants image in double
+// (f32 tapes widen exactly); `outs` is all_output_indices() after the upload
+// fallback (empty output_indices -> [output_index]).
+struct HostTape {
+  std::vector<uint32_t> op, a0, a1;
+  std::vector<double> vals;
+  uint32_t nv = 0, ni = 0, out_index = 0;
+  std::vector<uint32_t> outs;
+};
+
+enum class Kind { Forward, Gradient, Hvp, Jvp, Taylor };
+
+struct PlanStats {
+  uint64_t fwd_ops = 0;        // tape ops executed per unit in the forward program
+  uint64_t rev_ops = 0;        // tape ops executed per unit in the reverse program
+  uint64_t max_live_fwd = 0;   // peak live values (forward)
+  uint64_t max_live_rev = 0;   // peak live adjoints (reverse)
+  uint64_t traj_values = 0;    // values saved for the reverse (T_val)
+  uint64_t flops_fwd = 0;      // arithmetic ops per unit (forward)
+  uint64_t flops_rev = 0;      // arithmetic ops per unit (reverse)
+  uint64_t specials_fwd = 0;   // libm-class calls per unit (forward)
+  uint64_t specials_rev = 0;
+};
+
+struct Plan {
+  std::vector<Ins> fwd;
+  std::vector<RIns> rev;
+  std::vector<double> pool;
+  uint32_t smem_regs = 0;      // shared registers used
+  uint32_t far_slots = 0;      // global registers (max of both sweeps)
+  uint32_t traj_slots = 0;     // trajectory slots
+  PlanStats stats;
+};
+
+// Builds the programs for `kind` with at most `smem_cap` shared registers.
+Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap);
+
+// Validation with the reference's messages.  Empty string = valid.
+//   BytecodeTape::validate   (src/bytecode_tape/mod.rs:575-705)
+//   GpuTapeData::validate    (src/gpu/mod.rs:397-564)
+std::string validate_bytecode_tape(const uint32_t* op, const uint32_t* a0, const uint32_t* a1, uint32_t nv,
+                                   uint32_t ni, uint32_t output_index, const uint32_t* outs, uint32_t nouts,
+                                   bool has_custom_ops);
+std::string validate_gpu_tape_data(const uint32_t* op, const uint32_t* a0, const uint32_t* a1, uint32_t n_op,
+                                   uint32_t n_a0, uint32_t n_a1, uint32_t n_const, uint32_t num_ops,
+                                   uint32_t num_inputs, uint32_t num_variables, uint32_t output_index,
+                                   const uint32_t* outs, uint32_t nouts);
+
+bool is_binary(uint32_t op);
+
+}  // namespace ech

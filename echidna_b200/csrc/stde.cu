@@ -1,0 +1,127 @@
+// STDE reductions on the device.
+//
+// The Taylor sweep writes c2 for every (point, direction) unit; these kernels
+// turn them into per-point EstimatorResults with the reference's Welford
+// accumulator (src/stde/types.rs:44-113): non-finite samples are skipped, the
+// mean is NaN when nothing contributed, the variance m2/(n-1) is clamped at 0
+// and the standard error is sqrt(var/n).  Samples are visited in direction
+// order, as the reference's host loop does (src/gpu/stde_gpu.rs:84-97).
+//
+// Accumulator precision: `Acc` = the sample type for the drop-in calls (so an
+// f32 laplacian_gpu reproduces the reference's f32 Welford exactly), and double
+// for the batched extension (FP64 final reduction of FP32 samples).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/echidna_b200.h"
+#include "launch.h"
+
+namespace ech {
+
+template <class Acc>
+struct Welford {
+  Acc mean = Acc(0), m2 = Acc(0);
+  uint64_t count = 0;
+  __device__ void update(Acc s) {
+    if (!isfinite(s)) return;
+    count += 1;
+    const Acc k1 = (Acc)count;
+    const Acc delta = s - mean;
+    mean = mean + delta / k1;
+    const Acc delta2 = s - mean;
+    m2 = m2 + delta * delta2;
+  }
+  __device__ void finalize(Acc* est, Acc* var, Acc* se) const {
+    if (count == 0) {
+      *est = __longlong_as_double(0x7ff8000000000000ll);
+      *var = Acc(0);
+      *se = Acc(0);
+      return;
+    }
+    const Acc nf = (Acc)count;
+    if (count > 1) {
+      const Acc v = fmax(m2 / (nf - Acc(1)), Acc(0));
+      *est = mean;
+      *var = v;
+      *se = sqrt(v / nf);
+    } else {
+      *est = mean;
+      *var = Acc(0);
+      *se = Acc(0);
+    }
+  }
+};
+
+// One thread per point: samples 2*c2 of units [p*S, (p+1)*S), optionally minus
+// a control term cv[s] plus `offset` (laplacian_with_control).
+template <class T, class Acc>
+__global__ void stde_reduce_kernel(const T* c0, const T* c2, uint64_t npoints, uint32_t S, const T* cv, T trace,
+                                   int control, ech_estimator_result* out) {
+  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npoints) return;
+  Welford<Acc> acc;
+  for (uint32_t s = 0; s < S; ++s) {
+    const T vhv = T(2) * c2[p * S + s];
+    if (control) acc.update((Acc)(vhv - cv[s]));
+    else acc.update((Acc)vhv);
+  }
+  Acc est, var, se;
+  acc.finalize(&est, &var, &se);
+  ech_estimator_result r;
+  // every direction of a point shares the primal; report the first's c0
+  // (src/gpu/stde_gpu.rs:88 reads values[0])
+  r.value = (double)c0[p * S];
+  r.estimate = control ? (double)((T)trace + (T)est) : (double)est;
+  r.sample_variance = (double)var;
+  r.standard_error = (double)se;
+  r.num_samples = acc.count;
+  out[p] = r;
+}
+
+// v^T diag(H) v per direction, summed in index order in T (src/gpu/stde_gpu.rs:178-184).
+template <class T>
+__global__ void control_term_kernel(const T* dirs, const T* diag, uint32_t S, uint32_t n, T* cv) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S) return;
+  T acc = T(0);
+  for (uint32_t j = 0; j < n; ++j) {
+    const T vj = dirs[(uint64_t)s * n + j];
+    acc = acc + diag[j] * vj * vj;
+  }
+  cv[s] = acc;
+}
+
+cudaError_t launch_stde_reduce_t(bool f64, bool acc64, const void* c0, const void* c2, uint64_t npoints, uint32_t S,
+                                 const void* cv, double trace, int control, void* results, cudaStream_t st) {
+  const int threads = 128;
+  const unsigned blocks = (unsigned)((npoints + threads - 1) / threads);
+  if (blocks == 0) return cudaSuccess;
+  if (f64) {
+    stde_reduce_kernel<double, double><<<blocks, threads, 0, st>>>((const double*)c0, (const double*)c2, npoints, S,
+                                                                   (const double*)cv, trace, control,
+                                                                   (ech_estimator_result*)results);
+  } else if (acc64) {
+    stde_reduce_kernel<float, double><<<blocks, threads, 0, st>>>((const float*)c0, (const float*)c2, npoints, S,
+                                                                  (const float*)cv, (float)trace, control,
+                                                                  (ech_estimator_result*)results);
+  } else {
+    stde_reduce_kernel<float, float><<<blocks, threads, 0, st>>>((const float*)c0, (const float*)c2, npoints, S,
+                                                                 (const float*)cv, (float)trace, control,
+                                                                 (ech_estimator_result*)results);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_control_term(bool f64, const void* dirs, const void* diag, uint32_t S, uint32_t n, void* cv,
+                                cudaStream_t st) {
+  const int threads = 128;
+  const unsigned blocks = (S + threads - 1) / threads;
+  if (blocks == 0) return cudaSuccess;
+  if (f64)
+    control_term_kernel<double><<<blocks, threads, 0, st>>>((const double*)dirs, (const double*)diag, S, n, (double*)cv);
+  else
+    control_term_kernel<float><<<blocks, threads, 0, st>>>((const float*)dirs, (const float*)diag, S, n, (float*)cv);
+  return cudaGetLastError();
+}
+
+}  // namespace ech

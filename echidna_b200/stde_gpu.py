@@ -1,0 +1,87 @@
+"""GPU STDE estimators (``src/gpu/stde_gpu.rs``) over the engine's C ABI.
+
+``laplacian_gpu``, ``hessian_diagonal_gpu`` and ``laplacian_with_control_gpu`` keep
+the reference's signatures and errors.  ``laplacian_batch`` is this engine's
+extension: many points, ``S`` directions each, one Taylor launch plus an on-device
+per-point Welford reduction; directions come from the caller or from a
+counter-based device RNG.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .gpu import CudaContext, CudaTapeBuffers, CudaTapeBuffersF64, EstimatorResult, _check
+
+DIR_PER_POINT, DIR_SHARED, DIR_RADEMACHER = 0, 1, 2
+
+
+def _result(r: _lib.EstimatorResultC, dt=float) -> EstimatorResult:
+    return EstimatorResult(dt(r.value), dt(r.estimate), dt(r.sample_variance), dt(r.standard_error),
+                           int(r.num_samples))
+
+
+def laplacian_gpu(backend: CudaContext, tape: CudaTapeBuffers, x, directions) -> EstimatorResult:
+    """Hutchinson Laplacian at one point (``src/gpu/stde_gpu.rs:51-81``)."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    dirs = [np.ascontiguousarray(d, dtype=np.float32) for d in directions]
+    for d in dirs:
+        assert d.size == x.size, "direction length must match x"
+    flat = np.ascontiguousarray(np.stack(dirs) if dirs else np.zeros((0, x.size), np.float32), dtype=np.float32)
+    out = _lib.EstimatorResultC()
+    _check(_lib.load().ech_laplacian_gpu_f32(backend._h, tape._h, _lib.ptr(x), x.size, _lib.ptr(flat), len(dirs),
+                                             ctypes.byref(out)))
+    return _result(out, np.float32)
+
+
+def hessian_diagonal_gpu(backend: CudaContext, tape: CudaTapeBuffers, x):
+    """Exact Hessian diagonal via ``n`` basis pushforwards (``src/gpu/stde_gpu.rs:103-129``)."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    value = np.zeros(1, dtype=np.float32)
+    diag = np.empty(x.size, dtype=np.float32)
+    _check(_lib.load().ech_hessian_diagonal_gpu_f32(backend._h, tape._h, _lib.ptr(x), x.size, _lib.ptr(value),
+                                                    _lib.ptr(diag)))
+    return value[0], diag
+
+
+def laplacian_with_control_gpu(backend: CudaContext, tape: CudaTapeBuffers, x, directions,
+                               control_diagonal) -> EstimatorResult:
+    """Control-variate Laplacian (``src/gpu/stde_gpu.rs:135-200``)."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    c = np.ascontiguousarray(control_diagonal, dtype=np.float32)
+    assert c.size == x.size, "control diagonal length must match x"
+    dirs = [np.ascontiguousarray(d, dtype=np.float32) for d in directions]
+    for d in dirs:
+        assert d.size == x.size, "direction length must match x"
+    flat = np.ascontiguousarray(np.stack(dirs) if dirs else np.zeros((0, x.size), np.float32), dtype=np.float32)
+    out = _lib.EstimatorResultC()
+    _check(_lib.load().ech_laplacian_with_control_gpu_f32(backend._h, tape._h, _lib.ptr(x), x.size, _lib.ptr(flat),
+                                                          len(dirs), _lib.ptr(c), ctypes.byref(out)))
+    return _result(out, np.float32)
+
+
+def laplacian_batch(backend: CudaContext, tape, xs, num_directions: int, directions=None,
+                    mode: int = DIR_PER_POINT, seed: int = 0):
+    """Per-point Hutchinson Laplacians for ``xs[B, n]`` with ``num_directions`` each.
+
+    ``mode``: ``DIR_PER_POINT`` (``directions[B, S, n]``), ``DIR_SHARED``
+    (``directions[S, n]``) or ``DIR_RADEMACHER`` (device RNG, ``directions=None``).
+    Returns a structured array with fields value/estimate/sample_variance/
+    standard_error/num_samples.
+    """
+    f64 = isinstance(tape, CudaTapeBuffersF64)
+    dt = np.float64 if f64 else np.float32
+    xs = np.ascontiguousarray(xs, dtype=dt)
+    B = xs.shape[0] if xs.ndim > 1 else 1
+    d = None if directions is None else np.ascontiguousarray(directions, dtype=dt)
+    res = (_lib.EstimatorResultC * B)()
+    fn = _lib.load().ech_laplacian_batch_f64 if f64 else _lib.load().ech_laplacian_batch_f32
+    _check(fn(backend._h, tape._h, _lib.ptr(xs), xs.size, B, _lib.ptr(d), 0 if d is None else d.size,
+              int(num_directions), int(mode), ctypes.c_uint64(seed & 0xFFFFFFFFFFFFFFFF), res))
+    out = np.zeros(B, dtype=[("value", "f8"), ("estimate", "f8"), ("sample_variance", "f8"),
+                             ("standard_error", "f8"), ("num_samples", "u8")])
+    for i in range(B):
+        out[i] = (res[i].value, res[i].estimate, res[i].sample_variance, res[i].standard_error, res[i].num_samples)
+    return out

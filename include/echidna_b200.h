@@ -1,0 +1,222 @@
+/*
+ * echidna_b200 — C ABI of the B200-native batched BytecodeTape engine.
+ *
+ * Every entry point replaces one method of echidna's CUDA backend; the comment on
+ * each names the reference interface (path:line inside the echidna crate).  All
+ * host buffers are caller-owned, borrowed for the duration of the call, and
+ * every length is passed explicitly and checked.  Calls on a context are
+ * synchronous (they return after the device work and copies have finished),
+ * like the reference's `&self` methods that end in `stream.synchronize()`.
+ *
+ * Errors are returned as `ech_status`; `ech_last_error()` gives the message of
+ * the last failing call on the calling thread.  Messages for the cases the
+ * reference reports as `GpuError::Other` use the reference's text (for example
+ * "batch_size must be non-zero").  Length mismatches, which the Rust API treats
+ * as `assert_eq!` panics, return ECH_ERR_INVALID_ARG.
+ *
+ * Layouts: inputs are row-major [batch][num_inputs]; outputs are row-major
+ * [batch][num_outputs]; Taylor coefficients are coefficient-major
+ * [order][batch * num_outputs] (the reference's `TaylorKthBatchResult`).
+ */
+#ifndef ECHIDNA_B200_H
+#define ECHIDNA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define ECH_API __attribute__((visibility("default")))
+#else
+#define ECH_API
+#endif
+
+typedef struct ech_ctx ech_ctx;
+typedef struct ech_tape ech_tape;
+
+/* Mirrors GpuError (src/gpu/mod.rs:276-287) plus two codes of this ABI. */
+typedef enum ech_status {
+  ECH_OK = 0,
+  ECH_ERR_NO_DEVICE = 1,                /* GpuError::NoDevice */
+  ECH_ERR_SHADER_COMPILATION = 2,       /* GpuError::ShaderCompilation (kernels are built offline) */
+  ECH_ERR_OUT_OF_MEMORY = 3,            /* GpuError::OutOfMemory */
+  ECH_ERR_CUSTOM_OPS_NOT_SUPPORTED = 4, /* GpuError::CustomOpsNotSupported */
+  ECH_ERR_OTHER = 5,                    /* GpuError::Other(msg) */
+  ECH_ERR_TIMEOUT = 6,                  /* a bounded device-side wait gave up */
+  ECH_ERR_INVALID_ARG = 7               /* length mismatch / null pointer (Rust: assert panic) */
+} ech_status;
+
+/* EstimatorResult<F> (src/stde/types.rs:9-22), widened to double. */
+typedef struct ech_estimator_result {
+  double value;
+  double estimate;
+  double sample_variance;
+  double standard_error;
+  uint64_t num_samples;
+} ech_estimator_result;
+
+/* Message of the last failing call on this thread ("" if none). */
+ECH_API const char* ech_last_error(void);
+ECH_API const char* ech_version(void);
+
+/* ── context ─────────────────────────────────────────────────────────────── */
+/* CudaContext::new (src/gpu/cuda_backend.rs:503-552).  NO_DEVICE when the
+ * device is absent; kernels are compiled offline, so nothing is JIT-compiled. */
+ECH_API ech_status ech_ctx_create(int device, ech_ctx** out);
+ECH_API void ech_ctx_destroy(ech_ctx* ctx);
+
+/* ── validation (host only, no device needed) ──────────────────────────────── */
+/* BytecodeTape::validate (src/bytecode_tape/mod.rs:575-705). */
+ECH_API ech_status ech_validate_bytecode_tape(const uint32_t* opcodes, const uint32_t* arg0, const uint32_t* arg1,
+                                              uint32_t num_variables, uint32_t num_inputs, uint32_t output_index,
+                                              const uint32_t* output_indices, uint32_t n_output_indices,
+                                              int has_custom_ops);
+/* GpuTapeData::validate (src/gpu/mod.rs:397-564). */
+ECH_API ech_status ech_validate_gpu_tape_data(const uint32_t* opcodes, uint32_t n_opcodes, const uint32_t* arg0,
+                                              uint32_t n_arg0, const uint32_t* arg1, uint32_t n_arg1,
+                                              uint32_t n_constants, uint32_t num_ops, uint32_t num_inputs,
+                                              uint32_t num_variables, uint32_t output_index,
+                                              const uint32_t* output_indices, uint32_t n_output_indices);
+
+/* ── tape upload ───────────────────────────────────────────────────────────── */
+/* GpuBackend::upload_tape (src/gpu/cuda_backend.rs:628-659): GpuTapeData fields
+ * (src/gpu/mod.rs:313-334) with f32 constants.  Invalid data -> ECH_ERR_OTHER
+ * with "refusing to upload invalid GpuTapeData: ..." (the Rust method panics). */
+ECH_API ech_status ech_upload_tape_f32(ech_ctx* ctx, const uint32_t* opcodes, uint32_t n_opcodes,
+                                       const uint32_t* arg0, uint32_t n_arg0, const uint32_t* arg1, uint32_t n_arg1,
+                                       const float* constants, uint32_t n_constants, uint32_t num_ops,
+                                       uint32_t num_inputs, uint32_t num_variables, uint32_t output_index,
+                                       const uint32_t* output_indices, uint32_t n_output_indices, ech_tape** out);
+/* CudaContext::upload_tape_f64 (src/gpu/cuda_backend.rs:566-611): BytecodeTape<f64>
+ * fields.  Custom ops -> CUSTOM_OPS_NOT_SUPPORTED; invalid tape -> OTHER. */
+ECH_API ech_status ech_upload_tape_f64(ech_ctx* ctx, const uint32_t* opcodes, const uint32_t* arg0,
+                                       const uint32_t* arg1, const double* values, uint32_t num_variables,
+                                       uint32_t num_inputs, uint32_t output_index, const uint32_t* output_indices,
+                                       uint32_t n_output_indices, int has_custom_ops, ech_tape** out);
+ECH_API void ech_tape_destroy(ech_tape* tape);
+/* GpuBackend::num_outputs (src/gpu/mod.rs:113). */
+ECH_API uint32_t ech_tape_num_outputs(const ech_tape* tape);
+ECH_API uint32_t ech_tape_num_inputs(const ech_tape* tape);
+ECH_API uint32_t ech_tape_num_variables(const ech_tape* tape);
+
+/* ── batched sweeps (host buffers) ─────────────────────────────────────────── */
+/* forward_batch / forward_batch_f64 (src/gpu/cuda_backend.rs:661-676, 878-893). */
+ECH_API ech_status ech_forward_batch_f32(ech_ctx* ctx, const ech_tape* tape, const float* inputs, size_t n_inputs,
+                                         uint32_t batch_size, float* outputs, size_t n_outputs);
+ECH_API ech_status ech_forward_batch_f64(ech_ctx* ctx, const ech_tape* tape, const double* inputs, size_t n_inputs,
+                                         uint32_t batch_size, double* outputs, size_t n_outputs);
+/* gradient_batch / gradient_batch_f64 (src/gpu/cuda_backend.rs:678-694, 896-912). */
+ECH_API ech_status ech_gradient_batch_f32(ech_ctx* ctx, const ech_tape* tape, const float* inputs, size_t n_inputs,
+                                          uint32_t batch_size, float* outputs, size_t n_outputs, float* grads,
+                                          size_t n_grads);
+ECH_API ech_status ech_gradient_batch_f64(ech_ctx* ctx, const ech_tape* tape, const double* inputs,
+                                          size_t n_inputs, uint32_t batch_size, double* outputs, size_t n_outputs,
+                                          double* grads, size_t n_grads);
+/* hvp_batch / hvp_batch_f64 (src/gpu/cuda_backend.rs:705-722, 935-952): one x,
+ * batch_size directions. */
+ECH_API ech_status ech_hvp_batch_f32(ech_ctx* ctx, const ech_tape* tape, const float* x, size_t n_x,
+                                     const float* tangent_dirs, size_t n_dirs, uint32_t batch_size, float* grads,
+                                     size_t n_grads, float* hvps, size_t n_hvps);
+ECH_API ech_status ech_hvp_batch_f64(ech_ctx* ctx, const ech_tape* tape, const double* x, size_t n_x,
+                                     const double* tangent_dirs, size_t n_dirs, uint32_t batch_size, double* grads,
+                                     size_t n_grads, double* hvps, size_t n_hvps);
+/* Extension (no reference counterpart): per-point HVP, x row-major [batch][n]. */
+ECH_API ech_status ech_hvp_batch_points_f32(ech_ctx* ctx, const ech_tape* tape, const float* xs, size_t n_xs,
+                                            const float* tangent_dirs, size_t n_dirs, uint32_t batch_size,
+                                            float* grads, size_t n_grads, float* hvps, size_t n_hvps);
+ECH_API ech_status ech_hvp_batch_points_f64(ech_ctx* ctx, const ech_tape* tape, const double* xs, size_t n_xs,
+                                            const double* tangent_dirs, size_t n_dirs, uint32_t batch_size,
+                                            double* grads, size_t n_grads, double* hvps, size_t n_hvps);
+/* The tangent_forward kernel of the reference (src/gpu/kernels/tape_eval.cu:357-510)
+ * that sparse_jacobian dispatches (src/gpu/cuda_backend.rs:306-358): JVP per row. */
+ECH_API ech_status ech_tangent_forward_batch_f32(ech_ctx* ctx, const ech_tape* tape, const float* primals,
+                                                 size_t n_primals, const float* seeds, size_t n_seeds,
+                                                 uint32_t batch_size, float* values, float* tangents,
+                                                 size_t n_outputs);
+ECH_API ech_status ech_tangent_forward_batch_f64(ech_ctx* ctx, const ech_tape* tape, const double* primals,
+                                                 size_t n_primals, const double* seeds, size_t n_seeds,
+                                                 uint32_t batch_size, double* values, double* tangents,
+                                                 size_t n_outputs);
+/* taylor_forward_kth_batch{,_f64} (src/gpu/cuda_backend.rs:829-873): order 1..=5,
+ * otherwise ECH_ERR_OTHER "unsupported Taylor order {k}, must be 1..=5".
+ * coefficients: [order][batch_size * num_outputs]. */
+ECH_API ech_status ech_taylor_forward_kth_batch_f32(ech_ctx* ctx, const ech_tape* tape, const float* primals,
+                                                    size_t n_primals, const float* seeds, size_t n_seeds,
+                                                    uint32_t batch_size, uint32_t order, float* coefficients,
+                                                    size_t n_coefficients);
+ECH_API ech_status ech_taylor_forward_kth_batch_f64(ech_ctx* ctx, const ech_tape* tape, const double* primals,
+                                                    size_t n_primals, const double* seeds, size_t n_seeds,
+                                                    uint32_t batch_size, uint32_t order, double* coefficients,
+                                                    size_t n_coefficients);
+
+/* ── STDE (src/gpu/stde_gpu.rs) ───────────────────────────────────────────── */
+/* laplacian_gpu (src/gpu/stde_gpu.rs:51-97): directions row-major [S][n]. */
+ECH_API ech_status ech_laplacian_gpu_f32(ech_ctx* ctx, const ech_tape* tape, const float* x, size_t n,
+                                         const float* directions, uint32_t num_directions,
+                                         ech_estimator_result* out);
+/* hessian_diagonal_gpu (src/gpu/stde_gpu.rs:103-129). */
+ECH_API ech_status ech_hessian_diagonal_gpu_f32(ech_ctx* ctx, const ech_tape* tape, const float* x, size_t n,
+                                                float* value, float* diag);
+/* laplacian_with_control_gpu (src/gpu/stde_gpu.rs:135-200). */
+ECH_API ech_status ech_laplacian_with_control_gpu_f32(ech_ctx* ctx, const ech_tape* tape, const float* x, size_t n,
+                                                      const float* directions, uint32_t num_directions,
+                                                      const float* control_diagonal, ech_estimator_result* out);
+/* Extension (no reference counterpart): many points x S directions in one launch
+ * with the per-point reduction on the device.  dir_mode 0: directions
+ * [batch][S][n]; 1: directions [S][n] shared by all points; 2: Rademacher
+ * directions from a counter-based device RNG (Philox-4x32-10) keyed by `seed`.
+ * results: [batch] EstimatorResult of the samples 2*c2 (Welford order = S). */
+ECH_API ech_status ech_laplacian_batch_f32(ech_ctx* ctx, const ech_tape* tape, const float* xs, size_t n_xs,
+                                           uint32_t batch_size, const float* directions, size_t n_directions,
+                                           uint32_t num_directions, int dir_mode, uint64_t seed,
+                                           ech_estimator_result* results);
+ECH_API ech_status ech_laplacian_batch_f64(ech_ctx* ctx, const ech_tape* tape, const double* xs, size_t n_xs,
+                                           uint32_t batch_size, const double* directions, size_t n_directions,
+                                           uint32_t num_directions, int dir_mode, uint64_t seed,
+                                           ech_estimator_result* results);
+
+/* ── device-pointer variants (inputs already resident in HBM) ─────────────── */
+/* Same semantics as the host-buffer calls; pointers are device pointers, the
+ * work is enqueued on `stream` (a cudaStream_t, NULL = the context's stream)
+ * and the call returns without synchronising.  Scratch is owned by the
+ * context, so calls on one context must not overlap on different streams. */
+ECH_API ech_status ech_forward_batch_device(ech_ctx* ctx, const ech_tape* tape, int f64, const void* inputs,
+                                            uint32_t batch_size, void* outputs, void* stream);
+ECH_API ech_status ech_gradient_batch_device(ech_ctx* ctx, const ech_tape* tape, int f64, const void* inputs,
+                                             uint32_t batch_size, void* outputs, void* grads, void* stream);
+ECH_API ech_status ech_hvp_batch_device(ech_ctx* ctx, const ech_tape* tape, int f64, const void* xs, int x_per_point,
+                                        const void* dirs, uint32_t batch_size, void* grads, void* hvps, void* stream);
+ECH_API ech_status ech_taylor_batch_device(ech_ctx* ctx, const ech_tape* tape, int f64, const void* primals,
+                                           const void* seeds, uint32_t batch_size, uint32_t order,
+                                           void* coefficients, void* stream);
+/* Waits for the context's stream and reports any device-side error word. */
+ECH_API ech_status ech_ctx_synchronize(ech_ctx* ctx);
+
+/* ── introspection ────────────────────────────────────────────────────────── */
+/* kind: 0 forward, 1 gradient, 2 hvp, 3 tangent, 4 taylor(order).  Fills
+ * stats[12]: fwd_ops, rev_ops, max_live_fwd, max_live_rev, traj_values,
+ * flops_fwd, flops_rev, specials_fwd, specials_rev, smem_regs, far_slots,
+ * n_instructions. */
+ECH_API ech_status ech_tape_plan_stats(ech_ctx* ctx, const ech_tape* tape, int kind, uint32_t order, int f64,
+                                       uint64_t* stats);
+/* Host-only lowering dump (no device needed): the forward / reverse programs
+ * (32-byte records) and constant pool for `kind` with `smem_reg_cap` shared
+ * registers.  counts[6]: n_fwd, n_rev, n_pool, smem_regs, far_slots,
+ * traj_slots.  Used to check the lowering on machines without a GPU. */
+ECH_API ech_status ech_plan_dump(const uint32_t* opcodes, const uint32_t* arg0, const uint32_t* arg1,
+                                 const double* values, uint32_t num_variables, uint32_t num_inputs,
+                                 uint32_t output_index, const uint32_t* output_indices, uint32_t n_output_indices,
+                                 int kind, uint32_t smem_reg_cap, void* fwd, size_t fwd_cap, void* rev,
+                                 size_t rev_cap, double* pool, size_t pool_cap, uint64_t* counts);
+/* Launch configuration override for tuning (0 = automatic): threads per CTA,
+ * points per thread and the shared-register cap. */
+ECH_API ech_status ech_ctx_set_launch(ech_ctx* ctx, uint32_t threads, uint32_t points_per_thread,
+                                      uint32_t smem_reg_cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ECHIDNA_B200_H */

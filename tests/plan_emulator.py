@@ -1,0 +1,165 @@
+"""Executes the engine's lowered programs on the CPU (numpy, float64).
+
+A checker for the host-side lowering: register allocation, trajectory saves and
+the reverse schedule.  It supports the opcodes the lowering tests use and the
+plain-value (gradient) kind.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import struct
+
+import numpy as np
+
+from echidna_b200 import _lib
+from echidna_b200.tape import OpCode
+
+INS = struct.Struct("<BBBBIIIIid")
+RINS = struct.Struct("<BBHIIIIIIi")
+XI_LDIN, XI_STOUT, XI_MOV, XI_SEED, XI_STGRAD = 64, 65, 66, 67, 68
+M_SMEM, M_GLOB, M_IMM, M_NONE = 0, 1, 2, 3
+NONE = 0xFFFFFFFF
+RF = dict(R_GLOB=1, A_GLOB=2, B_GLOB=4, A_INIT=8, B_INIT=16, VA_IMM=32, VB_IMM=64, HAS_A=128, HAS_B=256)
+KIND = {"forward": 0, "gradient": 1, "hvp": 2, "tangent": 3, "taylor": 4}
+
+
+def plan_dump(tape, kind: str, cap: int):
+    lib = _lib.load()
+    op, a0, a1, vals = tape.arrays()
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    outs = np.asarray(tape.output_indices, dtype=np.uint32)
+    counts = (ctypes.c_uint64 * 6)()
+    args = [_lib.ptr(op), _lib.ptr(a0), _lib.ptr(a1), _lib.ptr(vals), len(op), tape.num_inputs, tape.output_index,
+            _lib.ptr(outs), len(outs), KIND[kind], cap]
+    st = lib.ech_plan_dump(*args, None, 0, None, 0, None, 0, counts)
+    assert st == 0, _lib.last_error()
+    nf, nr, npool = counts[0], counts[1], counts[2]
+    fb = ctypes.create_string_buffer(max(nf, 1) * 32)
+    rb = ctypes.create_string_buffer(max(nr, 1) * 32)
+    pool = np.zeros(max(npool, 1), dtype=np.float64)
+    st = lib.ech_plan_dump(*args, ctypes.addressof(fb), nf, ctypes.addressof(rb), nr, _lib.ptr(pool), npool, counts)
+    assert st == 0, _lib.last_error()
+    fwd = [INS.unpack_from(fb, 32 * k) for k in range(nf)]
+    rev = [RINS.unpack_from(rb, 32 * k) for k in range(nr)]
+    return fwd, rev, pool, dict(smem_regs=counts[3], far_slots=counts[4], traj_slots=counts[5])
+
+
+def _fwd(op, a, b, aux):
+    with np.errstate(all="ignore"):
+        if op == OpCode.Add: return a + b
+        if op == OpCode.Sub: return a - b
+        if op == OpCode.Mul: return a * b
+        if op == OpCode.Div: return a / b
+        if op == OpCode.Neg: return -a
+        if op == OpCode.Sin: return np.array([math.sin(v) for v in a])
+        if op == OpCode.Cos: return np.array([math.cos(v) for v in a])
+        if op == OpCode.Exp: return np.array([math.exp(v) for v in a])
+        if op == OpCode.Tanh: return np.array([math.tanh(v) for v in a])
+        if op == OpCode.Ln: return np.array([math.log(v) for v in a])
+        if op == OpCode.Sqrt: return np.sqrt(a)
+        if op == OpCode.Powi:
+            out = np.empty_like(a)
+            for i, v in enumerate(a):
+                m, r, base = abs(aux), 1.0, v
+                while True:
+                    if m & 1:
+                        r = r * base
+                    m >>= 1
+                    if m == 0:
+                        break
+                    base = base * base
+                out[i] = 1.0 / r if aux < 0 else r
+            return out
+    raise NotImplementedError(OpCode(op).name)
+
+
+def _partials(op, a, b, r, aux):
+    one = np.ones_like(r if r is not None else a)
+    zero = np.zeros_like(one)
+    with np.errstate(all="ignore"):
+        if op == OpCode.Add: return one, one
+        if op == OpCode.Sub: return one, -one
+        if op == OpCode.Mul: return b, a
+        if op == OpCode.Div:
+            inv = 1.0 / b
+            return inv, -r * inv
+        if op == OpCode.Neg: return -one, zero
+        if op == OpCode.Sin: return np.array([math.cos(v) for v in a]), zero
+        if op == OpCode.Cos: return -np.array([math.sin(v) for v in a]), zero
+        if op == OpCode.Exp: return r, zero
+        if op == OpCode.Tanh:
+            c = np.array([math.cosh(v) for v in a])
+            return 1.0 / (c * c), zero
+        if op == OpCode.Ln: return np.where(a >= 0, 1.0 / a, np.nan), zero
+        if op == OpCode.Sqrt: return 1.0 / ((1.0 + 1.0) * r), zero
+        if op == OpCode.Powi:
+            if aux == 0: return zero, zero
+            return aux * _fwd(OpCode.Powi, a, None, aux - 1), zero
+    raise NotImplementedError(OpCode(op).name)
+
+
+def run_gradient(tape, X, cap):
+    """Emulates the gradient programs; returns (outputs, grads)."""
+    fwd, rev, pool, _ = plan_dump(tape, "gradient", cap)
+    X = np.asarray(X, dtype=np.float64)
+    B = X.shape[0]
+    regs = {M_SMEM: {}, M_GLOB: {}}
+    traj = {}
+    nout = len(tape.all_output_indices())
+    outs = np.full((B, nout), np.nan)
+
+    def ld(mode, idx, imm):
+        if mode == M_IMM:
+            return np.full(B, imm)
+        return regs[mode][idx]
+
+    for (opc, ma, mb, md, a, b, d, save, aux, imm) in fwd:
+        if opc == XI_LDIN:
+            v = X[:, aux].copy()
+        elif opc == XI_STOUT:
+            outs[:, aux] = ld(ma, a, imm)
+            continue
+        elif opc == XI_MOV:
+            v = ld(ma, a, imm)
+        else:
+            av = ld(ma, a, imm)
+            bv = np.zeros(B) if mb == M_NONE else ld(mb, b, imm)
+            v = _fwd(opc, av, bv, aux)
+        if md != M_NONE:
+            regs[md][d] = v
+        if save != NONE:
+            traj[save] = v
+    grads = np.full((B, tape.num_inputs), np.nan)
+    regs = {M_SMEM: {}, M_GLOB: {}}
+    for (opc, _pad, fl, r, a, b, va, vb, vr, aux) in rev:
+        mr = M_GLOB if fl & RF["R_GLOB"] else M_SMEM
+        if opc == XI_SEED:
+            regs[mr][r] = np.ones(B)
+            continue
+        if opc == XI_STGRAD:
+            grads[:, aux] = 0.0 if r == NONE else regs[mr][r]
+            continue
+        adj = regs[mr][r]
+
+        def val(idx, is_imm):
+            if idx == NONE:
+                return np.zeros(B)
+            return np.full(B, pool[idx]) if is_imm else traj[idx]
+
+        A = val(va, fl & RF["VA_IMM"])
+        Bv = val(vb, fl & RF["VB_IMM"])
+        R = None if vr == NONE else traj[vr]
+        da, db = _partials(opc, A, Bv, R if R is not None else np.zeros(B), aux)
+        live = adj != 0
+        for has, init, glob, idx, dd in ((RF["HAS_A"], RF["A_INIT"], RF["A_GLOB"], a, da),
+                                         (RF["HAS_B"], RF["B_INIT"], RF["B_GLOB"], b, db)):
+            if not fl & has:
+                continue
+            m = M_GLOB if fl & glob else M_SMEM
+            old = np.zeros(B) if fl & init else regs[m][idx]
+            hit = live & (dd != 0)
+            with np.errstate(all="ignore"):
+                new = np.where(hit, old + dd * adj, old)
+            regs[m][idx] = new
+    return outs, grads

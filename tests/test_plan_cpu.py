@@ -1,0 +1,57 @@
+"""The host lowering, checked on the CPU: the emulated programs must reproduce
+the oracle's outputs and gradients bit for bit at every shared-register cap
+(cap 1 forces nearly every value into the global slots)."""
+import numpy as np
+import pytest
+
+from echidna_b200 import configs, constant, record
+from oracle.oracle import OracleTape
+from tests.plan_emulator import plan_dump, run_gradient
+
+
+def _tapes():
+    yield "rosen10", configs.rosenbrock(10)
+    yield "mlp4", configs.mlp(4, 4)
+    yield "dag", configs.random_dag(6, 300, seed=7)
+    yield "dag2", configs.random_dag(3, 120, seed=11)
+    yield "square", record(lambda v: v[0] * v[0], [2.0])[0]
+    yield "powi", record(lambda v: v[0].powi(3) + v[1].powi(-2), [2.0, 1.5])[0]
+    yield "output_is_input", record(lambda v: v[1], [2.0, 3.0])[0]
+    yield "const_output", record(lambda v: constant(2.0) * constant(3.0), [2.0])[0]
+    yield "unused_input", record(lambda v: v[0].sin() * v[0], [2.0, 5.0])[0]
+
+
+@pytest.mark.parametrize("cap", [1, 2, 3, 8, 4096])
+@pytest.mark.parametrize("name,tape", list(_tapes()))
+def test_lowered_gradient_matches_oracle(name, tape, cap):
+    rng = np.random.default_rng(3)
+    X = rng.uniform(-1.5, 1.5, size=(7, tape.num_inputs))
+    out, grad = run_gradient(tape, X, cap)
+    o = OracleTape(tape)
+    ref_out, ref_grad = o.gradient(X)
+    np.testing.assert_array_equal(out, ref_out)
+    np.testing.assert_array_equal(grad, ref_grad)
+
+
+@pytest.mark.parametrize("cap", [1, 4, 64, 4096])
+def test_register_caps_respected(cap):
+    tape = configs.mlp(8, 8)
+    fwd, rev, pool, info = plan_dump(tape, "gradient", cap)
+    assert info["smem_regs"] <= cap
+    # every shared / global index referenced is in range
+    for ins in fwd:
+        _, ma, mb, md, a, b, d, save, aux, imm = ins
+        for m, i in ((ma, a), (mb, b), (md, d)):
+            if m == 0:
+                assert i < info["smem_regs"]
+            elif m == 1:
+                assert i < info["far_slots"]
+        if save != 0xFFFFFFFF:
+            assert save < info["traj_slots"]
+
+
+def test_mlp_trajectory_is_three_layers_of_width():
+    # values read by reverse partials: the 2x64 tanh arguments and the 64 squared outputs
+    tape = configs.mlp(64, 64)
+    _, _, _, info = plan_dump(tape, "gradient", 4096)
+    assert info["traj_slots"] == 3 * 64
