@@ -26,7 +26,8 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC
            "--expt-relaxed-constexpr", "-I", CSRC, "-I", os.path.join(ROOT, "include")]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-ffp-contract=off", "-I", CSRC]
 
-CU_SOURCES = ["abi.cu", "k_plain.cu", "k_dual.cu", "k_jet.cu", "stde.cu"]
+CU_SOURCES = ["abi.cu", "k_plain.cu", "k_dual.cu", "k_jet.cu", "k_jet1.cu", "k_jet2.cu", "k_jet3.cu", "k_jet4.cu", "k_jet5.cu",
+              "stde.cu"]
 CXX_SOURCES = ["plan.cpp"]
 HEADERS = ["ech_types.h", "device_math.cuh", "interp.cuh", "launch.h", "plan.h", "k_common.cuh"]
 

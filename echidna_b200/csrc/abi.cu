@@ -60,13 +60,15 @@ struct DevBuf {
 
 struct DevPlan {
   Plan host;
-  Ins* d_fwd = nullptr;
-  RIns* d_rev = nullptr;
-  double* d_pool = nullptr;
+  DIns* d_fwd = nullptr;
+  DRIns* d_rev = nullptr;
+  DFTerm* d_fterms = nullptr;  // fused-chain terms (forward form)
+  DRTerm* d_rterms = nullptr;  // fused-chain terms (reverse form)
   ~DevPlan() {
     if (d_fwd) cudaFree(d_fwd);
     if (d_rev) cudaFree(d_rev);
-    if (d_pool) cudaFree(d_pool);
+    if (d_fterms) cudaFree(d_fterms);
+    if (d_rterms) cudaFree(d_rterms);
   }
 };
 
@@ -87,7 +89,7 @@ struct ech_tape {
   bool f64 = true;
   HostTape host;
   std::mutex mu;
-  std::map<std::tuple<int, int, uint32_t>, std::unique_ptr<DevPlan>> plans;  // (kind, K, cap)
+  std::map<std::tuple<int, int, uint32_t, uint32_t, uint32_t>, std::unique_ptr<DevPlan>> plans;  // (kind, K, cap, tile, vbytes)
 };
 
 // ───────────────────────────── context ──────────────────────────────────────
@@ -124,7 +126,7 @@ extern "C" ECH_API void ech_ctx_destroy(ech_ctx* ctx) {
 extern "C" ECH_API ech_status ech_ctx_set_launch(ech_ctx* ctx, uint32_t threads, uint32_t ppt, uint32_t cap) {
   if (!ctx) return fail(ECH_ERR_INVALID_ARG, "ctx is null");
   if (threads && (threads % 32 || threads > 256)) return fail(ECH_ERR_INVALID_ARG, "threads must be a multiple of 32, <= 256");
-  if (ppt && ppt != 1 && ppt != 2) return fail(ECH_ERR_INVALID_ARG, "points_per_thread must be 1 or 2");
+  if (ppt && ppt != 1 && ppt != 2 && ppt != 4) return fail(ECH_ERR_INVALID_ARG, "points_per_thread must be 1, 2 or 4");
   ctx->ov_threads = threads;
   ctx->ov_ppt = ppt;
   ctx->ov_cap = cap;
@@ -221,7 +223,6 @@ extern "C" ECH_API uint32_t ech_tape_num_inputs(const ech_tape* t) { return t ? 
 extern "C" ECH_API uint32_t ech_tape_num_variables(const ech_tape* t) { return t ? t->host.nv : 0; }
 
 // ───────────────────────────── plans and launch configuration ───────────────
-static const int kRingBytes = kStages * kChunk * 32;
 
 struct LaunchCfg {
   LaunchReq req;
@@ -262,9 +263,9 @@ static LaunchCfg choose_cfg(ech_ctx* ctx, const ech_tape* t, int kind, int K) {
   return c;
 }
 
-static ech_status get_plan(ech_tape* t, int kind, int K, uint32_t cap, DevPlan** out) {
+static ech_status get_plan(ech_tape* t, int kind, int K, uint32_t cap, uint32_t tile, uint32_t vbytes, DevPlan** out) {
   std::lock_guard<std::mutex> lk(t->mu);
-  auto key = std::make_tuple(kind, K, cap);
+  auto key = std::make_tuple(kind, K, cap, tile, vbytes);
   auto it = t->plans.find(key);
   if (it != t->plans.end()) {
     *out = it->second.get();
@@ -272,13 +273,19 @@ static ech_status get_plan(ech_tape* t, int kind, int K, uint32_t cap, DevPlan**
   }
   std::unique_ptr<DevPlan> dp(new DevPlan());
   dp->host = build_plan(t->host, kind_of(kind), cap);
-  const Plan& p = dp->host;
-  CU(cudaMalloc(&dp->d_fwd, std::max<size_t>(p.fwd.size(), 1) * sizeof(Ins)));
-  if (!p.fwd.empty()) CU(cudaMemcpy(dp->d_fwd, p.fwd.data(), p.fwd.size() * sizeof(Ins), cudaMemcpyHostToDevice));
-  CU(cudaMalloc(&dp->d_rev, std::max<size_t>(p.rev.size(), 1) * sizeof(RIns)));
-  if (!p.rev.empty()) CU(cudaMemcpy(dp->d_rev, p.rev.data(), p.rev.size() * sizeof(RIns), cudaMemcpyHostToDevice));
-  CU(cudaMalloc(&dp->d_pool, p.pool.size() * sizeof(double)));
-  CU(cudaMemcpy(dp->d_pool, p.pool.data(), p.pool.size() * sizeof(double), cudaMemcpyHostToDevice));
+  DevProgram prog;
+  std::string err;
+  if (!encode_plan(dp->host, tile, vbytes, prog, err)) return fail(ECH_ERR_OTHER, err);
+  CU(cudaMalloc(&dp->d_fwd, std::max<size_t>(prog.fwd.size(), 1) * sizeof(DIns)));
+  if (!prog.fwd.empty())
+    CU(cudaMemcpy(dp->d_fwd, prog.fwd.data(), prog.fwd.size() * sizeof(DIns), cudaMemcpyHostToDevice));
+  CU(cudaMalloc(&dp->d_rev, std::max<size_t>(prog.rev.size(), 1) * sizeof(DRIns)));
+  if (!prog.rev.empty())
+    CU(cudaMemcpy(dp->d_rev, prog.rev.data(), prog.rev.size() * sizeof(DRIns), cudaMemcpyHostToDevice));
+  CU(cudaMalloc(&dp->d_fterms, prog.fterms.size() * sizeof(DFTerm)));
+  CU(cudaMemcpy(dp->d_fterms, prog.fterms.data(), prog.fterms.size() * sizeof(DFTerm), cudaMemcpyHostToDevice));
+  CU(cudaMalloc(&dp->d_rterms, prog.rterms.size() * sizeof(DRTerm)));
+  CU(cudaMemcpy(dp->d_rterms, prog.rterms.data(), prog.rterms.size() * sizeof(DRTerm), cudaMemcpyHostToDevice));
   *out = dp.get();
   t->plans[key] = std::move(dp);
   return ECH_OK;
@@ -301,7 +308,7 @@ static ech_status enqueue(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n
                           cudaStream_t st) {
   LaunchCfg c = choose_cfg(ctx, t, kind, K);
   DevPlan* dp = nullptr;
-  ech_status s = get_plan(t, kind, K, c.cap, &dp);
+  ech_status s = get_plan(t, kind, K, c.cap, c.tile, (uint32_t)c.vbytes, &dp);
   if (s != ECH_OK) return s;
   const Plan& p = dp->host;
   const uint32_t regs = std::max<uint32_t>(p.smem_regs, 1);
@@ -311,7 +318,8 @@ static ech_status enqueue(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n
   kp.n_fwd = (uint32_t)p.fwd.size();
   kp.rev = dp->d_rev;
   kp.n_rev = c.req.rev ? (uint32_t)p.rev.size() : 0u;
-  kp.pool = dp->d_pool;
+  kp.fterms = dp->d_fterms;
+  kp.rterms = dp->d_rterms;
   kp.far_slots = p.far_slots;
   kp.smem_regs = regs;
   kp.tile = c.tile;
@@ -832,7 +840,8 @@ ECH_API ech_status ech_ctx_synchronize(ech_ctx* ctx) {
 ECH_API ech_status ech_plan_dump(const uint32_t* op, const uint32_t* a0, const uint32_t* a1, const double* values,
                                  uint32_t nv, uint32_t ni, uint32_t output_index, const uint32_t* outs,
                                  uint32_t nouts, int kind, uint32_t cap, void* fwd, size_t fwd_cap, void* rev,
-                                 size_t rev_cap, double* pool, size_t pool_cap, uint64_t* counts) {
+                                 size_t rev_cap, double* pool, size_t pool_cap, void* terms, size_t terms_cap,
+                                 uint64_t* counts) {
   if (!op || !a0 || !a1 || !values || !counts) return fail(ECH_ERR_INVALID_ARG, "null argument");
   std::string m = validate_bytecode_tape(op, a0, a1, nv, ni, output_index, outs, nouts, false);
   if (!m.empty()) return fail(ECH_ERR_OTHER, "invalid bytecode tape: " + m);
@@ -854,6 +863,8 @@ ECH_API ech_status ech_plan_dump(const uint32_t* op, const uint32_t* a0, const u
   counts[3] = p.smem_regs;
   counts[4] = p.far_slots;
   counts[5] = p.traj_slots;
+  counts[6] = p.terms.size();
+  if (terms) memcpy(terms, p.terms.data(), std::min(terms_cap, p.terms.size()) * sizeof(PTerm));
   if (fwd) memcpy(fwd, p.fwd.data(), std::min(fwd_cap, p.fwd.size()) * sizeof(Ins));
   if (rev) memcpy(rev, p.rev.data(), std::min(rev_cap, p.rev.size()) * sizeof(RIns));
   if (pool) memcpy(pool, p.pool.data(), std::min(pool_cap, p.pool.size()) * sizeof(double));

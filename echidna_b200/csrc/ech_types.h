@@ -19,6 +19,23 @@ enum OpCode : uint8_t {
   XI_MOV = 66,    // dst <- a (used to materialise a constant operand)
   XI_SEED = 67,   // reverse: adj(r) <- 1
   XI_STGRAD = 68, // reverse: grad[aux] <- adj(r)   (r mode NONE -> 0)
+  XI_CHAIN = 69,  // fused linear chain: dst <- acc0 (+|-) term_1 (+|-) ... ; terms in the chain table
+};
+
+// One term of a fused chain s_t = s_{t-1} (+|-) term_t.  `kind` says how the
+// term is formed, `op` where the running value sits in the Add/Sub:
+//   kind: 0 x, 1 c*x (Mul(c, x)), 2 x*c (Mul(x, c)), 3 x*y (Mul(x, y)), 4 c (constant)
+//   op:   0 acc+term, 1 term+acc, 2 acc-term, 3 term-acc
+// Index form (plan): x, y are value vregs (slot ids); ax/ay the same slots for
+// the adjoints; flags carry the reverse's first-contribution marks.
+enum ChainKind : uint8_t { CK_X = 0, CK_CX = 1, CK_XC = 2, CK_XY = 3, CK_C = 4 };
+enum ChainFlag : uint16_t {
+  CF_X_INIT = 1 << 0,   // first reverse contribution to adj(x): start from +0
+  CF_Y_INIT = 1 << 1,
+  CF_X_GLOB = 1 << 2,   // (device) adj(x) lives in global slots
+  CF_Y_GLOB = 1 << 3,
+  CF_X_ADJ = 1 << 4,    // adj(x) receives contributions (x is not a constant)
+  CF_Y_ADJ = 1 << 5,
 };
 
 constexpr uint32_t kUnused = 0xFFFFFFFFu;
@@ -68,9 +85,70 @@ struct alignas(16) RIns {
 };
 static_assert(sizeof(RIns) == 32, "RIns must be 32 bytes");
 
+// ───────── device encoding (what the kernels execute) ─────────
+// The plan above is in register-index form; before upload it is encoded for a
+// launch geometry: every register / slot becomes a byte offset from the
+// thread's column base (slot * tile * sizeof(value)), and ops whose operands
+// are all shared-memory registers or immediates get mode-specialised opcodes.
+enum DOp : uint8_t {
+  // 2..42: generic tape opcode, operand modes in the instruction
+  D_LDIN = 64, D_STOUT = 65, D_MOV = 66, D_SEED = 67, D_STGRAD = 68,
+  // forward binary fast forms: a, b in {smem register, immediate}, dst smem
+  D_ADD_RR = 72, D_ADD_IR, D_ADD_RI, D_SUB_RR, D_SUB_IR, D_SUB_RI,
+  D_MUL_RR, D_MUL_IR, D_MUL_RI, D_DIV_RR, D_DIV_IR, D_DIV_RI,  // .. 83
+  D_CHAIN = 69,     // fused linear chain (forward and reverse)
+  D_FU_BASE = 96,   // forward unary fast form: 96 + (op - OP_NEG), a and dst smem
+  D_RF_BASE = 128,  // reverse fast form: 128 + op, every adjoint location in smem
+};
+
+// Forward instruction as executed, 32 bytes.
+struct alignas(16) DIns {
+  uint8_t opc;
+  uint8_t ma, mb, md;
+  uint32_t a, b, d;    // byte offsets (smem / global region), unused for M_IMM
+  uint32_t save;       // byte offset in the trajectory region, or kNone
+  int32_t aux;
+  double imm;
+};
+static_assert(sizeof(DIns) == 32, "DIns must be 32 bytes");
+
+// Reverse instruction as executed, 48 bytes (carries its constant operand).
+struct alignas(16) DRIns {
+  uint8_t opc;
+  uint8_t pad;
+  uint16_t flags;      // RFlag bits
+  uint32_t r, a, b;    // byte offsets of adjoint locations
+  uint32_t va, vb, vr; // byte offsets in the trajectory region, or kNone
+  int32_t aux;
+  double imm;          // value of the constant operand (RF_VA_IMM / RF_VB_IMM)
+  uint64_t pad2;
+};
+static_assert(sizeof(DRIns) == 48, "DRIns must be 48 bytes");
+
+// Chain terms as executed.  Forward: operand locations; reverse: adjoint
+// locations and trajectory offsets of the values an x*y term reads.
+struct alignas(16) DFTerm {
+  uint8_t kind, op, xm, ym;   // xm / ym: M_SMEM or M_GLOB
+  uint32_t x, y;              // byte offsets
+  uint32_t pad;
+  double c;
+  uint64_t pad2;
+};
+static_assert(sizeof(DFTerm) == 32, "DFTerm must be 32 bytes");
+struct alignas(16) DRTerm {
+  uint8_t kind, op;
+  uint16_t flags;             // ChainFlag bits
+  uint32_t ax, ay;            // adjoint byte offsets
+  uint32_t vx, vy;            // trajectory byte offsets (x*y terms)
+  uint32_t pad;
+  double c;
+};
+static_assert(sizeof(DRTerm) == 32, "DRTerm must be 32 bytes");
+
 // Interpreter geometry shared by every kernel.
 constexpr int kChunk = 128;   // instructions per staged chunk
 constexpr int kStages = 3;    // staged chunks in flight
+constexpr int kRingBytes = kStages * kChunk * 48;  // sized for the larger record
 
 // Error word bits written by kernels (never trap).
 enum KErr : uint32_t {

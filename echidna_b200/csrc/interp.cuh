@@ -9,6 +9,9 @@
 //     sweep's trajectory), one region per CTA reused across its tiles.
 // The instruction stream is staged into shared memory chunk by chunk with
 // cp.async.bulk (TMA bulk copies) signalled on mbarriers, kStages deep.
+// Instructions carry byte offsets from the thread's column base and, for the
+// common shapes, mode-specialised opcodes (see DOp in ech_types.h), so a
+// typical op is: two vector loads, the arithmetic, one vector store.
 //
 // Semantics per instruction follow the reference's BytecodeTape sweeps:
 // forward_dispatch (src/bytecode_tape/forward.rs:11-43), reverse_sweep_core
@@ -24,11 +27,12 @@ namespace ech {
 
 // ───────────────────────────── launch parameters ────────────────────────────
 struct KParams {
-  const Ins* fwd;        // forward program
+  const DIns* fwd;       // forward program (device encoding)
   uint32_t n_fwd;
-  const RIns* rev;       // reverse program (gradient / HVP kinds)
+  const DRIns* rev;      // reverse program (gradient / HVP kinds)
   uint32_t n_rev;
-  const double* pool;    // reverse-side constant pool
+  const DFTerm* fterms;  // fused-chain terms, forward form (D_CHAIN)
+  const DRTerm* rterms;  // fused-chain terms, reverse form
   void* scratch;         // per-CTA global slot regions
   uint64_t scratch_stride_bytes;  // bytes per CTA region
   uint32_t far_slots;    // global slots before the trajectory region
@@ -97,54 +101,55 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 
 // ───────────────────────────── instruction ring ─────────────────────────────
 // All threads consume the same chunks in the same order.  `seq` counts chunks
-// consumed by this CTA over its lifetime and picks (stage, parity).
+// consumed by this CTA over its lifetime and picks (stage, parity).  Records are
+// REC bytes (32 forward, 48 reverse); a stage holds kChunk records.
 struct Ring {
-  unsigned char* buf;   // kStages * kChunk * 32 bytes
+  unsigned char* buf;   // kStages stages of kChunk * 48 bytes
   uint64_t* full;       // kStages mbarriers
   uint32_t seq;
   uint32_t inflight;    // bitmask of stages with an outstanding copy (thread 0)
 };
 
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+template <int REC>
 __device__ __forceinline__ void ring_issue(Ring& rg, const unsigned char* prog, uint32_t nins, uint32_t chunk,
                                            uint32_t stage) {
   const uint32_t first = chunk * kChunk;
   const uint32_t cnt = min((uint32_t)kChunk, nins - first);
-  const uint32_t bytes = cnt * 32u;
+  const uint32_t bytes = cnt * (uint32_t)REC;
   uint64_t* bar = rg.full + stage;
   mbar_expect_tx(bar, bytes);
-  bulk_g2s(rg.buf + (size_t)stage * kChunk * 32, prog + (size_t)first * 32, bytes, bar);
+  bulk_g2s(rg.buf + (size_t)stage * kChunk * 48, prog + (size_t)first * REC, bytes, bar);
   rg.inflight |= 1u << stage;
-}
-// Orders this CTA's earlier generic-proxy reads of the ring before the next
-// async-proxy (TMA) write into it.
-__device__ __forceinline__ void fence_proxy_async() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 // Drain outstanding copies before a CTA leaves on an error path.
 __device__ __forceinline__ void ring_drain(Ring& rg) {
   if (threadIdx.x != 0) return;
   for (uint32_t k = 0; k < (uint32_t)kStages; ++k) {
-    uint32_t s = (rg.seq + k) % kStages;
+    const uint32_t s = (rg.seq + k) % kStages;
     if (rg.inflight & (1u << s)) {
-      uint32_t parity = ((rg.seq + k) / kStages) & 1u;
+      const uint32_t parity = ((rg.seq + k) / kStages) & 1u;
       (void)mbar_wait_bounded(rg.full + s, parity);
     }
   }
   rg.inflight = 0;
 }
 
-// Runs one program through the ring, calling exec(ins_bytes) for each
+// Runs one program through the ring, calling exec(record) for each
 // instruction.  Returns false if a wait gave up (all threads agree).
-template <class Exec>
+template <int REC, class Exec>
 __device__ __forceinline__ bool run_program(Ring& rg, const unsigned char* prog, uint32_t nins, uint32_t* err,
-                                            Exec&& exec) {
+                                            Exec& exec) {
   const uint32_t nchunks = (nins + kChunk - 1) / kChunk;
   if (nchunks == 0) return true;
   if (threadIdx.x == 0) {
     fence_proxy_async();
     const uint32_t pre = min((uint32_t)kStages, nchunks);
-    for (uint32_t c = 0; c < pre; ++c) ring_issue(rg, prog, nins, c, (rg.seq + c) % kStages);
+    for (uint32_t c = 0; c < pre; ++c) ring_issue<REC>(rg, prog, nins, c, (rg.seq + c) % kStages);
   }
   for (uint32_t c = 0; c < nchunks; ++c) {
     const uint32_t stage = rg.seq % kStages;
@@ -153,9 +158,9 @@ __device__ __forceinline__ bool run_program(Ring& rg, const unsigned char* prog,
     if (ok) {
       if (threadIdx.x == 0) rg.inflight &= ~(1u << stage);
       const uint32_t cnt = min((uint32_t)kChunk, nins - c * kChunk);
-      const unsigned char* base = rg.buf + (size_t)stage * kChunk * 32;
+      const unsigned char* base = rg.buf + (size_t)stage * kChunk * 48;
 #pragma unroll 1
-      for (uint32_t k = 0; k < cnt; ++k) exec(base + k * 32u);
+      for (uint32_t k = 0; k < cnt; ++k) exec(base + k * (uint32_t)REC);
     }
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) atomicOr(err, (uint32_t)KERR_TIMEOUT);
@@ -165,33 +170,68 @@ __device__ __forceinline__ bool run_program(Ring& rg, const unsigned char* prog,
     rg.seq += 1;
     if (threadIdx.x == 0 && c + kStages < nchunks) {
       fence_proxy_async();
-      ring_issue(rg, prog, nins, c + kStages, stage);
+      ring_issue<REC>(rg, prog, nins, c + kStages, stage);
     }
   }
   return true;
 }
 
-// ───────────────────────────── slot file access ─────────────────────────────
-template <class V, int P> struct Slots {
-  V* sm;          // shared registers: sm[reg * tile + col + p]
-  V* gs;          // global scratch:   gs[slot * tile + col + p]
-  uint32_t tile;
-  uint32_t col;
+// ───────────────────────────── column access ────────────────────────────────
+// A thread owns P consecutive points of every slot row, so the P values of one
+// slot are contiguous and move with the widest aligned vector access.
+__host__ __device__ constexpr int gcd_c(int a, int b) { return b == 0 ? a : gcd_c(b, a % b); }
 
-  __device__ __forceinline__ V ld(uint8_t mode, uint32_t idx, int p) const {
-    if (mode == M_SMEM) return sm[(size_t)idx * tile + col + p];
-    return gs[(size_t)idx * tile + col + p];
+template <class V, int P> struct Col {
+  using T = typename dm::VT<V>::S;
+  static constexpr int N = (int)(sizeof(V) * P / sizeof(T));  // scalars per column access
+  static constexpr int B = N * (int)sizeof(T);
+  static __device__ __forceinline__ void ld(const unsigned char* p, V (&v)[P]) {
+    T* t = reinterpret_cast<T*>(v);
+    if constexpr (sizeof(T) == 4 && B % 16 == 0) {
+#pragma unroll
+      for (int i = 0; i < N / 4; ++i) {
+        const float4 q = reinterpret_cast<const float4*>(p)[i];
+        t[4 * i] = q.x; t[4 * i + 1] = q.y; t[4 * i + 2] = q.z; t[4 * i + 3] = q.w;
+      }
+    } else if constexpr (sizeof(T) == 4 && B % 8 == 0) {
+#pragma unroll
+      for (int i = 0; i < N / 2; ++i) {
+        const float2 q = reinterpret_cast<const float2*>(p)[i];
+        t[2 * i] = q.x; t[2 * i + 1] = q.y;
+      }
+    } else if constexpr (sizeof(T) == 8 && B % 16 == 0) {
+#pragma unroll
+      for (int i = 0; i < N / 2; ++i) {
+        const double2 q = reinterpret_cast<const double2*>(p)[i];
+        t[2 * i] = q.x; t[2 * i + 1] = q.y;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < N; ++i) t[i] = reinterpret_cast<const T*>(p)[i];
+    }
   }
-  __device__ __forceinline__ void st(uint8_t mode, uint32_t idx, int p, const V& v) const {
-    if (mode == M_SMEM) sm[(size_t)idx * tile + col + p] = v;
-    else if (mode == M_GLOB) gs[(size_t)idx * tile + col + p] = v;
+  static __device__ __forceinline__ void st(unsigned char* p, const V (&v)[P]) {
+    const T* t = reinterpret_cast<const T*>(v);
+    if constexpr (sizeof(T) == 4 && B % 16 == 0) {
+#pragma unroll
+      for (int i = 0; i < N / 4; ++i)
+        reinterpret_cast<float4*>(p)[i] = make_float4(t[4 * i], t[4 * i + 1], t[4 * i + 2], t[4 * i + 3]);
+    } else if constexpr (sizeof(T) == 4 && B % 8 == 0) {
+#pragma unroll
+      for (int i = 0; i < N / 2; ++i) reinterpret_cast<float2*>(p)[i] = make_float2(t[2 * i], t[2 * i + 1]);
+    } else if constexpr (sizeof(T) == 8 && B % 16 == 0) {
+#pragma unroll
+      for (int i = 0; i < N / 2; ++i) reinterpret_cast<double2*>(p)[i] = make_double2(t[2 * i], t[2 * i + 1]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < N; ++i) reinterpret_cast<T*>(p)[i] = t[i];
+    }
   }
 };
 
 // Per-kind input construction and output handling; the primary template is
 // the plain-value kind (forward, gradient).
 template <class T> struct Lane {
-  using S = T;
   static __device__ __forceinline__ T make_input(const KParams& kp, uint64_t u, uint32_t i, bool valid) {
     if (!valid) return T(0);
     const T* x = (const T*)kp.x;
@@ -202,7 +242,6 @@ template <class T> struct Lane {
   }
 };
 template <class T> struct Lane<dm::Dual<T>> {
-  using S = T;
   static __device__ __forceinline__ dm::Dual<T> make_input(const KParams& kp, uint64_t u, uint32_t i, bool valid) {
     if (!valid) return {T(0), T(0)};
     const T* x = (const T*)kp.x;
@@ -217,11 +256,26 @@ template <class T> struct Lane<dm::Dual<T>> {
   }
 };
 
-// Direction component for STDE units (point = u / S, direction = u % S).
-__device__ __forceinline__ uint32_t philox_bits(uint64_t seed, uint64_t point, uint32_t dir, uint32_t i);
+// Philox-4x32-10 (Salmon et al., SC'11) keyed by `seed`; counter (point, dir, i).
+__device__ __forceinline__ uint32_t philox_bits(uint64_t seed, uint64_t point, uint32_t dir, uint32_t i) {
+  uint32_t c0 = (uint32_t)point, c1 = (uint32_t)(point >> 32), c2 = dir, c3 = i;
+  uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+    const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c0;
+}
 
+// Direction component for Taylor units; STDE units are (point = u / S, dir = u % S).
 template <class T, int K> struct Lane<dm::Jet<T, K>> {
-  using S = T;
   static __device__ __forceinline__ T dir_component(const KParams& kp, uint64_t u, uint32_t i) {
     const T* v = (const T*)kp.v;
     if (kp.S == 0 || kp.dir_mode == 0) return v[u * kp.ni + i];
@@ -253,74 +307,6 @@ template <class T, int K> struct Lane<dm::Jet<T, K>> {
   }
 };
 
-// Philox-4x32-10 (Salmon et al., SC'11) keyed by (seed); counter (point, dir, i).
-__device__ __forceinline__ uint32_t philox_bits(uint64_t seed, uint64_t point, uint32_t dir, uint32_t i) {
-  uint32_t c0 = (uint32_t)point, c1 = (uint32_t)(point >> 32), c2 = dir, c3 = i;
-  uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-#pragma unroll
-  for (int r = 0; r < 10; ++r) {
-    const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
-    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
-    const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
-    const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
-    const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
-    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
-    k0 += 0x9E3779B9u;
-    k1 += 0xBB67AE85u;
-  }
-  return c0;
-}
-
-// ───────────────────────────── forward executor ─────────────────────────────
-template <class V, int P> struct FwdExec {
-  using Kd = typename dm::KindOf<V>::K;
-  const KParams& kp;
-  Slots<V, P> sl;
-  uint64_t unit0;        // unit of point p = unit0 + p
-  V* traj;               // trajectory region of this CTA (gs + G*tile)
-  bool valid[P];
-
-  __device__ __forceinline__ V opnd(uint8_t mode, uint32_t idx, double imm, int p) const {
-    if (mode == M_IMM) return dm::VT<V>::cst(imm);
-    return sl.ld(mode, idx, p);
-  }
-  __device__ __forceinline__ void put(const Ins& in, int p, const V& r) const {
-    sl.st(in.md, in.d, p, r);
-    if (in.save != kNone) traj[(size_t)in.save * sl.tile + sl.col + p] = r;
-  }
-
-  __device__ __forceinline__ void operator()(const unsigned char* raw) const {
-    const Ins in = *reinterpret_cast<const Ins*>(raw);
-    switch (in.opc) {
-      case XI_LDIN:
-#pragma unroll
-        for (int p = 0; p < P; ++p) put(in, p, Lane<V>::make_input(kp, unit0 + p, (uint32_t)in.aux, valid[p]));
-        return;
-      case XI_STOUT:
-#pragma unroll
-        for (int p = 0; p < P; ++p)
-          Lane<V>::store_output(kp, unit0 + p, (uint32_t)in.aux, opnd(in.ma, in.a, in.imm, p), valid[p]);
-        return;
-      case XI_MOV:
-#pragma unroll
-        for (int p = 0; p < P; ++p) put(in, p, opnd(in.ma, in.a, in.imm, p));
-        return;
-      default: break;
-    }
-    V a[P], b[P], r[P];
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-      a[p] = opnd(in.ma, in.a, in.imm, p);
-      b[p] = (in.mb == M_NONE) ? Kd::c(0) : opnd(in.mb, in.b, in.imm, p);
-    }
-#pragma unroll
-    for (int p = 0; p < P; ++p) r[p] = dm::eval_forward<V>(in.opc, a[p], b[p], in.aux);
-#pragma unroll
-    for (int p = 0; p < P; ++p) put(in, p, r[p]);
-  }
-};
-
-// ───────────────────────────── reverse executor ─────────────────────────────
 // Gradient outputs: plain kind -> out2[u][k]; Dual kind -> out2 (re) and out3 (eps).
 template <class V> struct GradOut {
   static __device__ __forceinline__ void store(const KParams& kp, uint64_t u, uint32_t k, const V& g, bool valid) {
@@ -336,85 +322,357 @@ template <class T> struct GradOut<dm::Dual<T>> {
   }
 };
 
-template <class V, int P> struct RevExec {
+// ───────────────────────────── forward executor ─────────────────────────────
+// Instructions are decoded from two 16-byte words straight into registers
+// (DIns layout: opc|ma|mb|md, a, b, d | save, aux, imm).
+template <class V, int P> struct FwdExec {
   using Kd = typename dm::KindOf<V>::K;
+  using C = Col<V, P>;
   const KParams& kp;
-  Slots<V, P> sl;
-  uint64_t unit0;
-  const V* traj;
+  unsigned char* sm;     // this thread's column base in the shared slot file
+  unsigned char* gs;     // ... in the global slots
+  unsigned char* tj;     // ... in the trajectory region
+  uint64_t unit0;        // unit of point p = unit0 + p
   bool valid[P];
 
-  __device__ __forceinline__ V value(uint32_t idx, bool imm, int p) const {
-    if (idx == kNone) return Kd::c(0);
-    if (imm) return dm::VT<V>::cst(kp.pool[idx]);
-    return traj[(size_t)idx * sl.tile + sl.col + p];
+  __device__ __forceinline__ void ld(uint32_t mode, uint32_t off, double imm, V (&v)[P]) const {
+    if (mode == M_SMEM) C::ld(sm + off, v);
+    else if (mode == M_GLOB) C::ld(gs + off, v);
+    else {
+      const V c = dm::VT<V>::cst(imm);
+#pragma unroll
+      for (int p = 0; p < P; ++p) v[p] = c;
+    }
+  }
+  __device__ __forceinline__ void put(uint32_t md, uint32_t d, uint32_t save, const V (&r)[P]) const {
+    if (md == M_SMEM) C::st(sm + d, r);
+    else if (md == M_GLOB) C::st(gs + d, r);
+    if (save != kNone) C::st(tj + save, r);
+  }
+  __device__ __forceinline__ void put_sm(uint32_t d, uint32_t save, const V (&r)[P]) const {
+    C::st(sm + d, r);
+    if (save != kNone) C::st(tj + save, r);
+  }
+
+  __device__ __forceinline__ void ldv(uint32_t mode, uint32_t off, V (&v)[P]) const {
+    C::ld((mode == M_GLOB ? gs : sm) + off, v);
+  }
+
+  // Fused chain s_t = s_{t-1} (+|-) term_t, t = 1..n, s_0 = acc0: the same
+  // Mul / Add / Sub evaluations, in the same operand order, as the tape ops it
+  // replaces.  DFTerm layout: kind|op|xm|ym, x, y, pad | c, pad.
+  __device__ __forceinline__ void chain(uint32_t ma, uint32_t ao, double imm, uint32_t first, uint32_t n,
+                                        V (&acc)[P]) const {
+    ld(ma, ao, imm, acc);
+    const uint4* tp = reinterpret_cast<const uint4*>(kp.fterms + first);
+#pragma unroll 1
+    for (uint32_t q = 0; q < n; ++q) {
+      const uint4 w0 = __ldg(tp + 2 * q);
+      const uint2 w1 = __ldg(reinterpret_cast<const uint2*>(tp + 2 * q + 1));
+      const uint32_t kind = w0.x & 0xFFu, op = (w0.x >> 8) & 0xFFu;
+      V t[P], x[P];
+      if (kind == CK_C) {
+        const V c = dm::VT<V>::cst(__hiloint2double((int)w1.y, (int)w1.x));
+#pragma unroll
+        for (int p = 0; p < P; ++p) t[p] = c;
+      } else {
+        ldv((w0.x >> 16) & 0xFFu, w0.y, kind == CK_X ? t : x);
+        if (kind == CK_CX) {
+          const V c = dm::VT<V>::cst(__hiloint2double((int)w1.y, (int)w1.x));
+#pragma unroll
+          for (int p = 0; p < P; ++p) t[p] = Kd::mul(c, x[p]);
+        } else if (kind == CK_XC) {
+          const V c = dm::VT<V>::cst(__hiloint2double((int)w1.y, (int)w1.x));
+#pragma unroll
+          for (int p = 0; p < P; ++p) t[p] = Kd::mul(x[p], c);
+        } else if (kind == CK_XY) {
+          V y[P];
+          ldv(w0.x >> 24, w0.z, y);
+#pragma unroll
+          for (int p = 0; p < P; ++p) t[p] = Kd::mul(x[p], y[p]);
+        }
+      }
+      switch (op) {
+        case 0:
+#pragma unroll
+          for (int p = 0; p < P; ++p) acc[p] = Kd::add(acc[p], t[p]);
+          break;
+        case 1:
+#pragma unroll
+          for (int p = 0; p < P; ++p) acc[p] = Kd::add(t[p], acc[p]);
+          break;
+        case 2:
+#pragma unroll
+          for (int p = 0; p < P; ++p) acc[p] = Kd::sub(acc[p], t[p]);
+          break;
+        default:
+#pragma unroll
+          for (int p = 0; p < P; ++p) acc[p] = Kd::sub(t[p], acc[p]);
+          break;
+      }
+    }
   }
 
   __device__ __forceinline__ void operator()(const unsigned char* raw) const {
-    const RIns in = *reinterpret_cast<const RIns*>(raw);
-    const uint8_t mr = (in.flags & RF_R_GLOB) ? M_GLOB : M_SMEM;
-    if (in.opc == XI_SEED) {
+    const uint4 w0 = *reinterpret_cast<const uint4*>(raw);
+    const uint4 w1 = *reinterpret_cast<const uint4*>(raw + 16);
+    const uint32_t opc = w0.x & 0xFFu;
+    const uint32_t ao = w0.y, bo = w0.z, dof = w0.w, save = w1.x;
+    const int32_t aux = (int32_t)w1.y;
+    const double imm = __hiloint2double((int)w1.w, (int)w1.z);
+    V a[P], b[P], r[P];
+    switch (opc) {
+      case D_LDIN:
 #pragma unroll
-      for (int p = 0; p < P; ++p) sl.st(mr, in.r, p, Kd::c(1));
-      return;
-    }
-    if (in.opc == XI_STGRAD) {
+        for (int p = 0; p < P; ++p) r[p] = Lane<V>::make_input(kp, unit0 + p, (uint32_t)aux, valid[p]);
+        put(w0.x >> 24, dof, save, r);
+        return;
+      case D_STOUT:
+        ld((w0.x >> 8) & 0xFFu, ao, imm, a);
 #pragma unroll
-      for (int p = 0; p < P; ++p) {
-        const V g = (in.r == kNone) ? Kd::c(0) : sl.ld(mr, in.r, p);
-        GradOut<V>::store(kp, unit0 + p, (uint32_t)in.aux, g, valid[p]);
-      }
-      return;
+        for (int p = 0; p < P; ++p) Lane<V>::store_output(kp, unit0 + p, (uint32_t)aux, a[p], valid[p]);
+        return;
+      case D_MOV:
+        ld((w0.x >> 8) & 0xFFu, ao, imm, a);
+        put(w0.x >> 24, dof, save, a);
+        return;
+      case D_CHAIN:
+        chain((w0.x >> 8) & 0xFFu, ao, imm, bo, (uint32_t)aux, r);
+        put(w0.x >> 24, dof, save, r);
+        return;
+#define ECH_FB(NAME, FN)                                                     \
+  case D_##NAME##_RR:                                                        \
+    C::ld(sm + ao, a);                                                       \
+    C::ld(sm + bo, b);                                                       \
+    _Pragma("unroll") for (int p = 0; p < P; ++p) r[p] = Kd::FN(a[p], b[p]); \
+    put_sm(dof, save, r);                                                    \
+    return;                                                                  \
+  case D_##NAME##_IR: {                                                      \
+    const V c = dm::VT<V>::cst(imm);                                         \
+    C::ld(sm + bo, b);                                                       \
+    _Pragma("unroll") for (int p = 0; p < P; ++p) r[p] = Kd::FN(c, b[p]);    \
+    put_sm(dof, save, r);                                                    \
+    return;                                                                  \
+  }                                                                          \
+  case D_##NAME##_RI: {                                                      \
+    const V c = dm::VT<V>::cst(imm);                                         \
+    C::ld(sm + ao, a);                                                       \
+    _Pragma("unroll") for (int p = 0; p < P; ++p) r[p] = Kd::FN(a[p], c);    \
+    put_sm(dof, save, r);                                                    \
+    return;                                                                  \
+  }
+      ECH_FB(ADD, add)
+      ECH_FB(SUB, sub)
+      ECH_FB(MUL, mul)
+      ECH_FB(DIV, div)
+#undef ECH_FB
+#define ECH_FU(OP)                                                                               \
+  case D_FU_BASE + (OP - OP_NEG):                                                                \
+    C::ld(sm + ao, a);                                                                           \
+    _Pragma("unroll") for (int p = 0; p < P; ++p) r[p] = dm::eval_forward<V>(OP, a[p], a[p], aux); \
+    put_sm(dof, save, r);                                                                        \
+    return;
+      ECH_FU(OP_NEG) ECH_FU(OP_RECIP) ECH_FU(OP_SQRT) ECH_FU(OP_CBRT) ECH_FU(OP_POWI) ECH_FU(OP_EXP)
+      ECH_FU(OP_EXP2) ECH_FU(OP_EXPM1) ECH_FU(OP_LN) ECH_FU(OP_LOG2) ECH_FU(OP_LOG10) ECH_FU(OP_LN1P)
+      ECH_FU(OP_SIN) ECH_FU(OP_COS) ECH_FU(OP_TAN) ECH_FU(OP_ASIN) ECH_FU(OP_ACOS) ECH_FU(OP_ATAN)
+      ECH_FU(OP_SINH) ECH_FU(OP_COSH) ECH_FU(OP_TANH) ECH_FU(OP_ASINH) ECH_FU(OP_ACOSH) ECH_FU(OP_ATANH)
+      ECH_FU(OP_ABS) ECH_FU(OP_SIGNUM) ECH_FU(OP_FLOOR) ECH_FU(OP_CEIL) ECH_FU(OP_ROUND) ECH_FU(OP_TRUNC)
+      ECH_FU(OP_FRACT)
+#undef ECH_FU
+      default:
+        break;
     }
-    V adj[P], da[P], db[P];
-    bool live[P];
+    // generic path: any operand modes
+    const uint32_t mb = (w0.x >> 16) & 0xFFu;
+    ld((w0.x >> 8) & 0xFFu, ao, imm, a);
+    if (mb == M_NONE) {
+#pragma unroll
+      for (int p = 0; p < P; ++p) b[p] = Kd::c(0);
+    } else {
+      ld(mb, bo, imm, b);
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p) r[p] = dm::eval_forward<V>(opc, a[p], b[p], aux);
+    put(w0.x >> 24, dof, save, r);
+  }
+};
+
+// ───────────────────────────── reverse executor ─────────────────────────────
+// DRIns layout: opc|pad|flags, r, a, b | va, vb, vr, aux | imm, pad.
+template <class V, int P> struct RevExec {
+  using Kd = typename dm::KindOf<V>::K;
+  using C = Col<V, P>;
+  const KParams& kp;
+  unsigned char* sm;
+  unsigned char* gs;
+  const unsigned char* tj;
+  uint64_t unit0;
+  bool valid[P];
+
+  __device__ __forceinline__ void value(uint32_t off, bool imm, double c, V (&v)[P]) const {
+    if (imm) {
+      const V k = dm::VT<V>::cst(c);
+#pragma unroll
+      for (int p = 0; p < P; ++p) v[p] = k;
+    } else if (off == kNone) {
+#pragma unroll
+      for (int p = 0; p < P; ++p) v[p] = Kd::c(0);
+    } else {
+      C::ld(tj + off, v);
+    }
+  }
+  __device__ __forceinline__ unsigned char* loc(bool glob, uint32_t off) const { return (glob ? gs : sm) + off; }
+
+  template <bool FAST>
+  __device__ __forceinline__ void accumulate(unsigned char* ptr, bool init, const V (&adj)[P], const V (&d)[P]) const {
+    V cur[P];
+    if (init) {
+#pragma unroll
+      for (int p = 0; p < P; ++p) cur[p] = Kd::c(0);
+    } else {
+      C::ld(ptr, cur);
+    }
 #pragma unroll
     for (int p = 0; p < P; ++p) {
-      adj[p] = sl.ld(mr, in.r, p);
-      live[p] = !Kd::all_zero(adj[p]);
+      const bool hit = !Kd::all_zero(adj[p]) && !Kd::all_zero(d[p]);
+      if (hit) cur[p] = Kd::add(cur[p], Kd::mul(d[p], adj[p]));
     }
+    C::st(ptr, cur);
+  }
+
+  // Adjoint of a single-use intermediate after its only contribution.
+  __device__ __forceinline__ void internal(const V (&adj)[P], const V (&d)[P], V (&out)[P]) const {
 #pragma unroll
     for (int p = 0; p < P; ++p) {
-      const V va = value(in.va, (in.flags & RF_VA_IMM) != 0, p);
-      const V vb = value(in.vb, (in.flags & RF_VB_IMM) != 0, p);
-      const V vr = value(in.vr, false, p);
-      dm::reverse_partials<V>(in.opc, va, vb, vr, in.aux, da[p], db[p]);
+      const bool hit = !Kd::all_zero(adj[p]) && !Kd::all_zero(d[p]);
+      out[p] = hit ? Kd::add(Kd::c(0), Kd::mul(d[p], adj[p])) : Kd::c(0);
     }
-    if (in.flags & RF_HAS_A) {
-      const uint8_t ma = (in.flags & RF_A_GLOB) ? M_GLOB : M_SMEM;
-      const bool init = (in.flags & RF_A_INIT) != 0;
+  }
+
+  // Reverse of a fused chain: for t = n..1 the Add/Sub (its two operands in
+  // operand order), then the absorbed Mul, exactly as the per-op sweep visits
+  // them.  Adjoints of the chain's intermediates stay in registers.
+  // DRTerm layout: kind|op|flags, ax, ay, vx | vy, pad, c.
+  __device__ __forceinline__ void chain(uint32_t flags, uint32_t ro, uint32_t ao, uint32_t first, uint32_t n) const {
+    V adj[P];
+    C::ld(loc(flags & RF_R_GLOB, ro), adj);
+    const uint4* tp = reinterpret_cast<const uint4*>(kp.rterms + first);
+    V one[P], mone[P];
+    {
+      V d0, d1;
+      dm::reverse_partials<V>(OP_SUB, Kd::c(0), Kd::c(0), Kd::c(0), 0, d0, d1);
 #pragma unroll
-      for (int p = 0; p < P; ++p) {
-        const bool hit = live[p] && !Kd::all_zero(da[p]);
-        if (init) {
-          const V z = Kd::c(0);
-          sl.st(ma, in.a, p, hit ? Kd::add(z, Kd::mul(da[p], adj[p])) : z);
-        } else if (hit) {
-          sl.st(ma, in.a, p, Kd::add(sl.ld(ma, in.a, p), Kd::mul(da[p], adj[p])));
+      for (int p = 0; p < P; ++p) { one[p] = d0; mone[p] = d1; }
+    }
+#pragma unroll 1
+    for (uint32_t q = n; q-- > 0;) {
+      const uint4 w0 = __ldg(tp + 2 * q);
+      const uint4 w1 = __ldg(tp + 2 * q + 1);
+      const uint32_t kind = w0.x & 0xFFu, op = (w0.x >> 8) & 0xFFu, tf = w0.x >> 16;
+      const bool chain_a = (op & 1u) == 0;
+      // partials of the Add / Sub: acc side and term side
+      const V (&dacc)[P] = (op == 3) ? mone : one;
+      const V (&dterm)[P] = (op == 2) ? mone : one;
+      V nadj[P], tadj[P];
+      auto acc_side = [&]() {
+        if (q == 0) {
+          if (flags & RF_HAS_A) accumulate<false>(loc(flags & RF_A_GLOB, ao), (flags & RF_A_INIT) != 0, adj, dacc);
+        } else {
+          internal(adj, dacc, nadj);
         }
+      };
+      auto term_side = [&]() {
+        if (kind == CK_X) accumulate<false>(loc(tf & CF_X_GLOB, w0.y), (tf & CF_X_INIT) != 0, adj, dterm);
+        else if (kind != CK_C) internal(adj, dterm, tadj);
+      };
+      if (chain_a) { acc_side(); term_side(); } else { term_side(); acc_side(); }
+      if (kind == CK_CX || kind == CK_XC) {
+        V c[P];
+        const V cv = dm::VT<V>::cst(__hiloint2double((int)w1.w, (int)w1.z));
+#pragma unroll
+        for (int p = 0; p < P; ++p) c[p] = cv;
+        accumulate<false>(loc(tf & CF_X_GLOB, w0.y), (tf & CF_X_INIT) != 0, tadj, c);
+      } else if (kind == CK_XY) {
+        V xv[P], yv[P];
+        value(w0.w, false, 0.0, xv);
+        value(w1.x, false, 0.0, yv);
+        accumulate<false>(loc(tf & CF_X_GLOB, w0.y), (tf & CF_X_INIT) != 0, tadj, yv);
+        accumulate<false>(loc(tf & CF_Y_GLOB, w0.z), (tf & CF_Y_INIT) != 0, tadj, xv);
       }
-    }
-    if (in.flags & RF_HAS_B) {
-      const uint8_t mb = (in.flags & RF_B_GLOB) ? M_GLOB : M_SMEM;
-      const bool init = (in.flags & RF_B_INIT) != 0;
+      if (q > 0) {
 #pragma unroll
-      for (int p = 0; p < P; ++p) {
-        const bool hit = live[p] && !Kd::all_zero(db[p]);
-        if (init) {
-          const V z = Kd::c(0);
-          sl.st(mb, in.b, p, hit ? Kd::add(z, Kd::mul(db[p], adj[p])) : z);
-        } else if (hit) {
-          sl.st(mb, in.b, p, Kd::add(sl.ld(mb, in.b, p), Kd::mul(db[p], adj[p])));
-        }
+        for (int p = 0; p < P; ++p) adj[p] = nadj[p];
       }
     }
   }
 
+  // One reverse op: adj(a) += da * adj(r), adj(b) += db * adj(r) with the
+  // zero-adjoint skip and the zero-multiplier guard.  FAST: every adjoint
+  // location is in shared memory.
+  template <bool FAST>
+  __device__ __forceinline__ void body(uint32_t opc, uint32_t flags, uint32_t ro, uint32_t ao, uint32_t bo,
+                                       uint32_t vao, uint32_t vbo, uint32_t vro, int32_t aux, double imm) const {
+    V adj[P], va[P], vb[P], vr[P], da[P], db[P];
+    C::ld(FAST ? sm + ro : loc(flags & RF_R_GLOB, ro), adj);
+    value(vao, (flags & RF_VA_IMM) != 0, imm, va);
+    value(vbo, (flags & RF_VB_IMM) != 0, imm, vb);
+    value(vro, false, 0.0, vr);
+#pragma unroll
+    for (int p = 0; p < P; ++p) dm::reverse_partials<V>(opc, va[p], vb[p], vr[p], aux, da[p], db[p]);
+    if (flags & RF_HAS_A)
+      accumulate<FAST>(FAST ? sm + ao : loc(flags & RF_A_GLOB, ao), (flags & RF_A_INIT) != 0, adj, da);
+    if (flags & RF_HAS_B)
+      accumulate<FAST>(FAST ? sm + bo : loc(flags & RF_B_GLOB, bo), (flags & RF_B_INIT) != 0, adj, db);
+  }
+
+  __device__ __forceinline__ void operator()(const unsigned char* raw) const {
+    const uint4 w0 = *reinterpret_cast<const uint4*>(raw);
+    const uint4 w1 = *reinterpret_cast<const uint4*>(raw + 16);
+    const uint2 w2 = *reinterpret_cast<const uint2*>(raw + 32);
+    const uint32_t opc = w0.x & 0xFFu;
+    const uint32_t flags = w0.x >> 16;
+    const uint32_t ro = w0.y, ao = w0.z, bo = w0.w;
+    const int32_t aux = (int32_t)w1.w;
+    const double imm = __hiloint2double((int)w2.y, (int)w2.x);
+    switch (opc) {
+      case D_SEED: {
+        V one[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) one[p] = Kd::c(1);
+        C::st(loc(flags & RF_R_GLOB, ro), one);
+        return;
+      }
+      case D_CHAIN:
+        chain(flags, ro, ao, w1.x, (uint32_t)aux);
+        return;
+      case D_STGRAD: {
+        V g[P];
+        if (ro == kNone) {
+#pragma unroll
+          for (int p = 0; p < P; ++p) g[p] = Kd::c(0);
+        } else {
+          C::ld(loc(flags & RF_R_GLOB, ro), g);
+        }
+#pragma unroll
+        for (int p = 0; p < P; ++p) GradOut<V>::store(kp, unit0 + p, (uint32_t)aux, g[p], valid[p]);
+        return;
+      }
+#define ECH_RF(OP) \
+  case D_RF_BASE + OP: body<true>(OP, flags, ro, ao, bo, w1.x, w1.y, w1.z, aux, imm); return;
+      ECH_RF(OP_ADD) ECH_RF(OP_SUB) ECH_RF(OP_MUL) ECH_RF(OP_DIV) ECH_RF(OP_REM) ECH_RF(OP_POWF)
+      ECH_RF(OP_ATAN2) ECH_RF(OP_HYPOT) ECH_RF(OP_MAX) ECH_RF(OP_MIN) ECH_RF(OP_NEG) ECH_RF(OP_RECIP)
+      ECH_RF(OP_SQRT) ECH_RF(OP_CBRT) ECH_RF(OP_POWI) ECH_RF(OP_EXP) ECH_RF(OP_EXP2) ECH_RF(OP_EXPM1)
+      ECH_RF(OP_LN) ECH_RF(OP_LOG2) ECH_RF(OP_LOG10) ECH_RF(OP_LN1P) ECH_RF(OP_SIN) ECH_RF(OP_COS)
+      ECH_RF(OP_TAN) ECH_RF(OP_ASIN) ECH_RF(OP_ACOS) ECH_RF(OP_ATAN) ECH_RF(OP_SINH) ECH_RF(OP_COSH)
+      ECH_RF(OP_TANH) ECH_RF(OP_ASINH) ECH_RF(OP_ACOSH) ECH_RF(OP_ATANH) ECH_RF(OP_ABS) ECH_RF(OP_SIGNUM)
+      ECH_RF(OP_FLOOR) ECH_RF(OP_CEIL) ECH_RF(OP_ROUND) ECH_RF(OP_TRUNC) ECH_RF(OP_FRACT)
+#undef ECH_RF
+      default:
+        body<false>(opc, flags, ro, ao, bo, w1.x, w1.y, w1.z, aux, imm);
+        return;
+    }
+  }
 };
-
-}  // namespace ech
-
-namespace ech {
 
 // ───────────────────────────── the sweep kernel ─────────────────────────────
 // REV = false: forward program only (forward values, JVP, Taylor jets).
@@ -430,23 +688,24 @@ __global__ void __launch_bounds__(256) sweep_kernel(KParams kp) {
   }
   __syncthreads();
   Ring rg{smem_dyn, full, 0u, 0u};
-  V* regs = reinterpret_cast<V*>(smem_dyn + (size_t)kStages * kChunk * 32);
   const uint32_t tile = kp.tile;
-  const uint32_t col = threadIdx.x * P;
-  V* gs = reinterpret_cast<V*>(reinterpret_cast<unsigned char*>(kp.scratch) + blockIdx.x * kp.scratch_stride_bytes);
-  V* traj = gs + (size_t)kp.far_slots * tile;
+  const size_t colb = (size_t)threadIdx.x * P * sizeof(V);
+  unsigned char* sm = smem_dyn + kRingBytes + colb;
+  unsigned char* gbase = reinterpret_cast<unsigned char*>(kp.scratch) + blockIdx.x * kp.scratch_stride_bytes;
+  unsigned char* gs = gbase + colb;
+  unsigned char* tj = gbase + (size_t)kp.far_slots * tile * sizeof(V) + colb;
   const uint64_t ntiles = (kp.n_units + tile - 1) / tile;
   for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const uint64_t unit0 = t * tile + col;
-    FwdExec<V, P> fx{kp, Slots<V, P>{regs, gs, tile, col}, unit0, traj, {}};
+    const uint64_t unit0 = t * tile + (uint64_t)threadIdx.x * P;
+    FwdExec<V, P> fx{kp, sm, gs, tj, unit0, {}};
 #pragma unroll
     for (int p = 0; p < P; ++p) fx.valid[p] = unit0 + p < kp.n_units;
-    if (!run_program(rg, reinterpret_cast<const unsigned char*>(kp.fwd), kp.n_fwd, kp.err, fx)) return;
+    if (!run_program<32>(rg, reinterpret_cast<const unsigned char*>(kp.fwd), kp.n_fwd, kp.err, fx)) return;
     if (REV) {
-      RevExec<V, P> rx{kp, Slots<V, P>{regs, gs, tile, col}, unit0, traj, {}};
+      RevExec<V, P> rx{kp, sm, gs, tj, unit0, {}};
 #pragma unroll
       for (int p = 0; p < P; ++p) rx.valid[p] = fx.valid[p];
-      if (!run_program(rg, reinterpret_cast<const unsigned char*>(kp.rev), kp.n_rev, kp.err, rx)) return;
+      if (!run_program<48>(rg, reinterpret_cast<const unsigned char*>(kp.rev), kp.n_rev, kp.err, rx)) return;
     }
   }
 }

@@ -24,12 +24,14 @@ cudaError_t launch_by_p(const LaunchReq& r, const KParams& kp, int grid, int blo
     switch (r.P) {
       case 1: return launch_one<V, 1, true>(kp, grid, block, smem, st, bps);
       case 2: return launch_one<V, 2, true>(kp, grid, block, smem, st, bps);
+      case 4: return launch_one<V, 4, true>(kp, grid, block, smem, st, bps);
       default: return cudaErrorInvalidValue;
     }
   }
   switch (r.P) {
     case 1: return launch_one<V, 1, false>(kp, grid, block, smem, st, bps);
     case 2: return launch_one<V, 2, false>(kp, grid, block, smem, st, bps);
+    case 4: return launch_one<V, 4, false>(kp, grid, block, smem, st, bps);
     default: return cudaErrorInvalidValue;
   }
 }

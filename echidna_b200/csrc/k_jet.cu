@@ -1,22 +1,22 @@
-// Sweep kernels on Taylor jets, orders 1..5 (forward only).
-#include "k_common.cuh"
+// Dispatch over the per-order Taylor-jet kernel units (k_jet1.cu .. k_jet5.cu).
+#include "launch.h"
 
 namespace ech {
-template <class T>
-static cudaError_t jet_by_k(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
-                            int* bps) {
-  if (r.rev) return cudaErrorInvalidValue;
-  switch (r.K) {
-    case 1: return launch_by_p<dm::Jet<T, 1>>(r, kp, grid, block, smem, st, bps);
-    case 2: return launch_by_p<dm::Jet<T, 2>>(r, kp, grid, block, smem, st, bps);
-    case 3: return launch_by_p<dm::Jet<T, 3>>(r, kp, grid, block, smem, st, bps);
-    case 4: return launch_by_p<dm::Jet<T, 4>>(r, kp, grid, block, smem, st, bps);
-    case 5: return launch_by_p<dm::Jet<T, 5>>(r, kp, grid, block, smem, st, bps);
-    default: return cudaErrorInvalidValue;
-  }
-}
+cudaError_t launch_jet1(const LaunchReq&, const KParams&, int, int, size_t, cudaStream_t, int*);
+cudaError_t launch_jet2(const LaunchReq&, const KParams&, int, int, size_t, cudaStream_t, int*);
+cudaError_t launch_jet3(const LaunchReq&, const KParams&, int, int, size_t, cudaStream_t, int*);
+cudaError_t launch_jet4(const LaunchReq&, const KParams&, int, int, size_t, cudaStream_t, int*);
+cudaError_t launch_jet5(const LaunchReq&, const KParams&, int, int, size_t, cudaStream_t, int*);
+
 cudaError_t launch_jet(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
                        int* bps) {
-  return r.f64 ? jet_by_k<double>(r, kp, grid, block, smem, st, bps) : jet_by_k<float>(r, kp, grid, block, smem, st, bps);
+  switch (r.K) {
+    case 1: return launch_jet1(r, kp, grid, block, smem, st, bps);
+    case 2: return launch_jet2(r, kp, grid, block, smem, st, bps);
+    case 3: return launch_jet3(r, kp, grid, block, smem, st, bps);
+    case 4: return launch_jet4(r, kp, grid, block, smem, st, bps);
+    case 5: return launch_jet5(r, kp, grid, block, smem, st, bps);
+    default: return cudaErrorInvalidValue;
+  }
 }
 }  // namespace ech

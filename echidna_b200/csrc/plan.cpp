@@ -323,6 +323,118 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
   pl.traj_slots = ntraj;
   pl.stats.traj_values = ntraj;
 
+  // ---------------- fused linear chains ----------------
+  // A chain is a run of consecutive live ops (no other live op in between)
+  //   s_1 = acc0 (+|-) term_1, s_t = s_{t-1} (+|-) term_t, ...
+  // where every s_t (t < K) and every absorbed Mul term has exactly one use.
+  // Consecutive ops keep the reverse accumulation order identical to the
+  // per-op sweep, and no operand outlives the run, so register pressure is
+  // unchanged.
+  std::vector<uint32_t> uses(nv, 0);
+  for (uint32_t i = ni; i < nv; ++i) {
+    if (!live[i] || is_const(i)) continue;
+    uses[t.a0[i]]++;
+    if (has_b(i)) uses[t.a1[i]]++;
+  }
+  if (emit_outputs)
+    for (uint32_t o : t.outs) uses[o]++;
+  if (reverse) uses[seed]++;
+  struct Chain {
+    uint32_t first, last;        // tape index range of the absorbed ops
+    int64_t acc0;                // slot, or -1 for a constant
+    double acc0_val;
+    uint32_t tb, tn;             // term range in pl.terms
+  };
+  std::vector<Chain> chains;
+  std::vector<int32_t> chain_end(nv, -1);  // at s_K: chain id
+  std::vector<uint8_t> absorbed(nv, 0);
+  {
+    std::vector<uint32_t> L;
+    for (uint32_t i = ni; i < nv; ++i)
+      if (live[i] && !is_const(i)) L.push_back(i);
+    auto is_addsub = [&](uint32_t i) { return t.op[i] == OP_ADD || t.op[i] == OP_SUB; };
+    size_t k = 0;
+    while (k < L.size()) {
+      size_t j = k;
+      int64_t prev = -1;
+      std::vector<PTerm> tl;
+      int64_t acc0 = -1;
+      double acc0_val = 0.0;
+      uint32_t nops = 0;
+      while (j < L.size()) {
+        int64_t mul = -1;
+        uint32_t as;
+        if (j + 1 < L.size() && t.op[L[j]] == OP_MUL && is_addsub(L[j + 1]) && uses[L[j]] == 1 &&
+            (t.a0[L[j + 1]] == L[j]) != (t.a1[L[j + 1]] == L[j]) &&
+            !(is_const(t.a0[L[j]]) && is_const(t.a1[L[j]]))) {
+          mul = L[j];
+          as = L[j + 1];
+        } else if (is_addsub(L[j])) {
+          as = L[j];
+        } else {
+          break;
+        }
+        const uint32_t o0 = t.a0[as], o1 = t.a1[as];
+        bool chain_is_a;
+        if (prev < 0) {
+          if (mul >= 0) chain_is_a = (o1 == (uint32_t)mul);
+          else chain_is_a = true;
+        } else {
+          const bool pa = (o0 == (uint32_t)prev), pb = (o1 == (uint32_t)prev);
+          if (pa == pb || uses[prev] != 1) break;  // must consume prev exactly once
+          chain_is_a = pa;
+          if (mul >= 0 && (chain_is_a ? o1 : o0) != (uint32_t)mul) break;
+        }
+        const uint32_t term_slot = chain_is_a ? o1 : o0;
+        const uint32_t acc_slot = chain_is_a ? o0 : o1;
+        PTerm pt{};
+        pt.xs = pt.ys = kNone;
+        pt.vx = pt.vy = kNone;
+        const bool sub = t.op[as] == OP_SUB;
+        pt.op = (uint8_t)((sub ? 2 : 0) + (chain_is_a ? 0 : 1));
+        if (mul >= 0) {
+          const uint32_t ma = t.a0[mul], mb = t.a1[mul];
+          if (is_const(ma)) { pt.kind = CK_CX; pt.c = t.vals[ma]; pt.xs = mb; }
+          else if (is_const(mb)) { pt.kind = CK_XC; pt.c = t.vals[mb]; pt.xs = ma; }
+          else { pt.kind = CK_XY; pt.xs = ma; pt.ys = mb; }
+        } else if (is_const(term_slot)) {
+          pt.kind = CK_C;
+          pt.c = t.vals[term_slot];
+        } else {
+          pt.kind = CK_X;
+          pt.xs = term_slot;
+        }
+        if (prev < 0) {
+          if (is_const(acc_slot)) { acc0 = -1; acc0_val = t.vals[acc_slot]; }
+          else acc0 = acc_slot;
+        }
+        tl.push_back(pt);
+        nops += (mul >= 0) ? 2u : 1u;
+        prev = as;
+        j += (mul >= 0) ? 2 : 1;
+        if (uses[as] != 1) break;
+      }
+      if (nops >= 2 && !tl.empty()) {
+        Chain ch;
+        ch.first = L[k];
+        ch.last = (uint32_t)prev;
+        ch.acc0 = acc0;
+        ch.acc0_val = acc0_val;
+        ch.tb = (uint32_t)pl.terms.size();
+        ch.tn = (uint32_t)tl.size();
+        for (size_t q = k; q < j; ++q) absorbed[L[q]] = 1;
+        chain_end[ch.last] = (int32_t)chains.size();
+        chains.push_back(ch);
+        pl.terms.insert(pl.terms.end(), tl.begin(), tl.end());
+        pl.stats.chains++;
+        pl.stats.chain_ops += nops;
+        k = j;
+      } else {
+        k += 1;
+      }
+    }
+  }
+
   // ---------------- forward program (symbolic) ----------------
   struct FSym {
     uint8_t opc;
@@ -332,12 +444,12 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
     bool a_imm, b_imm;
     double a_val, b_val;
     uint32_t save;
+    int32_t chain;   // chain id for XI_CHAIN
   };
   std::vector<FSym> fs;
   fs.reserve(nv + t.outs.size());
   std::vector<int64_t> def_pos(nv, -1), last_pos(nv, -1);
   auto use = [&](uint32_t s, int64_t pos) { last_pos[s] = std::max(last_pos[s], pos); };
-  std::vector<std::vector<uint32_t>> outs_of;  // output ids per slot (sparse)
   std::vector<std::pair<uint32_t, uint32_t>> out_pairs;  // (slot, j)
   if (emit_outputs)
     for (uint32_t j = 0; j < (uint32_t)t.outs.size(); ++j) out_pairs.push_back({t.outs[j], j});
@@ -353,6 +465,7 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
       f.d = -1;
       f.b = -1;
       f.save = kNone;
+      f.chain = -1;
       if (is_const(s)) {
         f.a = -1; f.a_imm = true; f.a_val = t.vals[s];
       } else {
@@ -368,7 +481,7 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
     if (!is_const(pr.first)) continue;
     FSym f{};
     f.opc = XI_STOUT; f.aux = (int32_t)pr.second; f.d = -1; f.a = -1; f.b = -1;
-    f.a_imm = true; f.a_val = t.vals[pr.first]; f.save = kNone;
+    f.a_imm = true; f.a_val = t.vals[pr.first]; f.save = kNone; f.chain = -1;
     fs.push_back(f);
   }
   int64_t tmp_vreg = nv;  // extra vregs for materialised constants
@@ -380,7 +493,27 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
     f.d = i;
     f.save = traj[i];
     f.b = -1;
-    if (o == OP_INPUT) {
+    f.chain = -1;
+    if (absorbed[i] && chain_end[i] < 0) continue;  // inside a fused chain
+    if (chain_end[i] >= 0) {
+      const Chain& ch = chains[chain_end[i]];
+      const int64_t pos = (int64_t)fs.size();
+      f.opc = XI_CHAIN;
+      f.chain = chain_end[i];
+      f.aux = (int32_t)ch.tn;
+      if (ch.acc0 >= 0) { f.a = ch.acc0; f.a_imm = false; use((uint32_t)ch.acc0, pos); }
+      else { f.a = -1; f.a_imm = true; f.a_val = ch.acc0_val; }
+      for (uint32_t q = 0; q < ch.tn; ++q) {
+        const PTerm& pt = pl.terms[ch.tb + q];
+        if (pt.xs != kNone) use(pt.xs, pos);
+        if (pt.ys != kNone) use(pt.ys, pos);
+      }
+      for (uint32_t q = ch.first; q <= ch.last; ++q) {
+        if (!absorbed[q]) continue;
+        op_cost(t.op[q], pl.stats.flops_fwd, pl.stats.specials_fwd);
+        pl.stats.fwd_ops++;
+      }
+    } else if (o == OP_INPUT) {
       f.opc = XI_LDIN; f.aux = (int32_t)i; f.a = -1;
     } else {
       f.opc = (uint8_t)o;
@@ -393,6 +526,7 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
         // both operands constant (hand-built tapes): materialise a into a temp
         FSym m{};
         m.opc = XI_MOV; m.d = tmp_vreg; m.a = -1; m.b = -1; m.a_imm = true; m.a_val = t.vals[sa]; m.save = kNone;
+        m.chain = -1;
         const int64_t p = (int64_t)fs.size();
         fs.push_back(m);
         tmp_iv.push_back({p, p + 1});
@@ -436,10 +570,22 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
     if (f.a >= 0) { in.ma = lsf.loc[f.a].mode; in.a = lsf.loc[f.a].idx; }
     else if (f.a_imm) { in.ma = M_IMM; in.a = 0; in.imm = f.a_val; }
     else { in.ma = M_NONE; in.a = kNone; }
-    if (f.b >= 0) { in.mb = lsf.loc[f.b].mode; in.b = lsf.loc[f.b].idx; }
+    if (f.opc == XI_CHAIN) {
+      in.mb = M_NONE;
+      in.b = chains[f.chain].tb;  // first term
+    } else if (f.b >= 0) { in.mb = lsf.loc[f.b].mode; in.b = lsf.loc[f.b].idx; }
     else if (f.b_imm) { in.mb = M_IMM; in.b = 0; in.imm = f.b_val; }
     else { in.mb = M_NONE; in.b = kNone; }
     pl.fwd.push_back(in);
+  }
+  for (PTerm& pt : pl.terms) {
+    pt.fxm = pt.fym = M_NONE;
+    pt.fxi = pt.fyi = kNone;
+    if (pt.xs != kNone) { pt.fxm = lsf.loc[pt.xs].mode; pt.fxi = lsf.loc[pt.xs].idx; }
+    if (pt.ys != kNone) { pt.fym = lsf.loc[pt.ys].mode; pt.fyi = lsf.loc[pt.ys].idx; }
+    pt.rxm = pt.rym = M_NONE;
+    pt.rxi = pt.ryi = kNone;
+    if (pt.kind == CK_XY) { pt.vx = traj[pt.xs]; pt.vy = traj[pt.ys]; }
   }
   uint32_t smem_used = lsf.smem_used, glob_used = lsf.glob_used;
 
@@ -451,6 +597,7 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
       uint16_t flags;
       int64_t r, a, b;   // adjoint vregs (slot ids), -1 none
       uint32_t va, vb, vr;
+      int32_t chain;
     };
     std::vector<RSym> rs;
     std::vector<int64_t> birth(nv, -1), death(nv, -1);
@@ -465,27 +612,32 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
         if (sb < ni && min_cons[sb] < 0) min_cons[sb] = i;
       }
     }
-    std::vector<std::vector<uint32_t>> grads_after;  // by op -> inputs whose gradient completes there
-    // zero gradients for inputs without reachable consumers
+    auto mk = [](uint8_t opc) {
+      RSym r{};
+      r.opc = opc;
+      r.r = r.a = r.b = -1;
+      r.va = r.vb = r.vr = kNone;
+      r.chain = -1;
+      return r;
+    };
     const bool seed_const = is_const(seed);
     for (uint32_t k = 0; k < ni; ++k) {
       const bool seeded = (!seed_const && k == seed);
       if (min_cons[k] < 0 && !seeded) {
-        RSym g{};
-        g.opc = XI_STGRAD; g.aux = (int32_t)k; g.r = -1; g.a = -1; g.b = -1;
-        g.va = g.vb = g.vr = kNone;
+        RSym g = mk(XI_STGRAD);
+        g.aux = (int32_t)k;
         rs.push_back(g);
       }
     }
     if (!seed_const) {
-      RSym sd{};
-      sd.opc = XI_SEED; sd.r = seed; sd.a = -1; sd.b = -1; sd.va = sd.vb = sd.vr = kNone;
+      RSym sd = mk(XI_SEED);
+      sd.r = seed;
       birth[seed] = (int64_t)rs.size();
       rs.push_back(sd);
       if (seed < ni && min_cons[seed] < 0) {
-        RSym g{};
-        g.opc = XI_STGRAD; g.aux = (int32_t)seed; g.r = seed; g.a = -1; g.b = -1;
-        g.va = g.vb = g.vr = kNone;
+        RSym g = mk(XI_STGRAD);
+        g.aux = (int32_t)seed;
+        g.r = seed;
         death[seed] = (int64_t)rs.size();
         rs.push_back(g);
       }
@@ -500,9 +652,82 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
         imm = false;
       }
     };
+    // inputs whose gradient completes once tape ops [lo, hi] have been processed
+    auto emit_grads = [&](uint32_t lo, uint32_t hi) {
+      for (uint32_t q = hi + 1; q-- > lo;) {
+        if (!reach[q] || is_const(q)) continue;
+        const uint32_t ops2[2] = {t.a0[q], has_b(q) ? t.a1[q] : kUnused};
+        for (int w = 0; w < 2; ++w) {
+          const uint32_t s2 = ops2[w];
+          if (s2 == kUnused || s2 >= ni) continue;
+          if (w == 1 && s2 == ops2[0]) continue;
+          if (min_cons[s2] == (int64_t)q && death[s2] < 0) {
+            RSym g = mk(XI_STGRAD);
+            g.aux = (int32_t)s2;
+            g.r = s2;
+            death[s2] = (int64_t)rs.size();
+            rs.push_back(g);
+          }
+        }
+      }
+    };
     for (int64_t ii = (int64_t)nv - 1; ii >= (int64_t)ni && !seed_const; --ii) {
       const uint32_t i = (uint32_t)ii;
       if (!reach[i] || is_const(i)) continue;
+      if (chain_end[i] >= 0) {
+        const Chain& ch = chains[chain_end[i]];
+        const int64_t pos = (int64_t)rs.size();
+        if (birth[i] >= 0) death[i] = pos;
+        RSym r = mk(XI_CHAIN);
+        r.chain = chain_end[i];
+        r.r = i;
+        r.aux = (int32_t)ch.tn;
+        r.va = ch.tb;
+        uint16_t fl = 0;
+        // contributions in the per-op reverse order: for t = K..1 the Add/Sub
+        // (operand a, then b), then the absorbed Mul (a, then b)
+        auto touch = [&](uint32_t s2) -> bool {  // returns "first contribution"
+          if (birth[s2] < 0) { birth[s2] = pos; return true; }
+          return false;
+        };
+        for (uint32_t q = ch.tn; q-- > 0;) {
+          PTerm& pt = pl.terms[ch.tb + q];
+          const bool chain_a = (pt.op & 1) == 0;
+          auto acc_side = [&]() {
+            if (q == 0 && ch.acc0 >= 0) {
+              fl |= RF_HAS_A;
+              if (touch((uint32_t)ch.acc0)) fl |= RF_A_INIT;
+            }
+          };
+          auto term_side = [&]() {
+            if (pt.kind == CK_X) {
+              pt.flags |= CF_X_ADJ;
+              if (touch(pt.xs)) pt.flags |= CF_X_INIT;
+            }
+          };
+          if (chain_a) { acc_side(); term_side(); } else { term_side(); acc_side(); }
+          if (pt.kind == CK_CX || pt.kind == CK_XC) {
+            pt.flags |= CF_X_ADJ;
+            if (touch(pt.xs)) pt.flags |= CF_X_INIT;
+          } else if (pt.kind == CK_XY) {
+            pt.flags |= CF_X_ADJ | CF_Y_ADJ;
+            if (touch(pt.xs)) pt.flags |= CF_X_INIT;
+            if (touch(pt.ys)) pt.flags |= CF_Y_INIT;
+          }
+        }
+        if (fl & RF_HAS_A) r.a = ch.acc0;
+        r.flags = fl;
+        rs.push_back(r);
+        for (uint32_t q = ch.first; q <= ch.last; ++q) {
+          if (!absorbed[q]) continue;
+          op_cost(t.op[q], pl.stats.flops_rev, pl.stats.specials_rev);
+          pl.stats.flops_rev += (t.op[q] == OP_MUL) ? 2 : 2;
+          pl.stats.rev_ops++;
+        }
+        emit_grads(ch.first, ch.last);
+        ii = (int64_t)ch.first;  // loop decrement continues below the chain
+        continue;
+      }
       const uint32_t o = t.op[i];
       const uint32_t sa = t.a0[i];
       const bool bin = has_b(i);
@@ -512,13 +737,11 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
       const int64_t pos = (int64_t)rs.size();
       if (birth[i] >= 0) death[i] = pos;  // adj(i) read here
       if (!needA && !needB) continue;
-      RSym r{};
-      r.opc = (uint8_t)o;
+      RSym r = mk((uint8_t)o);
       r.aux = (o == OP_POWI) ? (int32_t)t.a1[i] : 0;
       r.r = i;
       r.a = needA ? (int64_t)sa : -1;
       r.b = needB ? (int64_t)sb : -1;
-      r.va = r.vb = r.vr = kNone;
       uint16_t fl = 0;
       if (needA) fl |= RF_HAS_A;
       if (needB) fl |= RF_HAS_B;
@@ -534,18 +757,7 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
       op_cost(o, pl.stats.flops_rev, pl.stats.specials_rev);
       pl.stats.flops_rev += 2 * ((needA ? 1 : 0) + (needB ? 1 : 0));
       pl.stats.rev_ops++;
-      // gradients that complete at this op
-      for (int which = 0; which < 2; ++which) {
-        const uint32_t s = which == 0 ? sa : sb;
-        if ((which == 0 && !needA) || (which == 1 && !needB)) continue;
-        if (which == 1 && sb == sa) continue;
-        if (s < ni && min_cons[s] == (int64_t)i) {
-          RSym g{};
-          g.opc = XI_STGRAD; g.aux = (int32_t)s; g.r = s; g.a = -1; g.b = -1; g.va = g.vb = g.vr = kNone;
-          death[s] = (int64_t)rs.size();
-          rs.push_back(g);
-        }
-      }
+      emit_grads(i, i);
     }
     // Every reachable op other than the seed has a reachable consumer, so its
     // adjoint is born (first contribution, RF_*_INIT) before it is read.
@@ -587,6 +799,19 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
       in.flags = fl;
       pl.rev.push_back(in);
     }
+    for (const Chain& ch : chains) {
+      for (uint32_t q = 0; q < ch.tn; ++q) {
+        PTerm& pt = pl.terms[ch.tb + q];
+        if (pt.flags & CF_X_ADJ) {
+          pt.rxm = lsr.loc[pt.xs].mode;
+          pt.rxi = lsr.loc[pt.xs].idx;
+        }
+        if (pt.flags & CF_Y_ADJ) {
+          pt.rym = lsr.loc[pt.ys].mode;
+          pt.ryi = lsr.loc[pt.ys].idx;
+        }
+      }
+    }
     smem_used = std::max(smem_used, lsr.smem_used);
     glob_used = std::max(glob_used, lsr.glob_used);
   }
@@ -594,6 +819,129 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
   pl.far_slots = glob_used;
   if (pl.pool.empty()) pl.pool.push_back(0.0);
   return pl;
+}
+
+bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out, std::string& err) {
+  const uint64_t row = (uint64_t)tile * vbytes;
+  bool ok = true;
+  auto off = [&](uint32_t idx) -> uint32_t {
+    if (idx == kNone) return kNone;
+    const uint64_t o = (uint64_t)idx * row;
+    if (o >= 0xFFFFFFFFull) {
+      ok = false;
+      return 0;
+    }
+    return (uint32_t)o;
+  };
+  out.fwd.clear();
+  out.rev.clear();
+  out.fwd.reserve(p.fwd.size());
+  for (const Ins& in : p.fwd) {
+    DIns d{};
+    d.ma = in.ma;
+    d.mb = in.mb;
+    d.md = in.md;
+    d.a = (in.ma == M_SMEM || in.ma == M_GLOB) ? off(in.a) : 0u;
+    d.b = (in.mb == M_SMEM || in.mb == M_GLOB) ? off(in.b) : 0u;
+    d.d = (in.md == M_SMEM || in.md == M_GLOB) ? off(in.d) : 0u;
+    d.save = off(in.save);
+    d.aux = in.aux;
+    d.imm = in.imm;
+    uint8_t opc = in.opc;
+    const bool dsm = in.md == M_SMEM;
+    if (opc == XI_CHAIN) {
+      d.b = in.b;  // first term (index into the term tables)
+      d.mb = M_NONE;
+      d.opc = D_CHAIN;
+      out.fwd.push_back(d);
+      continue;
+    }
+    if (dsm && (opc == OP_ADD || opc == OP_SUB || opc == OP_MUL || opc == OP_DIV)) {
+      const int base = opc == OP_ADD ? D_ADD_RR : opc == OP_SUB ? D_SUB_RR : opc == OP_MUL ? D_MUL_RR : D_DIV_RR;
+      if (in.ma == M_SMEM && in.mb == M_SMEM) opc = (uint8_t)base;
+      else if (in.ma == M_IMM && in.mb == M_SMEM) opc = (uint8_t)(base + 1);
+      else if (in.ma == M_SMEM && in.mb == M_IMM) opc = (uint8_t)(base + 2);
+    } else if (dsm && opc >= OP_NEG && opc <= OP_FRACT && in.ma == M_SMEM) {
+      opc = (uint8_t)(D_FU_BASE + (opc - OP_NEG));
+    }
+    d.opc = opc;
+    out.fwd.push_back(d);
+  }
+  out.rev.reserve(p.rev.size());
+  for (const RIns& in : p.rev) {
+    DRIns d{};
+    d.flags = in.flags;
+    d.aux = in.aux;
+    if (in.opc == XI_CHAIN) {
+      d.opc = D_CHAIN;
+      d.r = off(in.r);
+      d.a = off(in.a);
+      d.b = kNone;
+      d.va = in.va;  // first term
+      d.vb = kNone;
+      d.vr = kNone;
+      out.rev.push_back(d);
+      continue;
+    }
+    d.r = off(in.r);
+    d.a = off(in.a);
+    d.b = off(in.b);
+    d.vr = off(in.vr);
+    d.imm = 0.0;
+    if (in.flags & RF_VA_IMM) {
+      d.imm = p.pool[in.va];
+      d.va = kNone;
+    } else {
+      d.va = off(in.va);
+    }
+    if (in.flags & RF_VB_IMM) {
+      if (in.flags & RF_VA_IMM) {
+        err = "reverse op with two constant operands";
+        return false;
+      }
+      d.imm = p.pool[in.vb];
+      d.vb = kNone;
+    } else {
+      d.vb = off(in.vb);
+    }
+    uint8_t opc = in.opc;
+    if (opc != XI_SEED && opc != XI_STGRAD && !(in.flags & (RF_R_GLOB | RF_A_GLOB | RF_B_GLOB)))
+      opc = (uint8_t)(D_RF_BASE + opc);
+    d.opc = opc;
+    out.rev.push_back(d);
+  }
+  out.fterms.clear();
+  out.rterms.clear();
+  for (const PTerm& pt : p.terms) {
+    DFTerm f{};
+    f.kind = pt.kind;
+    f.op = pt.op;
+    f.xm = pt.fxm;
+    f.ym = pt.fym;
+    f.x = (pt.fxm == M_SMEM || pt.fxm == M_GLOB) ? off(pt.fxi) : kNone;
+    f.y = (pt.fym == M_SMEM || pt.fym == M_GLOB) ? off(pt.fyi) : kNone;
+    f.c = pt.c;
+    out.fterms.push_back(f);
+    DRTerm r{};
+    r.kind = pt.kind;
+    r.op = pt.op;
+    uint16_t fl = pt.flags & (CF_X_INIT | CF_Y_INIT | CF_X_ADJ | CF_Y_ADJ);
+    if (pt.rxm == M_GLOB) fl |= CF_X_GLOB;
+    if (pt.rym == M_GLOB) fl |= CF_Y_GLOB;
+    r.flags = fl;
+    r.ax = (pt.flags & CF_X_ADJ) ? off(pt.rxi) : kNone;
+    r.ay = (pt.flags & CF_Y_ADJ) ? off(pt.ryi) : kNone;
+    r.vx = off(pt.vx);
+    r.vy = off(pt.vy);
+    r.c = pt.c;
+    out.rterms.push_back(r);
+  }
+  if (out.fterms.empty()) {
+    out.fterms.push_back(DFTerm{});
+    out.rterms.push_back(DRTerm{});
+  }
+  if (!ok) err = "slot region exceeds the 32-bit offset encoding; use a smaller tile";
+  return ok;
 }
 
 }  // namespace ech

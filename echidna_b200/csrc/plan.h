@@ -29,9 +29,27 @@ struct PlanStats {
   uint64_t flops_rev = 0;      // arithmetic ops per unit (reverse)
   uint64_t specials_fwd = 0;   // libm-class calls per unit (forward)
   uint64_t specials_rev = 0;
+  uint64_t chains = 0;         // fused chains
+  uint64_t chain_ops = 0;      // tape ops absorbed into chains
 };
 
+// One term of a fused chain (XI_CHAIN) with its resolved locations.
+// Packed layout (48 bytes) so the host-only dump can hand it out as-is.
+struct PTerm {
+  uint8_t kind, op;     // ChainKind / operand position (see ech_types.h)
+  uint16_t flags;       // ChainFlag bits (CF_*_INIT, CF_*_ADJ, CF_*_GLOB)
+  uint32_t xs, ys;      // slot ids, kNone when absent
+  uint8_t fxm, fym;     // forward modes of x, y
+  uint8_t rxm, rym;     // reverse modes of adj(x), adj(y)
+  uint32_t fxi, fyi;    // forward register / slot indices
+  uint32_t rxi, ryi;    // reverse adjoint register / slot indices
+  uint32_t vx, vy;      // trajectory slots of the values x*y terms read
+  double c;             // constant of c*x / x*c / c terms
+};
+static_assert(sizeof(PTerm) == 48, "PTerm must be 48 bytes");
+
 struct Plan {
+  std::vector<PTerm> terms;  // fused-chain terms, shared by both programs
   std::vector<Ins> fwd;
   std::vector<RIns> rev;
   std::vector<double> pool;
@@ -43,6 +61,17 @@ struct Plan {
 
 // Builds the programs for `kind` with at most `smem_cap` shared registers.
 Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap);
+
+// Device encoding of a plan for a launch geometry (`tile` points per CTA,
+// `vbytes` bytes per slot value).  Returns false (with `err`) if an offset does
+// not fit the 32-bit encoding.
+struct DevProgram {
+  std::vector<DIns> fwd;
+  std::vector<DRIns> rev;
+  std::vector<DFTerm> fterms;
+  std::vector<DRTerm> rterms;
+};
+bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out, std::string& err);
 
 // Validation with the reference's messages.  Empty string = valid.
 //   BytecodeTape::validate   (src/bytecode_tape/mod.rs:575-705)

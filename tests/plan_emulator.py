@@ -17,7 +17,10 @@ from echidna_b200.tape import OpCode
 
 INS = struct.Struct("<BBBBIIIIid")
 RINS = struct.Struct("<BBHIIIIIIi")
-XI_LDIN, XI_STOUT, XI_MOV, XI_SEED, XI_STGRAD = 64, 65, 66, 67, 68
+TERM = struct.Struct("<BBHIIBBBBIIIIIId")   # PTerm, 48 bytes
+XI_LDIN, XI_STOUT, XI_MOV, XI_SEED, XI_STGRAD, XI_CHAIN = 64, 65, 66, 67, 68, 69
+CK_X, CK_CX, CK_XC, CK_XY, CK_C = range(5)
+CF = dict(X_INIT=1, Y_INIT=2, X_GLOB=4, Y_GLOB=8, X_ADJ=16, Y_ADJ=32)
 M_SMEM, M_GLOB, M_IMM, M_NONE = 0, 1, 2, 3
 NONE = 0xFFFFFFFF
 RF = dict(R_GLOB=1, A_GLOB=2, B_GLOB=4, A_INIT=8, B_INIT=16, VA_IMM=32, VB_IMM=64, HAS_A=128, HAS_B=256)
@@ -29,20 +32,27 @@ def plan_dump(tape, kind: str, cap: int):
     op, a0, a1, vals = tape.arrays()
     vals = np.ascontiguousarray(vals, dtype=np.float64)
     outs = np.asarray(tape.output_indices, dtype=np.uint32)
-    counts = (ctypes.c_uint64 * 6)()
+    counts = (ctypes.c_uint64 * 7)()
     args = [_lib.ptr(op), _lib.ptr(a0), _lib.ptr(a1), _lib.ptr(vals), len(op), tape.num_inputs, tape.output_index,
             _lib.ptr(outs), len(outs), KIND[kind], cap]
-    st = lib.ech_plan_dump(*args, None, 0, None, 0, None, 0, counts)
+    st = lib.ech_plan_dump(*args, None, 0, None, 0, None, 0, None, 0, counts)
     assert st == 0, _lib.last_error()
-    nf, nr, npool = counts[0], counts[1], counts[2]
+    nf, nr, npool, nt = counts[0], counts[1], counts[2], counts[6]
     fb = ctypes.create_string_buffer(max(nf, 1) * 32)
     rb = ctypes.create_string_buffer(max(nr, 1) * 32)
+    tb = ctypes.create_string_buffer(max(nt, 1) * 48)
     pool = np.zeros(max(npool, 1), dtype=np.float64)
-    st = lib.ech_plan_dump(*args, ctypes.addressof(fb), nf, ctypes.addressof(rb), nr, _lib.ptr(pool), npool, counts)
+    st = lib.ech_plan_dump(*args, ctypes.addressof(fb), nf, ctypes.addressof(rb), nr, _lib.ptr(pool), npool,
+                           ctypes.addressof(tb), nt, counts)
     assert st == 0, _lib.last_error()
     fwd = [INS.unpack_from(fb, 32 * k) for k in range(nf)]
     rev = [RINS.unpack_from(rb, 32 * k) for k in range(nr)]
-    return fwd, rev, pool, dict(smem_regs=counts[3], far_slots=counts[4], traj_slots=counts[5])
+    terms = []
+    for k in range(nt):
+        (kind_, op_, flags, xs, ys, fxm, fym, rxm, rym, fxi, fyi, rxi, ryi, vx, vy, c) = TERM.unpack_from(tb, 48 * k)
+        terms.append(dict(kind=kind_, op=op_, flags=flags, fxm=fxm, fym=fym, fxi=fxi, fyi=fyi, rxm=rxm, rym=rym,
+                          rxi=rxi, ryi=ryi, vx=vx, vy=vy, c=c))
+    return fwd, rev, pool, dict(smem_regs=counts[3], far_slots=counts[4], traj_slots=counts[5], terms=terms)
 
 
 def _fwd(op, a, b, aux):
@@ -101,7 +111,8 @@ def _partials(op, a, b, r, aux):
 
 def run_gradient(tape, X, cap):
     """Emulates the gradient programs; returns (outputs, grads)."""
-    fwd, rev, pool, _ = plan_dump(tape, "gradient", cap)
+    fwd, rev, pool, info = plan_dump(tape, "gradient", cap)
+    terms = info["terms"]
     X = np.asarray(X, dtype=np.float64)
     B = X.shape[0]
     regs = {M_SMEM: {}, M_GLOB: {}}
@@ -122,6 +133,25 @@ def run_gradient(tape, X, cap):
             continue
         elif opc == XI_MOV:
             v = ld(ma, a, imm)
+        elif opc == XI_CHAIN:
+            acc = ld(ma, a, imm)
+            for tm in terms[b:b + aux]:
+                k = tm["kind"]
+                with np.errstate(all="ignore"):
+                    if k == CK_C:
+                        prod = np.full(B, tm["c"])
+                    else:
+                        x = regs[tm["fxm"]][tm["fxi"]]
+                        if k == CK_X:
+                            prod = x
+                        elif k == CK_CX:
+                            prod = tm["c"] * x
+                        elif k == CK_XC:
+                            prod = x * tm["c"]
+                        else:
+                            prod = x * regs[tm["fym"]][tm["fyi"]]
+                    acc = [acc + prod, prod + acc, acc - prod, prod - acc][tm["op"]]
+            v = acc
         else:
             av = ld(ma, a, imm)
             bv = np.zeros(B) if mb == M_NONE else ld(mb, b, imm)
@@ -141,6 +171,61 @@ def run_gradient(tape, X, cap):
             grads[:, aux] = 0.0 if r == NONE else regs[mr][r]
             continue
         adj = regs[mr][r]
+        if opc == XI_CHAIN:
+            adj_s = adj
+
+            def acc_into(m, idx, init, d, a_):
+                old = np.zeros(B) if init else regs[m][idx]
+                hit = (a_ != 0) & (d != 0)
+                with np.errstate(all="ignore"):
+                    regs[m][idx] = np.where(hit, old + d * a_, old)
+
+            for q in range(aux - 1, -1, -1):
+                tm = terms[va + q]
+                k = tm["kind"]
+                sub = tm["op"] >= 2
+                chain_a = (tm["op"] & 1) == 0
+                one = np.ones(B)
+                dA, dB = one, (-one if sub else one)
+                d_acc, d_term = (dA, dB) if chain_a else (dB, dA)
+                live = adj_s != 0
+                new_prev = np.zeros(B)
+                adj_p = np.zeros(B)
+
+                def acc_side():
+                    nonlocal new_prev
+                    if q == 0 and fl & RF["HAS_A"]:
+                        ma_ = M_GLOB if fl & RF["A_GLOB"] else M_SMEM
+                        acc_into(ma_, a, fl & RF["A_INIT"], d_acc, adj_s)
+                    else:
+                        with np.errstate(all="ignore"):
+                            new_prev = np.where(live & (d_acc != 0), 0.0 + d_acc * adj_s, 0.0)
+
+                def term_side():
+                    nonlocal adj_p
+                    if k == CK_X:
+                        mx = tm["rxm"]
+                        acc_into(mx, tm["rxi"], tm["flags"] & CF["X_INIT"], d_term, adj_s)
+                    elif k in (CK_CX, CK_XC, CK_XY):
+                        with np.errstate(all="ignore"):
+                            adj_p = np.where(live & (d_term != 0), 0.0 + d_term * adj_s, 0.0)
+
+                if chain_a:
+                    acc_side(); term_side()
+                else:
+                    term_side(); acc_side()
+                if k in (CK_CX, CK_XC):
+                    mx = tm["rxm"]
+                    acc_into(mx, tm["rxi"], tm["flags"] & CF["X_INIT"], np.full(B, tm["c"]), adj_p)
+                elif k == CK_XY:
+                    xv = traj[tm["vx"]]
+                    yv = traj[tm["vy"]]
+                    mx = tm["rxm"]
+                    my = tm["rym"]
+                    acc_into(mx, tm["rxi"], tm["flags"] & CF["X_INIT"], yv, adj_p)
+                    acc_into(my, tm["ryi"], tm["flags"] & CF["Y_INIT"], xv, adj_p)
+                adj_s = new_prev
+            continue
 
         def val(idx, is_imm):
             if idx == NONE:
