@@ -76,6 +76,8 @@ _SIGS = {
     "ech_gradient_batch_device": ([_P, _P, _I, _P, _U32, _P, _P, _P], _I),
     "ech_hvp_batch_device": ([_P, _P, _I, _P, _I, _P, _U32, _P, _P, _P], _I),
     "ech_taylor_batch_device": ([_P, _P, _I, _P, _P, _U32, _U32, _P, _P], _I),
+    "ech_noalloc_region_bytes": ([], _SZ),
+    "ech_gradient_batch_device_noalloc": ([_P, _P, _I, _P, _U32, _P, _P, _P], _I),
     "ech_tape_plan_stats": ([_P, _P, _I, _U32, _I, ctypes.POINTER(_U64)], _I),
     "ech_plan_dump": ([_P, _P, _P, _P, _U32, _U32, _U32, _P, _U32, _I, _U32, _P, _SZ, _P, _SZ, _P, _SZ, _P, _SZ,
                        ctypes.POINTER(_U64)], _I),

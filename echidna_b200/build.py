@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import concurrent.futures as cf
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -27,9 +28,28 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-ffp-contract=off", "-I", CSRC]
 
 CU_SOURCES = ["abi.cu", "k_plain.cu", "k_dual.cu", "k_jet.cu", "k_jet1.cu", "k_jet2.cu", "k_jet3.cu", "k_jet4.cu", "k_jet5.cu",
-              "stde.cu"]
+              "stde.cu", "noalloc.cu"]
 CXX_SOURCES = ["plan.cpp"]
-HEADERS = ["ech_types.h", "device_math.cuh", "interp.cuh", "launch.h", "plan.h", "k_common.cuh"]
+
+
+_INC = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _deps(src: str, seen=None) -> set:
+    """Local headers `src` includes, transitively (quoted includes only)."""
+    seen = set() if seen is None else seen
+    try:
+        text = open(src).read()
+    except OSError:
+        return seen
+    for name in _INC.findall(text):
+        path = os.path.normpath(os.path.join(os.path.dirname(src), name))
+        if not os.path.exists(path):
+            path = os.path.join(CSRC, name)
+        if os.path.exists(path) and path not in seen:
+            seen.add(path)
+            _deps(path, seen)
+    return seen
 
 
 def _newer(src: str, obj: str, deps) -> bool:
@@ -48,19 +68,18 @@ def _compile(cmd):
 
 def build(verbose: bool = False, jobs: int | None = None) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    deps = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "echidna_b200.h")]
     cmds, objs = [], []
     for s in CU_SOURCES:
         src = os.path.join(CSRC, s)
         obj = os.path.join(BUILD, s + ".o")
         objs.append(obj)
-        if _newer(src, obj, deps):
+        if _newer(src, obj, _deps(src)):
             cmds.append([NVCC, *ARCH, *NVFLAGS, "-c", src, "-o", obj])
     for s in CXX_SOURCES:
         src = os.path.join(CSRC, s)
         obj = os.path.join(BUILD, s + ".o")
         objs.append(obj)
-        if _newer(src, obj, deps):
+        if _newer(src, obj, _deps(src)):
             cmds.append(["g++", *CXXFLAGS, "-c", src, "-o", obj])
     if cmds:
         with cf.ThreadPoolExecutor(max_workers=jobs or min(8, os.cpu_count() or 4)) as ex:

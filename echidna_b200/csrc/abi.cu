@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/echidna_b200.h"
+#include "abi_internal.h"
 #include "interp.cuh"
 #include "launch.h"
 #include "plan.h"
@@ -90,6 +91,12 @@ struct ech_tape {
   HostTape host;
   std::mutex mu;
   std::map<std::tuple<int, int, uint32_t, uint32_t, uint32_t>, std::unique_ptr<DevPlan>> plans;  // (kind, K, cap, tile, vbytes)
+  // host-encoded programs for entry points that place them in their own memory
+  struct HostProgram {
+    Plan plan;
+    DevProgram prog;
+  };
+  std::map<std::tuple<int, int, uint32_t, uint32_t, uint32_t>, std::unique_ptr<HostProgram>> host_programs;
 };
 
 // ───────────────────────────── context ──────────────────────────────────────
@@ -898,4 +905,47 @@ size_t value_bytes(const LaunchReq& r) {
   }
   return s;
 }
+}  // namespace ech
+
+// ───────────────────────────── internal hooks ───────────────────────────────
+namespace ech {
+
+ech_status set_error(ech_status st, const std::string& msg) { return fail(st, msg); }
+
+ech_status prepare_gradient_host(ech_ctx* ctx, const ech_tape* tc, int f64, uint32_t B, HostSweep* out) {
+  CHECK(common_checks(ctx, tc, f64 != 0));
+  CHECK(batch_args(tc, B));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  const LaunchCfg c = choose_cfg(ctx, t, 1, 0);
+  const ech_tape::HostProgram* hp = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(t->mu);
+    auto key = std::make_tuple(1, 0, c.cap, c.tile, (uint32_t)c.vbytes);
+    auto it = t->host_programs.find(key);
+    if (it == t->host_programs.end()) {
+      std::unique_ptr<ech_tape::HostProgram> np(new ech_tape::HostProgram());
+      np->plan = build_plan(t->host, Kind::Gradient, c.cap);
+      std::string err;
+      if (!encode_plan(np->plan, c.tile, (uint32_t)c.vbytes, np->prog, err)) return fail(ECH_ERR_OTHER, err);
+      it = t->host_programs.emplace(key, std::move(np)).first;
+    }
+    hp = it->second.get();
+  }
+  out->req = c.req;
+  out->threads = c.threads;
+  out->tile = c.tile;
+  out->vbytes = c.vbytes;
+  out->smem = kRingBytes + (size_t)std::max<uint32_t>(hp->plan.smem_regs, 1) * c.tile * c.vbytes;
+  out->plan = &hp->plan;
+  out->prog = &hp->prog;
+  out->device = ctx->device;
+  out->sm_count = ctx->sm_count;
+  out->ni = t->host.ni;
+  out->no = (uint32_t)t->host.outs.size();
+  out->d_err = ctx->d_err;
+  out->stream = ctx->stream;
+  out->mu = &ctx->mu;
+  return ECH_OK;
+}
+
 }  // namespace ech

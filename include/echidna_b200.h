@@ -195,6 +195,26 @@ ECH_API ech_status ech_taylor_batch_device(ech_ctx* ctx, const ech_tape* tape, i
 /* Waits for the context's stream and reports any device-side error word. */
 ECH_API ech_status ech_ctx_synchronize(ech_ctx* ctx);
 
+/* ── gradient without device allocation ─────────────────────────────────────
+ * No counterpart in the reference.  Same arguments, results and checks as
+ * ech_gradient_batch_device, but the call allocates no device memory: the
+ * programs and the per-CTA slot scratch live in one fixed region of
+ * ech_noalloc_region_bytes() bytes (64 MiB) compiled into the library, one per
+ * device.  For callers that must not allocate: a host runtime that owns a
+ * fixed device-memory budget or its own pool, or a latency-critical loop that
+ * cannot take the device-wide synchronisation cudaMalloc/cudaFree may imply.
+ * The first call on a device looks the region up (cudaGetSymbolAddress);
+ * make it before any stream capture.  Large batches run with a smaller grid;
+ * a tape whose program plus one CTA's scratch exceeds the region fails with
+ * ECH_ERR_OUT_OF_MEMORY.  Nothing in the region needs to start at zero.
+ * Calls share the one region per device, so calls whose work overlaps in
+ * time (different streams, or different contexts on one device) race on it:
+ * order them on one stream.  Device-side errors are reported by
+ * ech_ctx_synchronize, as for the other *_device calls. */
+ECH_API size_t ech_noalloc_region_bytes(void);
+ECH_API ech_status ech_gradient_batch_device_noalloc(ech_ctx* ctx, const ech_tape* tape, int f64, const void* inputs,
+                                                     uint32_t batch_size, void* outputs, void* grads, void* stream);
+
 /* ── introspection ────────────────────────────────────────────────────────── */
 /* kind: 0 forward, 1 gradient, 2 hvp, 3 tangent, 4 taylor(order).  Fills
  * stats[12]: fwd_ops, rev_ops, max_live_fwd, max_live_rev, traj_values,
