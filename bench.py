@@ -319,7 +319,9 @@ def main():
                 "d2h_bytes_per_step": int(ho.nbytes + hg.nbytes + hg2.nbytes + hh.nbytes)},
         "clocks": clk.summary(),
         "detail": {"gradient_ms": g_ms, "hvp_ms": h_ms, "gradient_points_per_s": BATCH / (g_ms * 1e-3),
-                   "hvp_points_per_s": BATCH / (h_ms * 1e-3), "plan_gradient": sg, "plan_hvp": sh},
+                   "hvp_points_per_s": BATCH / (h_ms * 1e-3), "plan_gradient": sg, "plan_hvp": sh,
+                   "shape_gradient": ctx.launch_shape(gt, "gradient", BATCH),
+                   "shape_hvp": ctx.launch_shape(gt, "hvp", BATCH)},
     }
     if rank == 0 and not args.no_cpu_baseline:
         nth = os.cpu_count() or 1

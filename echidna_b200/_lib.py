@@ -77,6 +77,8 @@ _SIGS = {
     "ech_hvp_batch_device": ([_P, _P, _I, _P, _I, _P, _U32, _P, _P, _P], _I),
     "ech_taylor_batch_device": ([_P, _P, _I, _P, _P, _U32, _U32, _P, _P], _I),
     "ech_noalloc_region_bytes": ([], _SZ),
+    "ech_ctx_set_autotune": ([_P, _I], _I),
+    "ech_tape_launch_shape": ([_P, _P, _I, _U32, _U64, ctypes.POINTER(_U64)], _I),
     "ech_gradient_batch_device_noalloc": ([_P, _P, _I, _P, _U32, _P, _P, _P], _I),
     "ech_tape_plan_stats": ([_P, _P, _I, _U32, _I, ctypes.POINTER(_U64)], _I),
     "ech_plan_dump": ([_P, _P, _P, _P, _U32, _U32, _U32, _P, _U32, _I, _U32, _P, _SZ, _P, _SZ, _P, _SZ, _P, _SZ,

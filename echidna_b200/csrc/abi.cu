@@ -78,11 +78,20 @@ struct ech_ctx {
   cudaStream_t stream = nullptr;
   int sm_count = 0;
   size_t smem_optin = 0;
+  size_t smem_per_sm = 0;      // shared memory per SM
+  size_t smem_reserved = 0;    // shared memory the runtime reserves per block
+  bool autotune = true;        // pick launch shapes by timing (per tape, kind, batch size)
   std::mutex mu;
   DevBuf scratch, io_in, io_in2, io_out, io_out2, io_out3, stde_tmp;
   uint32_t* d_err = nullptr;
   // launch overrides (0 = automatic)
   uint32_t ov_threads = 0, ov_ppt = 0, ov_cap = 0;
+};
+
+// Launch shape: block size, points per thread, and how many CTAs should share
+// an SM (which sets the shared-register cap).
+struct Shape {
+  uint32_t threads = 128, P = 1, ctas = 2;
 };
 
 struct ech_tape {
@@ -97,6 +106,8 @@ struct ech_tape {
     DevProgram prog;
   };
   std::map<std::tuple<int, int, uint32_t, uint32_t, uint32_t>, std::unique_ptr<HostProgram>> host_programs;
+  // autotuned launch shapes, keyed (kind, K, log2 of the unit count)
+  std::map<std::tuple<int, int, int>, Shape> shapes;
 };
 
 // ───────────────────────────── context ──────────────────────────────────────
@@ -114,6 +125,8 @@ extern "C" ECH_API ech_status ech_ctx_create(int device, ech_ctx** out) {
   if (prop.major < 10) return fail(ECH_ERR_NO_DEVICE, "no suitable GPU device found (sm_100a required)");
   c->sm_count = prop.multiProcessorCount;
   c->smem_optin = prop.sharedMemPerBlockOptin;
+  c->smem_per_sm = prop.sharedMemPerMultiprocessor;
+  c->smem_reserved = prop.reservedSharedMemPerBlock;
   CU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   CU(cudaMalloc(&c->d_err, sizeof(uint32_t)));
   CU(cudaMemset(c->d_err, 0, sizeof(uint32_t)));
@@ -137,6 +150,12 @@ extern "C" ECH_API ech_status ech_ctx_set_launch(ech_ctx* ctx, uint32_t threads,
   ctx->ov_threads = threads;
   ctx->ov_ppt = ppt;
   ctx->ov_cap = cap;
+  return ECH_OK;
+}
+
+extern "C" ECH_API ech_status ech_ctx_set_autotune(ech_ctx* ctx, int enable) {
+  if (!ctx) return fail(ECH_ERR_INVALID_ARG, "ctx is null");
+  ctx->autotune = enable != 0;
   return ECH_OK;
 }
 
@@ -250,24 +269,38 @@ static Kind kind_of(int k) {
   }
 }
 
-// Shared-register budget: the ring plus `cap` registers of `tile` values must
-// fit, aiming at two CTAs per SM when the live set allows it.
-static LaunchCfg choose_cfg(ech_ctx* ctx, const ech_tape* t, int kind, int K) {
+// The shared-register cap follows from the shape: the ring plus `cap`
+// registers of `tile` values per CTA, `ctas` CTAs per SM.
+static LaunchCfg cfg_for(ech_ctx* ctx, const ech_tape* t, int kind, int K, Shape sh) {
   LaunchCfg c;
   c.req.f64 = t->f64;
   c.req.K = K;
   c.req.vk = (kind == 2 || kind == 3) ? VKind::Dual : (kind == 4 ? VKind::Jet : VKind::Plain);
   c.req.rev = (kind == 1 || kind == 2);
-  c.req.P = ctx->ov_ppt ? (int)ctx->ov_ppt : 1;
-  c.threads = ctx->ov_threads ? (int)ctx->ov_threads : 128;
-  c.tile = (uint32_t)(c.threads * c.req.P);
+  c.req.P = (int)sh.P;
+  c.threads = (int)sh.threads;
+  c.tile = sh.threads * sh.P;
   c.vbytes = value_bytes(c.req);
-  const size_t budget_total = std::min<size_t>(ctx->smem_optin, 227 * 1024) - 1024;
-  const size_t per_cta = ctx->ov_cap ? budget_total : budget_total / 2;
-  size_t cap = (per_cta - kRingBytes) / (c.tile * c.vbytes);
+  // per-SM shared memory split between `ctas` CTAs, each paying the
+  // per-block reservation and the kernel's static barriers
+  const size_t per_sm = ctx->smem_per_sm ? ctx->smem_per_sm : 233472;
+  size_t per_cta = per_sm / std::max<uint32_t>(sh.ctas, 1);
+  per_cta = per_cta > ctx->smem_reserved + 128 ? per_cta - ctx->smem_reserved - 128 : 0;
+  per_cta = std::min(per_cta, ctx->smem_optin);
+  size_t cap = per_cta > (size_t)kRingBytes ? (per_cta - kRingBytes) / (c.tile * c.vbytes) : 0;
   if (ctx->ov_cap) cap = std::min<size_t>(cap, ctx->ov_cap);
   c.cap = (uint32_t)std::max<size_t>(cap, 1);
   return c;
+}
+
+// The fixed shape used with launch overrides, for small batches, and when
+// autotuning is off: 128 threads, one point per thread, two CTAs per SM.
+static LaunchCfg choose_cfg(ech_ctx* ctx, const ech_tape* t, int kind, int K) {
+  Shape sh;
+  sh.threads = ctx->ov_threads ? ctx->ov_threads : 128;
+  sh.P = ctx->ov_ppt ? ctx->ov_ppt : 1;
+  sh.ctas = ctx->ov_cap ? 1 : 2;
+  return cfg_for(ctx, t, kind, K, sh);
 }
 
 static ech_status get_plan(ech_tape* t, int kind, int K, uint32_t cap, uint32_t tile, uint32_t vbytes, DevPlan** out) {
@@ -311,9 +344,8 @@ struct SweepIO {
   uint64_t seed = 0;
 };
 
-static ech_status enqueue(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n_units, const SweepIO& io,
-                          cudaStream_t st) {
-  LaunchCfg c = choose_cfg(ctx, t, kind, K);
+static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n_units, const SweepIO& io,
+                             cudaStream_t st, LaunchCfg c) {
   DevPlan* dp = nullptr;
   ech_status s = get_plan(t, kind, K, c.cap, c.tile, (uint32_t)c.vbytes, &dp);
   if (s != ECH_OK) return s;
@@ -359,6 +391,82 @@ static ech_status enqueue(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n
   e = launch_sweep(c.req, kp, (int)grid, c.threads, c.smem, st, &bps);
   if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
   return ECH_OK;
+}
+
+// Autotuning applies from this many units up; smaller batches use the fixed shape.
+static constexpr uint64_t kTuneMinUnits = 16384;
+
+static int size_bucket(uint64_t n) {
+  int b = 0;
+  while ((1ull << (b + 1)) <= n && b < 40) ++b;
+  return b;
+}
+
+// Candidate shapes, timed on the call's own inputs (every shape computes
+// bit-identical results: a point's arithmetic does not depend on the launch).
+static const Shape kShapes[] = {
+    {128, 1, 1}, {128, 1, 2}, {128, 1, 3}, {128, 1, 4}, {128, 2, 1}, {128, 2, 2},
+    {128, 2, 3}, {128, 4, 1}, {128, 4, 2}, {256, 1, 1}, {256, 1, 2}, {64, 2, 4},
+};
+
+static ech_status tune(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n_units, const SweepIO& io,
+                       cudaStream_t st, Shape* best) {
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  float best_ms = -1.0f;
+  ech_status first_err = ECH_OK;
+  std::string first_msg;
+  for (const Shape& sh : kShapes) {
+    const LaunchCfg c = cfg_for(ctx, t, kind, K, sh);
+    if (c.cap < 1 || kRingBytes + (size_t)c.tile * c.vbytes > ctx->smem_optin) continue;
+    ech_status s = launch_cfg(ctx, t, kind, K, n_units, io, st, c);  // warm: plan build + upload
+    if (s == ECH_OK) {
+      cudaEventRecord(e0, st);
+      s = launch_cfg(ctx, t, kind, K, n_units, io, st, c);
+      cudaEventRecord(e1, st);
+    }
+    if (s != ECH_OK) {
+      if (first_err == ECH_OK) { first_err = s; first_msg = g_last_error; }
+      continue;
+    }
+    if (cudaEventSynchronize(e1) != cudaSuccess) break;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (best_ms < 0.0f || ms < best_ms) {
+      best_ms = ms;
+      *best = sh;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (best_ms < 0.0f) return first_err != ECH_OK ? fail(first_err, first_msg) : fail(ECH_ERR_OTHER, "no launch shape fits");
+  return ECH_OK;
+}
+
+static ech_status enqueue(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n_units, const SweepIO& io,
+                          cudaStream_t st) {
+  const bool overridden = ctx->ov_threads || ctx->ov_ppt || ctx->ov_cap;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (!overridden && ctx->autotune && n_units >= kTuneMinUnits && cudaStreamIsCapturing(st, &cap) == cudaSuccess &&
+      cap == cudaStreamCaptureStatusNone) {
+    const auto key = std::make_tuple(kind, K, size_bucket(n_units));
+    Shape sh;
+    bool have = false;
+    {
+      std::lock_guard<std::mutex> lk(t->mu);
+      auto it = t->shapes.find(key);
+      if (it != t->shapes.end()) { sh = it->second; have = true; }
+    }
+    if (!have) {
+      ech_status s = tune(ctx, t, kind, K, n_units, io, st, &sh);
+      if (s != ECH_OK) return s;
+      std::lock_guard<std::mutex> lk(t->mu);
+      t->shapes[key] = sh;
+    }
+    return launch_cfg(ctx, t, kind, K, n_units, io, st, cfg_for(ctx, t, kind, K, sh));
+  }
+  return launch_cfg(ctx, t, kind, K, n_units, io, st, choose_cfg(ctx, t, kind, K));
 }
 
 static ech_status check_err_word(ech_ctx* ctx) {
@@ -890,6 +998,27 @@ ECH_API ech_status ech_tape_plan_stats(ech_ctx* ctx, const ech_tape* tc, int kin
   uint64_t v[12] = {s.fwd_ops, s.rev_ops, s.max_live_fwd, s.max_live_rev, s.traj_values, s.flops_fwd, s.flops_rev,
                     s.specials_fwd, s.specials_rev, p.smem_regs, p.far_slots, p.fwd.size() + p.rev.size()};
   memcpy(stats, v, sizeof v);
+  return ECH_OK;
+}
+
+ECH_API ech_status ech_tape_launch_shape(ech_ctx* ctx, const ech_tape* tc, int kind, uint32_t order,
+                                        uint64_t n_units, uint64_t* shape) {
+  if (!ctx || !tc || !shape) return fail(ECH_ERR_INVALID_ARG, "null argument");
+  if (kind < 0 || kind > 4) return fail(ECH_ERR_INVALID_ARG, "kind must be 0..4");
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  Shape sh;
+  uint64_t tuned = 0;
+  LaunchCfg c;
+  {
+    std::lock_guard<std::mutex> lk(t->mu);
+    auto it = t->shapes.find(std::make_tuple(kind, (int)order, size_bucket(n_units)));
+    if (it != t->shapes.end()) { sh = it->second; tuned = 1; }
+  }
+  c = tuned ? cfg_for(ctx, t, kind, (int)order, sh) : choose_cfg(ctx, t, kind, (int)order);
+  Plan p = build_plan(t->host, kind_of(kind), c.cap);
+  uint64_t v[8] = {(uint64_t)c.threads, (uint64_t)c.req.P, tuned ? sh.ctas : 0, c.cap, p.smem_regs, p.far_slots,
+                   p.traj_slots, tuned};
+  memcpy(shape, v, sizeof v);
   return ECH_OK;
 }
 

@@ -218,6 +218,17 @@ class CudaContext:
     def set_launch(self, threads: int = 0, points_per_thread: int = 0, smem_reg_cap: int = 0):
         _check(_lib.load().ech_ctx_set_launch(self._h, threads, points_per_thread, smem_reg_cap))
 
+    def set_autotune(self, enable: bool):
+        _check(_lib.load().ech_ctx_set_autotune(self._h, 1 if enable else 0))
+
+    def launch_shape(self, tape: _TapeHandle, kind: str, n_units: int, order: int = 0) -> dict:
+        kinds = {"forward": 0, "gradient": 1, "hvp": 2, "tangent": 3, "taylor": 4}
+        buf = (ctypes.c_uint64 * 8)()
+        _check(_lib.load().ech_tape_launch_shape(self._h, tape._h, kinds[kind], order, n_units, buf))
+        keys = ["threads", "points_per_thread", "ctas_per_sm", "smem_reg_cap", "smem_regs", "far_slots",
+                "traj_slots", "tuned"]
+        return dict(zip(keys, [int(v) for v in buf]))
+
     def plan_stats(self, tape: _TapeHandle, kind: str, order: int = 0) -> dict:
         kinds = {"forward": 0, "gradient": 1, "hvp": 2, "tangent": 3, "taylor": 4}
         buf = (ctypes.c_uint64 * 12)()

@@ -237,6 +237,18 @@ ECH_API ech_status ech_plan_dump(const uint32_t* opcodes, const uint32_t* arg0, 
  * points per thread and the shared-register cap. */
 ECH_API ech_status ech_ctx_set_launch(ech_ctx* ctx, uint32_t threads, uint32_t points_per_thread,
                                       uint32_t smem_reg_cap);
+/* Launch-shape autotuning (default on).  Without overrides, the first sweep of
+ * a (tape, kind, order, batch-size octave) with at least 16,384 units times a
+ * fixed set of shapes (threads per CTA, points per thread, CTAs per SM) on the
+ * call's own inputs and keeps the fastest; every shape computes bit-identical
+ * results.  That first call waits for its timing runs; calls made while the
+ * stream is being captured use the fixed shape. */
+ECH_API ech_status ech_ctx_set_autotune(ech_ctx* ctx, int enable);
+/* The shape a sweep of `n_units` units uses.  shape[8]: threads, points per
+ * thread, CTAs per SM (0 = fixed shape), shared-register cap, shared registers
+ * used, global slots, trajectory slots, tuned (1/0). */
+ECH_API ech_status ech_tape_launch_shape(ech_ctx* ctx, const ech_tape* tape, int kind, uint32_t order,
+                                        uint64_t n_units, uint64_t* shape);
 
 #ifdef __cplusplus
 }
