@@ -17,8 +17,9 @@ sweep over the whole batch, FP32 (the throughput precision of that configuration
   bounded sample of the same workload, on all host cores.
 
 ``--impl reference`` times that CPU implementation alone as the reference arm.
-Multi-GPU (torchrun): every rank evaluates its own 65,536-point shard (points are
-independent, no collective on the data path); timing is the max over ranks.
+Multi-GPU (torchrun): the global batch is world * 65,536 points and every rank
+evaluates its own contiguous 65,536-point shard (points are independent, no
+collective on the data path); timing is the max over ranks.
 """
 from __future__ import annotations
 
@@ -105,12 +106,15 @@ class ClockSampler:
                 "samples": len(mhz)}
 
 
-def _workload(dtype):
+def _workload(dtype, rank=0, world=1):
+    """The tape and this rank's shard of the global batch (world * 65,536 points)."""
     from echidna_b200 import configs
+    from echidna_b200.multi import rank_rows
     tape = configs.mlp(N_IN, 64, dtype=np.float64)
-    rng = np.random.default_rng(configs.SEEDS["mlp"])
-    X = rng.normal(size=(BATCH, N_IN))
-    V = rng.choice([-1.0, 1.0], size=(BATCH, N_IN))
+    seed = configs.SEEDS["mlp"]
+    n = world * BATCH
+    X = rank_rows(n, rank, world, seed, N_IN, lambda g, s: g.normal(size=s))
+    V = rank_rows(n, rank, world, seed + 1, N_IN, lambda g, s: g.choice([-1.0, 1.0], size=s))
     return tape, X.astype(dtype), V.astype(dtype)
 
 
@@ -178,6 +182,7 @@ def main():
     import torch.distributed as dist
     from echidna_b200 import _lib
     from echidna_b200.gpu import CudaContext, GpuTapeData
+    from echidna_b200.multi import max_over_ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -190,7 +195,7 @@ def main():
     ctx = CudaContext.new(local)
     assert ctx is not None, "no CUDA device"
 
-    tape, X, V = _workload(np.float32)
+    tape, X, V = _workload(np.float32, rank, world)
     gt = ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(tape))
     # a dedicated stream: the events below and the engine's launches must share it
     stream = torch.cuda.Stream()
@@ -244,9 +249,7 @@ def main():
     assert lib.ech_ctx_synchronize(ctx._h) == 0, _lib.last_error()
     step_ms = float(np.sum(t_grad) + np.sum(t_hvp)) / args.steps
     if world > 1:
-        tt = torch.tensor([step_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        step_ms = float(tt.item())
+        step_ms = max_over_ranks(step_ms, "cuda")
 
     # end-to-end through the host-buffer ABI (pinned host buffers)
     hX = torch.from_numpy(X).pin_memory().numpy()
@@ -275,9 +278,7 @@ def main():
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e_step_ms = float(np.median(e2e_ms))
     if world > 1:
-        tt = torch.tensor([e2e_step_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_step_ms = float(tt.item())
+        e2e_step_ms = max_over_ranks(e2e_step_ms, "cuda")
 
     # roofline of the dominant kernel
     sg = ctx.plan_stats(gt, "gradient")

@@ -608,6 +608,9 @@ class BReverse:
     def atanh(self):
         return self._unary(OpCode.Atanh, "atanh")
 
+    def __abs__(self):
+        return self.abs()
+
     def abs(self):
         return self._unary(OpCode.Abs, "abs")
 
