@@ -77,6 +77,13 @@ _SIGS = {
     "ech_hvp_batch_device": ([_P, _P, _I, _P, _I, _P, _U32, _P, _P, _P], _I),
     "ech_taylor_batch_device": ([_P, _P, _I, _P, _P, _U32, _U32, _P, _P], _I),
     "ech_noalloc_region_bytes": ([], _SZ),
+    "ech_diagonal_kth_order_stochastic_f32": ([_P, _P, _P, _SZ, _U32, _P, _SZ, _P], _I),
+    "ech_diagonal_kth_order_stochastic_f64": ([_P, _P, _P, _SZ, _U32, _P, _SZ, _P], _I),
+    "ech_detect_hessian_sparsity": ([_P, _P, _P, _U32, _U32, _P, _P, _SZ, ctypes.POINTER(_SZ)], _I),
+    "ech_detect_jacobian_sparsity": ([_P, _P, _P, _U32, _U32, _P, _U32, _P, _P, _SZ, ctypes.POINTER(_SZ)], _I),
+    "ech_greedy_coloring": ([_U32, _P, _P, _SZ, _P, ctypes.POINTER(_U32)], _I),
+    "ech_column_coloring": ([_U32, _U32, _P, _P, _SZ, _P, ctypes.POINTER(_U32)], _I),
+    "ech_row_coloring": ([_U32, _U32, _P, _P, _SZ, _P, ctypes.POINTER(_U32)], _I),
     "ech_ctx_set_autotune": ([_P, _I], _I),
     "ech_tape_launch_shape": ([_P, _P, _I, _U32, _U64, ctypes.POINTER(_U64)], _I),
     "ech_gradient_batch_device_noalloc": ([_P, _P, _I, _P, _U32, _P, _P, _P], _I),

@@ -29,7 +29,7 @@ CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-ffp-contract=
 
 CU_SOURCES = ["abi.cu", "k_plain.cu", "k_dual.cu", "k_jet.cu", "k_jet1.cu", "k_jet2.cu", "k_jet3.cu", "k_jet4.cu", "k_jet5.cu",
               "stde.cu", "noalloc.cu"]
-CXX_SOURCES = ["plan.cpp"]
+CXX_SOURCES = ["plan.cpp", "sparsity.cpp"]
 
 
 _INC = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)

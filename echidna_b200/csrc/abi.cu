@@ -791,14 +791,16 @@ static ech_status stde_checks(const ech_tape* t, size_t n, const char* caller, c
   return ECH_OK;
 }
 
-// Taylor K=3 over npoints*S units, then the per-point Welford reduction.
+// Taylor order K (default 3) over npoints*S units, then the per-point Welford
+// reduction of scale*c_kk (default 2*c2).
 // dir_mode: 0 dirs per unit, 1 shared [S][n], 2 device Rademacher, 3 basis e_s.
 template <class T>
 static ech_status stde_run(ech_ctx* ctx, ech_tape* t, const T* d_x, bool x_bcast, uint64_t npoints, uint32_t S,
                            const T* d_dirs, int dir_mode, uint64_t seed, bool acc64, const T* d_cv, double trace,
-                           int control, ech_estimator_result* d_res, T* d_c0_out, T* d_c2_out) {
+                           int control, ech_estimator_result* d_res, T* d_c0_out, T* d_c2_out, int K = 3,
+                           int kk = 2, double scale = 2.0) {
   const uint64_t units = npoints * S;
-  CU(ctx->stde_tmp.ensure(units * 3 * sizeof(T)));
+  CU(ctx->stde_tmp.ensure(units * (uint64_t)K * sizeof(T)));
   SweepIO io;
   io.x = d_x;
   io.x_bcast = x_bcast ? 1 : 0;
@@ -807,11 +809,12 @@ static ech_status stde_run(ech_ctx* ctx, ech_tape* t, const T* d_x, bool x_bcast
   io.S = S;
   io.dir_mode = dir_mode;
   io.seed = seed;
-  CHECK(enqueue(ctx, t, 4, 3, units, io, ctx->stream));
+  CHECK(enqueue(ctx, t, 4, K, units, io, ctx->stream));
   const T* c0 = (const T*)ctx->stde_tmp.p;
-  const T* c2 = c0 + 2 * units;
+  const T* c2 = c0 + (uint64_t)kk * units;
   if (d_res) {
-    CU(launch_stde_reduce_t(sizeof(T) == 8, acc64, c0, c2, npoints, S, d_cv, trace, control, d_res, ctx->stream));
+    CU(launch_stde_reduce_t(sizeof(T) == 8, acc64, c0, c2, scale, npoints, S, d_cv, trace, control, d_res,
+                            ctx->stream));
   }
   if (d_c0_out) CU(cudaMemcpyAsync(d_c0_out, c0, units * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
   if (d_c2_out) CU(cudaMemcpyAsync(d_c2_out, c2, units * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
@@ -935,6 +938,67 @@ ECH_API ech_status ech_laplacian_batch_f64(ech_ctx* ctx, const ech_tape* t, cons
                                            uint32_t B, const double* dirs, size_t n_dirs, uint32_t S, int dir_mode,
                                            uint64_t seed, ech_estimator_result* res) {
   return do_laplacian_batch<double>(ctx, t, xs, n_xs, B, dirs, n_dirs, S, dir_mode, seed, res);
+}
+
+// diagonal_kth_order_stochastic (src/stde/higher_order.rs:173-227): one jet of
+// order k+1 along e_j per sampled coordinate j, samples k! * c_k, Welford in
+// the sample type, then the n / |J| rescaling of the estimate, variance and SE.
+template <class T>
+static ech_status do_diag_kth(ech_ctx* ctx, const ech_tape* tc, const T* x, size_t n, uint32_t k,
+                              const uint32_t* idx, size_t n_idx, ech_estimator_result* out) {
+  CHECK(common_checks(ctx, tc, sizeof(T) == 8));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(stde_checks(t, n, "diagonal_kth_order_stochastic", "diagonal"));
+  if (n_idx == 0) return fail(ECH_ERR_OTHER, "sampled_indices must not be empty");
+  if (k < 2) return fail(ECH_ERR_OTHER, "k must be >= 2 (use gradient for k=1)");
+  if (k + 1 > 5) {
+    char buf[96];
+    snprintf(buf, sizeof buf, "unsupported Taylor order %u, must be 1..=5", k + 1);
+    return fail(ECH_ERR_OTHER, buf);
+  }
+  if (!x || !idx || !out) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  for (size_t s = 0; s < n_idx; ++s) {
+    if (idx[s] >= n) {
+      char buf[96];
+      snprintf(buf, sizeof buf, "sampled index %u out of bounds (n=%zu)", idx[s], n);
+      return fail(ECH_ERR_OTHER, buf);
+    }
+  }
+  std::vector<T> dirs(n_idx * n, T(0));
+  for (size_t s = 0; s < n_idx; ++s) dirs[s * n + idx[s]] = T(1);
+  T kfact = T(1);
+  for (uint32_t i = 2; i <= k; ++i) kfact = kfact * (T)i;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  CU(ctx->io_in.ensure(n * sizeof(T)));
+  CU(ctx->io_in2.ensure(dirs.size() * sizeof(T)));
+  CU(ctx->io_out3.ensure(sizeof(ech_estimator_result)));
+  CU(cudaMemcpyAsync(ctx->io_in.p, x, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(ctx->io_in2.p, dirs.data(), dirs.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  CHECK(stde_run<T>(ctx, t, (const T*)ctx->io_in.p, true, 1, (uint32_t)n_idx, (const T*)ctx->io_in2.p, 1, 0, false,
+                    nullptr, 0.0, 0, (ech_estimator_result*)ctx->io_out3.p, nullptr, nullptr, (int)k + 1, (int)k,
+                    (double)kfact));
+  ech_estimator_result r;
+  CU(cudaMemcpyAsync(&r, ctx->io_out3.p, sizeof r, cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  CHECK(check_err_word(ctx));
+  const T nf = (T)n;
+  r.estimate = (double)((T)r.estimate * nf);
+  r.sample_variance = (double)((T)r.sample_variance * nf * nf);
+  r.standard_error = (double)((T)r.standard_error * nf);
+  *out = r;
+  return ECH_OK;
+}
+
+ECH_API ech_status ech_diagonal_kth_order_stochastic_f32(ech_ctx* ctx, const ech_tape* t, const float* x, size_t n,
+                                                         uint32_t k, const uint32_t* sampled_indices,
+                                                         size_t n_indices, ech_estimator_result* out) {
+  return do_diag_kth<float>(ctx, t, x, n, k, sampled_indices, n_indices, out);
+}
+ECH_API ech_status ech_diagonal_kth_order_stochastic_f64(ech_ctx* ctx, const ech_tape* t, const double* x, size_t n,
+                                                         uint32_t k, const uint32_t* sampled_indices,
+                                                         size_t n_indices, ech_estimator_result* out) {
+  return do_diag_kth<double>(ctx, t, x, n, k, sampled_indices, n_indices, out);
 }
 
 extern "C" {

@@ -38,10 +38,11 @@ inline cudaError_t launch_sweep(const LaunchReq& r, const KParams& kp, int grid,
   return cudaErrorInvalidValue;
 }
 
-// STDE per-point reduction of 2*c2 samples (Welford in direction order);
+// STDE per-point reduction of scale*c_k samples (Welford in direction order);
 // acc64 selects a double accumulator for f32 samples.
-cudaError_t launch_stde_reduce_t(bool f64, bool acc64, const void* c0, const void* c2, uint64_t npoints, uint32_t S,
-                                 const void* cv, double trace, int control, void* results, cudaStream_t st);
+cudaError_t launch_stde_reduce_t(bool f64, bool acc64, const void* c0, const void* ck, double scale, uint64_t npoints,
+                                 uint32_t S, const void* cv, double trace, int control, void* results,
+                                 cudaStream_t st);
 cudaError_t launch_control_term(bool f64, const void* dirs, const void* diag, uint32_t S, uint32_t n, void* cv,
                                 cudaStream_t st);
 

@@ -52,16 +52,17 @@ struct Welford {
   }
 };
 
-// One thread per point: samples 2*c2 of units [p*S, (p+1)*S), optionally minus
-// a control term cv[s] plus `offset` (laplacian_with_control).
+// One thread per point: samples scale*c_k of units [p*S, (p+1)*S) (scale 2,
+// k = 2 for the Laplacian; k!, k for k-th order diagonals), optionally minus a
+// control term cv[s] plus `trace` (laplacian_with_control).
 template <class T, class Acc>
-__global__ void stde_reduce_kernel(const T* c0, const T* c2, uint64_t npoints, uint32_t S, const T* cv, T trace,
-                                   int control, ech_estimator_result* out) {
+__global__ void stde_reduce_kernel(const T* c0, const T* ck, T scale, uint64_t npoints, uint32_t S, const T* cv,
+                                   T trace, int control, ech_estimator_result* out) {
   const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npoints) return;
   Welford<Acc> acc;
   for (uint32_t s = 0; s < S; ++s) {
-    const T vhv = T(2) * c2[p * S + s];
+    const T vhv = scale * ck[p * S + s];
     if (control) acc.update((Acc)(vhv - cv[s]));
     else acc.update((Acc)vhv);
   }
@@ -91,21 +92,24 @@ __global__ void control_term_kernel(const T* dirs, const T* diag, uint32_t S, ui
   cv[s] = acc;
 }
 
-cudaError_t launch_stde_reduce_t(bool f64, bool acc64, const void* c0, const void* c2, uint64_t npoints, uint32_t S,
-                                 const void* cv, double trace, int control, void* results, cudaStream_t st) {
+cudaError_t launch_stde_reduce_t(bool f64, bool acc64, const void* c0, const void* c2, double scale, uint64_t npoints,
+                                 uint32_t S, const void* cv, double trace, int control, void* results,
+                                 cudaStream_t st) {
   const int threads = 128;
   const unsigned blocks = (unsigned)((npoints + threads - 1) / threads);
   if (blocks == 0) return cudaSuccess;
   if (f64) {
-    stde_reduce_kernel<double, double><<<blocks, threads, 0, st>>>((const double*)c0, (const double*)c2, npoints, S,
+    stde_reduce_kernel<double, double><<<blocks, threads, 0, st>>>((const double*)c0, (const double*)c2, scale, npoints, S,
                                                                    (const double*)cv, trace, control,
                                                                    (ech_estimator_result*)results);
   } else if (acc64) {
-    stde_reduce_kernel<float, double><<<blocks, threads, 0, st>>>((const float*)c0, (const float*)c2, npoints, S,
+    stde_reduce_kernel<float, double><<<blocks, threads, 0, st>>>((const float*)c0, (const float*)c2, (float)scale,
+                                                                  npoints, S,
                                                                   (const float*)cv, (float)trace, control,
                                                                   (ech_estimator_result*)results);
   } else {
-    stde_reduce_kernel<float, float><<<blocks, threads, 0, st>>>((const float*)c0, (const float*)c2, npoints, S,
+    stde_reduce_kernel<float, float><<<blocks, threads, 0, st>>>((const float*)c0, (const float*)c2, (float)scale,
+                                                                 npoints, S,
                                                                  (const float*)cv, (float)trace, control,
                                                                  (ech_estimator_result*)results);
   }

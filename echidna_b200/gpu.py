@@ -78,6 +78,10 @@ def _check(status: int):
         _raise(status)
 
 
+# WGPU_MAX_BUFFER_BYTES (src/gpu/mod.rs:619): the default chunk budget of the chunked Taylor call.
+WGPU_MAX_BUFFER_BYTES = 128 * 1024 * 1024
+
+
 @dataclass
 class GpuTapeData:
     """Flattened tape for upload (``src/gpu/mod.rs:313-334``), f32 constants."""
@@ -357,6 +361,39 @@ class CudaContext:
                                      batch_size: int) -> TaylorBatchResult:
         k = self.taylor_forward_kth_batch_f64(tape, primal_inputs, direction_seeds, batch_size, 3)
         return TaylorBatchResult(*k.coefficients)
+
+    def taylor_forward_2nd_batch_chunked(self, tape: CudaTapeBuffers, primal_inputs, direction_seeds,
+                                         batch_size: int, num_inputs: int, num_variables: int,
+                                         max_buffer_bytes: int = WGPU_MAX_BUFFER_BYTES) -> TaylorBatchResult:
+        """``taylor_forward_2nd_batch_chunked`` (``src/gpu/mod.rs:652-733``): the same chunk
+        size rule (jets working buffer of ``num_variables * 3 * 4`` bytes per element, the
+        65535 x 256 dispatch cap and the u32 index cap), each chunk one K=3 sweep."""
+        if batch_size == 0:
+            e = np.zeros(0, np.float32)
+            return TaylorBatchResult(e, e.copy(), e.copy())
+        per = int(num_variables) * 3 * 4
+        if per == 0:
+            raise GpuError("num_variables is zero")
+        chunk = int(max_buffer_bytes) // per
+        if chunk == 0:
+            raise GpuError(f"max_buffer_bytes ({max_buffer_bytes}) too small for a single element "
+                           f"({per} bytes per element)")
+        chunk = min(chunk, 65535 * 256, 0xFFFFFFFF // (int(num_variables) * 3))
+        p = _arr(primal_inputs, np.float32)
+        s = _arr(direction_seeds, np.float32)
+        if batch_size <= chunk:
+            return self.taylor_forward_2nd_batch(tape, p, s, batch_size)
+        ni = int(num_inputs)
+        vals, c1s, c2s = [], [], []
+        off = 0
+        while off < batch_size:
+            n = min(chunk, batch_size - off)
+            r = self.taylor_forward_2nd_batch(tape, p[off * ni:(off + n) * ni], s[off * ni:(off + n) * ni], n)
+            vals.append(r.values)
+            c1s.append(r.c1s)
+            c2s.append(r.c2s)
+            off += n
+        return TaylorBatchResult(np.concatenate(vals), np.concatenate(c1s), np.concatenate(c2s))
 
     # -- sparse drop-ins (src/gpu/cuda_backend.rs:306-441) ---------------------
     def sparse_jacobian(self, tape: CudaTapeBuffers, tape_cpu: BytecodeTape, x):

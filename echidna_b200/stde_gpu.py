@@ -85,3 +85,17 @@ def laplacian_batch(backend: CudaContext, tape, xs, num_directions: int, directi
     for i in range(B):
         out[i] = (res[i].value, res[i].estimate, res[i].sample_variance, res[i].standard_error, res[i].num_samples)
     return out
+
+
+def diagonal_kth_order_stochastic_gpu(backend: CudaContext, tape, x, k: int, sampled_indices) -> EstimatorResult:
+    """``stde::diagonal_kth_order_stochastic`` (``src/stde/higher_order.rs:173-227``) on the GPU:
+    ``n * mean_j(k! * c_k)`` over jets along ``e_j`` for the sampled coordinates (k = 2..4)."""
+    lib = _lib.load()
+    f64 = bool(tape.f64)
+    dt = np.float64 if f64 else np.float32
+    xx = np.ascontiguousarray(x, dtype=dt).ravel()
+    idx = np.ascontiguousarray(sampled_indices, dtype=np.uint32).ravel()
+    r = _lib.EstimatorResultC()
+    fn = lib.ech_diagonal_kth_order_stochastic_f64 if f64 else lib.ech_diagonal_kth_order_stochastic_f32
+    _check(fn(backend._h, tape._h, _lib.ptr(xx), xx.size, int(k), _lib.ptr(idx), idx.size, ctypes.byref(r)))
+    return _result(r, float)

@@ -215,6 +215,45 @@ ECH_API size_t ech_noalloc_region_bytes(void);
 ECH_API ech_status ech_gradient_batch_device_noalloc(ech_ctx* ctx, const ech_tape* tape, int f64, const void* inputs,
                                                      uint32_t batch_size, void* outputs, void* grads, void* stream);
 
+/* Extension: stde::diagonal_kth_order_stochastic (src/stde/higher_order.rs:173-227)
+ * on the GPU: one jet of order k+1 along e_j per sampled index j, samples k!*c_k,
+ * Welford in the sample type, estimate / variance / SE rescaled by n, n^2, n.
+ * k in 2..=4 (jets up to order 5).  Errors use the reference's texts
+ * ("sampled_indices must not be empty", "k must be >= 2 (use gradient for k=1)",
+ * "sampled index {j} out of bounds (n={n})"); scalar-output tapes only. */
+ECH_API ech_status ech_diagonal_kth_order_stochastic_f32(ech_ctx* ctx, const ech_tape* tape, const float* x, size_t n,
+                                                         uint32_t k, const uint32_t* sampled_indices,
+                                                         size_t n_indices, ech_estimator_result* out);
+ECH_API ech_status ech_diagonal_kth_order_stochastic_f64(ech_ctx* ctx, const ech_tape* tape, const double* x,
+                                                         size_t n, uint32_t k, const uint32_t* sampled_indices,
+                                                         size_t n_indices, ech_estimator_result* out);
+
+/* ── structural sparsity and coloring (host only, no device needed) ──────────
+ * Used by the sparse Jacobian / Hessian drop-ins (src/gpu/cuda_backend.rs:306-441),
+ * which seed the tangent / HVP sweeps with one row per color.  Two-call
+ * pattern: with rows == cols == NULL and cap == 0 only *nnz is set.
+ * BytecodeTape::detect_sparsity (src/bytecode_tape/sparse.rs:463-593): the
+ * lower triangle (row >= col) of the Hessian pattern, sorted by (row, col). */
+ECH_API ech_status ech_detect_hessian_sparsity(const uint32_t* opcodes, const uint32_t* arg0, const uint32_t* arg1,
+                                               uint32_t num_variables, uint32_t num_inputs, uint32_t* rows,
+                                               uint32_t* cols, size_t cap, size_t* nnz);
+/* BytecodeTape::detect_jacobian_sparsity (src/bytecode_tape/sparse.rs:716-776):
+ * (output row, input col) in output order, columns ascending. */
+ECH_API ech_status ech_detect_jacobian_sparsity(const uint32_t* opcodes, const uint32_t* arg0, const uint32_t* arg1,
+                                                uint32_t num_variables, uint32_t num_inputs,
+                                                const uint32_t* output_indices, uint32_t n_outputs, uint32_t* rows,
+                                                uint32_t* cols, size_t cap, size_t* nnz);
+/* sparse::greedy_coloring (src/sparse.rs:57-98): distance-2 coloring of the
+ * Hessian pattern; colors[dim]. */
+ECH_API ech_status ech_greedy_coloring(uint32_t dim, const uint32_t* rows, const uint32_t* cols, size_t nnz,
+                                       uint32_t* colors, uint32_t* num_colors);
+/* sparse::column_coloring / row_coloring (src/sparse.rs:292-316): colors[num_inputs]
+ * / colors[num_outputs] of the Jacobian pattern's intersection graph. */
+ECH_API ech_status ech_column_coloring(uint32_t num_outputs, uint32_t num_inputs, const uint32_t* rows,
+                                       const uint32_t* cols, size_t nnz, uint32_t* colors, uint32_t* num_colors);
+ECH_API ech_status ech_row_coloring(uint32_t num_outputs, uint32_t num_inputs, const uint32_t* rows,
+                                    const uint32_t* cols, size_t nnz, uint32_t* colors, uint32_t* num_colors);
+
 /* ── introspection ────────────────────────────────────────────────────────── */
 /* kind: 0 forward, 1 gradient, 2 hvp, 3 tangent, 4 taylor(order).  Fills
  * stats[12]: fwd_ops, rev_ops, max_live_fwd, max_live_rev, traj_values,

@@ -181,3 +181,47 @@ def test_laplacian_batch_device_rng_statistics(ctx):
         tr = np.trace(H)
         z = (res["estimate"][b] - tr) / max(res["standard_error"][b], 1e-300)
         assert abs(z) < 5.0, (b, res["estimate"][b], tr, res["standard_error"][b])
+
+
+def test_taylor_2nd_chunked_matches_single_dispatch(ctx):
+    # src/gpu/mod.rs:652-733: a buffer budget of 3 elements forces 4 chunks for 10 points
+    tape, _ = record(rosenbrock_2, [1.0, 2.0])
+    gt = ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(tape))
+    rng = np.random.default_rng(11)
+    P = rng.uniform(-1, 1, size=(10, 2)).astype(np.float32)
+    S = rng.normal(size=(10, 2)).astype(np.float32)
+    nv = len(tape.opcodes)
+    whole = ctx.taylor_forward_2nd_batch(gt, P, S, 10)
+    chunked = ctx.taylor_forward_2nd_batch_chunked(gt, P, S, 10, 2, nv, max_buffer_bytes=3 * nv * 12)
+    for a, b in ((whole.values, chunked.values), (whole.c1s, chunked.c1s), (whole.c2s, chunked.c2s)):
+        assert np.array_equal(a, b)
+    with pytest.raises(GpuError, match="too small for a single element"):
+        ctx.taylor_forward_2nd_batch_chunked(gt, P, S, 10, 2, nv, max_buffer_bytes=nv * 12 - 1)
+
+
+@pytest.mark.parametrize("k", [2, 3, 4])
+def test_diagonal_kth_order_stochastic_matches_oracle(ctx, k):
+    # stde/higher_order.rs:173-227 on the GPU vs the oracle restatement, same sampled indices
+    tape = configs.random_dag(8, 400, seed=20 + k)
+    rng = np.random.default_rng(k)
+    x = rng.uniform(-0.8, 0.8, size=8)
+    idx = rng.integers(0, 8, size=12)
+    gt = ctx.upload_tape_f64(tape)
+    got = stde_gpu.diagonal_kth_order_stochastic_gpu(ctx, gt, x, k, idx)
+    ref = OracleTape(tape).diagonal_kth_order_stochastic(x, k, idx)
+    assert got.num_samples == int(ref[4])
+    for j, key in enumerate(("value", "estimate", "sample_variance", "standard_error")):
+        a, b = getattr(got, key), float(ref[j])
+        assert abs(a - b) <= 1e-10 * max(1.0, abs(b)), (key, a, b)
+
+
+def test_diagonal_kth_order_stochastic_errors(ctx):
+    tape = configs.random_dag(4, 50, seed=1)
+    gt = ctx.upload_tape_f64(tape)
+    x = np.zeros(4)
+    with pytest.raises(GpuError, match="sampled_indices must not be empty"):
+        stde_gpu.diagonal_kth_order_stochastic_gpu(ctx, gt, x, 2, [])
+    with pytest.raises(GpuError, match="k must be >= 2"):
+        stde_gpu.diagonal_kth_order_stochastic_gpu(ctx, gt, x, 1, [0])
+    with pytest.raises(GpuError, match="out of bounds"):
+        stde_gpu.diagonal_kth_order_stochastic_gpu(ctx, gt, x, 2, [4])
