@@ -1,25 +1,35 @@
-"""Benchmark: batched BytecodeTape gradient + HVP throughput on B200.
+"""Benchmark: batched BytecodeTape sweeps on B200 (one JSON line on rank 0).
 
-Default workload (the configuration the headline metric is quoted on): the MLP-shaped
-scalar function of 64 inputs (two tanh layers of width 64, W ~ N(0, 1/64), b = 0
-baked in as tape constants, output 0.5*||h||^2; ~25k tape slots), batch 65,536
-points x ~ N(0, I), Rademacher v.  One step = a gradient sweep and a per-point HVP
-sweep over the whole batch, FP32 (the throughput precision of that configuration).
+Workloads (``--workload``, default ``mlp``):
+
+* ``mlp`` — the configuration the headline metric is quoted on: the MLP-shaped
+  scalar function of 64 inputs (two tanh layers of width 64, W ~ N(0, 1/64), b = 0
+  baked in as tape constants, output 0.5*||h||^2; ~25k tape slots), 65,536 points
+  x ~ N(0, I), Rademacher v.  One step = a gradient sweep and a per-point HVP sweep
+  over the whole batch, FP32 (the throughput precision of that configuration).
+* ``rosenbrock`` — extended Rosenbrock n=100 (bench-style recording), 1,024 points
+  x ~ U[-2, 2]^100, f64; one step = one forward + gradient sweep.
+* ``stde`` — f(x) = logsumexp(tanh(W x + b)), n=256, W in R^{512x256}; 16,384
+  points, 64 Rademacher directions each from the device RNG, order-3 jets in FP32
+  and a per-point Welford reduction in FP64; one step = one Laplacian batch.
+
+Reported per line:
 
 * ``value``: points/s with inputs resident in HBM (device-pointer C ABI calls),
-  CUDA events on the launching stream, L2 flushed between steps.
-* ``e2e``: the same step through the host-buffer C ABI (ech_gradient_batch_f32 +
-  ech_hvp_batch_points_f32): host->device copies of the inputs and device->host
-  copies of the results are inside the timed region.
-* ``roofline``: the dominant sweep kernel, algorithmic bytes per launch from the
-  tape (``s*(2ni+no) + 2s*T_val`` per point for the gradient) over its event time.
+  CUDA events on the launching stream, L2 flushed between steps (256 MiB write
+  outside the timed events).
+* ``e2e``: the same step through the host-buffer C ABI: host->device copies of the
+  inputs and device->host copies of the results are inside the timed region.
+* ``roofline``: the dominant kernel's algorithmic bytes per launch (the
+  store-all model, from the tape) over its event time, against the measured HBM
+  copy bandwidth; the scalar op rate is reported beside it.
 * ``cpu_baseline``: the oracle (the reference's CPU sweeps restated in C++) on a
   bounded sample of the same workload, on all host cores.
 
 ``--impl reference`` times that CPU implementation alone as the reference arm.
-Multi-GPU (torchrun): the global batch is world * 65,536 points and every rank
-evaluates its own contiguous 65,536-point shard (points are independent, no
-collective on the data path); timing is the max over ranks.
+Multi-GPU (torchrun): the global batch is world x (per-GPU batch) points and every
+rank evaluates its own contiguous shard (points are independent, no collective
+on the data path); timing is the max over ranks.
 """
 from __future__ import annotations
 
@@ -39,8 +49,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "grad/HVP/Laplacian points/s (% roofline); time to 1% STDE error, learned vs plain"
 UNIT = "points/s"
-BATCH = 65536
-N_IN = 64
+L2_FLUSH_BYTES = 256 * 1024 * 1024
 
 
 def _peaks():
@@ -68,7 +77,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
@@ -106,60 +115,279 @@ class ClockSampler:
                 "samples": len(mhz)}
 
 
-def _workload(dtype, rank=0, world=1):
-    """The tape and this rank's shard of the global batch (world * 65,536 points)."""
-    from echidna_b200 import configs
-    from echidna_b200.multi import rank_rows
-    tape = configs.mlp(N_IN, 64, dtype=np.float64)
-    seed = configs.SEEDS["mlp"]
-    n = world * BATCH
-    X = rank_rows(n, rank, world, seed, N_IN, lambda g, s: g.normal(size=s))
-    V = rank_rows(n, rank, world, seed + 1, N_IN, lambda g, s: g.choice([-1.0, 1.0], size=s))
-    return tape, X.astype(dtype), V.astype(dtype)
+# ───────────────────────────── workloads ─────────────────────────────────────
+
+def _pinned(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
 
 
-def cpu_reference(tape, X, V, budget_s: float, nthreads: int):
-    """Oracle gradient + HVP (f64, the reference's CPU path) on a bounded sample."""
-    from oracle.oracle import OracleTape
-    o = OracleTape(tape)
-    Xd = X.astype(np.float64)
-    Vd = V.astype(np.float64)
+class MlpWorkload:
+    name = "mlp"
+    batch = 65536
     n = 64
-    t0 = time.perf_counter()
-    o.gradient(Xd[:n], nthreads)
-    o.hvp(Xd[:n], Vd[:n], nthreads)
-    dt = time.perf_counter() - t0
-    n = int(min(len(Xd), max(n, n * budget_s / max(dt, 1e-6))))
-    t0 = time.perf_counter()
-    o.gradient(Xd[:n], nthreads)
-    o.hvp(Xd[:n], Vd[:n], nthreads)
-    dt = time.perf_counter() - t0
-    return n / dt, n, dt
+    launches_per_step = 2
 
+    def __init__(self, rank, world):
+        from echidna_b200 import configs
+        from echidna_b200.multi import rank_rows
+        self.tape = configs.mlp(self.n, 64, dtype=np.float64)
+        seed = configs.SEEDS["mlp"]
+        total = world * self.batch
+        self.X = rank_rows(total, rank, world, seed, self.n, lambda g, s: g.normal(size=s)).astype(np.float32)
+        self.V = rank_rows(total, rank, world, seed + 1, self.n,
+                           lambda g, s: g.choice([-1.0, 1.0], size=s)).astype(np.float32)
+
+    def describe(self):
+        return {"workload": "mlp n=64 width=64 (~25k-slot tape): gradient + per-point HVP, Rademacher v",
+                "batch_per_gpu": self.batch}, "f32"
+
+    def setup(self, ctx, lib, torch, sp):
+        from echidna_b200.gpu import GpuTapeData
+        self.ctx, self.lib, self.sp = ctx, lib, sp
+        self.gt = ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(self.tape))
+        B, n = self.batch, self.n
+        self.dX = torch.from_numpy(self.X).cuda()
+        self.dV = torch.from_numpy(self.V).cuda()
+        self.d_out = torch.empty(B, device="cuda")
+        self.d_g = torch.empty(B * n, device="cuda")
+        self.d_g2 = torch.empty(B * n, device="cuda")
+        self.d_h = torch.empty(B * n, device="cuda")
+        self.hX, self.hV = _pinned(torch, self.X), _pinned(torch, self.V)
+        self.ho = _pinned(torch, np.empty(B, np.float32))
+        self.hg = _pinned(torch, np.empty(B * n, np.float32))
+        self.hg2 = _pinned(torch, np.empty(B * n, np.float32))
+        self.hh = _pinned(torch, np.empty(B * n, np.float32))
+
+    def kernels(self):
+        from echidna_b200 import _lib
+        lib, ctx, gt, sp = self.lib, self.ctx, self.gt, self.sp
+
+        def grad():
+            st = lib.ech_gradient_batch_device(ctx._h, gt._h, 0, self.dX.data_ptr(), self.batch,
+                                               self.d_out.data_ptr(), self.d_g.data_ptr(), sp)
+            assert st == 0, _lib.last_error()
+
+        def hvp():
+            st = lib.ech_hvp_batch_device(ctx._h, gt._h, 0, self.dX.data_ptr(), 1, self.dV.data_ptr(), self.batch,
+                                          self.d_g2.data_ptr(), self.d_h.data_ptr(), sp)
+            assert st == 0, _lib.last_error()
+        return [("gradient sweep", grad), ("hvp sweep", hvp)]
+
+    def e2e_step(self):
+        from echidna_b200 import _lib
+        lib, ctx, gt, P, B = self.lib, self.ctx, self.gt, _lib.ptr, self.batch
+        st = lib.ech_gradient_batch_f32(ctx._h, gt._h, P(self.hX), self.hX.size, B, P(self.ho), self.ho.size,
+                                        P(self.hg), self.hg.size)
+        assert st == 0, _lib.last_error()
+        st = lib.ech_hvp_batch_points_f32(ctx._h, gt._h, P(self.hX), self.hX.size, P(self.hV), self.hV.size, B,
+                                          P(self.hg2), self.hg2.size, P(self.hh), self.hh.size)
+        assert st == 0, _lib.last_error()
+
+    def io_bytes(self):
+        return (int(self.hX.nbytes * 2 + self.hV.nbytes),
+                int(self.ho.nbytes + self.hg.nbytes + self.hg2.nbytes + self.hh.nbytes))
+
+    def roofline_inputs(self, kernel):
+        s, ni, no, B = 4, self.n, 1, self.batch
+        if kernel == "gradient sweep":
+            st = self.ctx.plan_stats(self.gt, "gradient")
+            return B * (s * (2 * ni + no) + 2 * s * st["traj_values"]), B * (st["flops_fwd"] + st["flops_rev"])
+        st = self.ctx.plan_stats(self.gt, "hvp")
+        return B * (s * (4 * ni + no) + 2 * s * 2 * st["traj_values"]), B * 4 * (st["flops_fwd"] + st["flops_rev"])
+
+    def detail(self):
+        return {"plan_gradient": self.ctx.plan_stats(self.gt, "gradient"),
+                "plan_hvp": self.ctx.plan_stats(self.gt, "hvp"),
+                "shape_gradient": self.ctx.launch_shape(self.gt, "gradient", self.batch),
+                "shape_hvp": self.ctx.launch_shape(self.gt, "hvp", self.batch)}
+
+    def cpu_reference(self, budget_s, nthreads):
+        from oracle.oracle import OracleTape
+        o = OracleTape(self.tape)
+        Xd, Vd = self.X.astype(np.float64), self.V.astype(np.float64)
+        n = 64
+        t0 = time.perf_counter()
+        o.gradient(Xd[:n], nthreads)
+        o.hvp(Xd[:n], Vd[:n], nthreads)
+        dt = time.perf_counter() - t0
+        n = int(min(len(Xd), max(n, n * budget_s / max(dt, 1e-6))))
+        t0 = time.perf_counter()
+        o.gradient(Xd[:n], nthreads)
+        o.hvp(Xd[:n], Vd[:n], nthreads)
+        dt = time.perf_counter() - t0
+        return n / dt, f"{n} points of the batch: oracle gradient + per-point HVP (f64), {dt:.1f} s"
+
+
+class RosenbrockWorkload:
+    name = "rosenbrock"
+    batch = 1024
+    n = 100
+    launches_per_step = 1
+
+    def __init__(self, rank, world):
+        from echidna_b200 import configs
+        from echidna_b200.multi import rank_rows
+        self.tape = configs.rosenbrock(self.n)
+        self.X = rank_rows(world * self.batch, rank, world, configs.SEEDS["rosenbrock"], self.n,
+                           lambda g, s: g.uniform(-2.0, 2.0, size=s))
+
+    def describe(self):
+        return {"workload": "extended Rosenbrock n=100 (1,091-slot tape): forward value + gradient",
+                "batch_per_gpu": self.batch}, "f64"
+
+    def setup(self, ctx, lib, torch, sp):
+        self.ctx, self.lib, self.sp = ctx, lib, sp
+        self.gt = ctx.upload_tape_f64(self.tape)
+        B, n = self.batch, self.n
+        self.dX = torch.from_numpy(self.X).cuda()
+        self.d_out = torch.empty(B, dtype=torch.float64, device="cuda")
+        self.d_g = torch.empty(B * n, dtype=torch.float64, device="cuda")
+        self.hX = _pinned(torch, self.X)
+        self.ho = _pinned(torch, np.empty(B))
+        self.hg = _pinned(torch, np.empty(B * n))
+
+    def kernels(self):
+        from echidna_b200 import _lib
+
+        def grad():
+            st = self.lib.ech_gradient_batch_device(self.ctx._h, self.gt._h, 1, self.dX.data_ptr(), self.batch,
+                                                    self.d_out.data_ptr(), self.d_g.data_ptr(), self.sp)
+            assert st == 0, _lib.last_error()
+        return [("gradient sweep", grad)]
+
+    def e2e_step(self):
+        from echidna_b200 import _lib
+        P = _lib.ptr
+        st = self.lib.ech_gradient_batch_f64(self.ctx._h, self.gt._h, P(self.hX), self.hX.size, self.batch,
+                                             P(self.ho), self.ho.size, P(self.hg), self.hg.size)
+        assert st == 0, _lib.last_error()
+
+    def io_bytes(self):
+        return int(self.hX.nbytes), int(self.ho.nbytes + self.hg.nbytes)
+
+    def roofline_inputs(self, kernel):
+        st = self.ctx.plan_stats(self.gt, "gradient")
+        s, B = 8, self.batch
+        return B * (s * (2 * self.n + 1) + 2 * s * st["traj_values"]), B * (st["flops_fwd"] + st["flops_rev"])
+
+    def detail(self):
+        return {"plan_gradient": self.ctx.plan_stats(self.gt, "gradient"),
+                "shape_gradient": self.ctx.launch_shape(self.gt, "gradient", self.batch)}
+
+    def cpu_reference(self, budget_s, nthreads):
+        from oracle.oracle import OracleTape
+        o = OracleTape(self.tape)
+        reps, t0 = 0, time.perf_counter()
+        while True:
+            o.gradient(self.X, nthreads)
+            reps += 1
+            dt = time.perf_counter() - t0
+            if dt >= budget_s or reps >= 100000:
+                break
+        return reps * self.batch / dt, f"{reps} x {self.batch} points: oracle forward + gradient (f64), {dt:.1f} s"
+
+
+class StdeWorkload:
+    name = "stde"
+    batch = 16384
+    n = 256
+    S = 64
+    launches_per_step = 2
+
+    def __init__(self, rank, world):
+        from echidna_b200 import configs
+        from echidna_b200.multi import rank_rows
+        self.tape = configs.logsumexp_tanh(self.n, 512)
+        self.seed = configs.SEEDS["logsumexp_tanh"]
+        self.X = rank_rows(world * self.batch, rank, world, self.seed, self.n,
+                           lambda g, s: g.normal(size=s)).astype(np.float32)
+
+    def describe(self):
+        return {"workload": "STDE Laplacian: logsumexp(tanh(Wx+b)), n=256, W 512x256 (~395k-slot tape), "
+                            "S=64 device-RNG Rademacher directions, order-3 jets (FP32), FP64 Welford",
+                "batch_per_gpu": self.batch, "directions": self.S}, "f32"
+
+    def setup(self, ctx, lib, torch, sp):
+        from echidna_b200 import _lib
+        from echidna_b200.gpu import GpuTapeData
+        self.ctx, self.lib, self.sp = ctx, lib, sp
+        self.gt = ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(self.tape))
+        self.dX = torch.from_numpy(self.X).cuda()
+        self.d_res = torch.empty(self.batch * 5, dtype=torch.float64, device="cuda")
+        self.hX = _pinned(torch, self.X)
+        self.h_res = (_lib.EstimatorResultC * self.batch)()
+
+    def kernels(self):
+        from echidna_b200 import _lib
+
+        def lap():
+            st = self.lib.ech_laplacian_batch_device(self.ctx._h, self.gt._h, 0, self.dX.data_ptr(), self.batch, None,
+                                                     self.S, 2, self.seed, self.d_res.data_ptr(), self.sp)
+            assert st == 0, _lib.last_error()
+        return [("taylor-3 sweep + reduction", lap)]
+
+    def e2e_step(self):
+        from echidna_b200 import _lib
+        st = self.lib.ech_laplacian_batch_f32(self.ctx._h, self.gt._h, _lib.ptr(self.hX), self.hX.size, self.batch,
+                                              None, 0, self.S, 2, self.seed, self.h_res)
+        assert st == 0, _lib.last_error()
+
+    def io_bytes(self):
+        return int(self.hX.nbytes), int(self.batch * 40)
+
+    def roofline_inputs(self, kernel):
+        st = self.ctx.plan_stats(self.gt, "taylor", 3)
+        s, K = 4, 3
+        units = self.batch * self.S
+        # per unit: x amortised over the S directions, no direction bytes (device RNG), K coefficients out
+        return int(units * s * (self.n / self.S + K)), units * st["flops_fwd"]
+
+    def detail(self):
+        return {"plan_taylor3": self.ctx.plan_stats(self.gt, "taylor", 3),
+                "shape_taylor3": self.ctx.launch_shape(self.gt, "taylor", self.batch * self.S, 3)}
+
+    def cpu_reference(self, budget_s, nthreads):
+        from oracle.oracle import OracleTape
+        o = OracleTape(self.tape)
+        rng = np.random.default_rng(self.seed)
+        dirs = rng.choice([-1.0, 1.0], size=(self.S, self.n))
+        Xd = self.X.astype(np.float64)
+        n = 4
+        t0 = time.perf_counter()
+        o.laplacian_stats_batch(Xd[:n], dirs, nthreads)
+        dt = time.perf_counter() - t0
+        n = int(min(len(Xd), max(n, n * budget_s / max(dt, 1e-6))))
+        t0 = time.perf_counter()
+        o.laplacian_stats_batch(Xd[:n], dirs, nthreads)
+        dt = time.perf_counter() - t0
+        return n / dt, f"{n} points x 64 directions: oracle stde::laplacian per point (f64), {dt:.1f} s"
+
+
+WORKLOADS = {"mlp": MlpWorkload, "rosenbrock": RosenbrockWorkload, "stde": StdeWorkload}
+
+
+# ───────────────────────────── arms ──────────────────────────────────────────
 
 def run_reference(args):
     """Reference arm: the reference's CPU implementation (C++ restatement) alone."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from oracle import oracle as orc
-    tape, X, V = _workload(np.float32)
+    wl = WORKLOADS[args.workload](0, 1)
     nth = os.cpu_count() or 1
-    vals = []
     for _ in range(args.warmup):
-        cpu_reference(tape, X, V, 0.5, nth)
+        wl.cpu_reference(0.3, nth)
+    vals, sample = [], ""
     for _ in range(args.steps):
-        v, n, dt = cpu_reference(tape, X, V, 3.0, nth)
+        v, sample = wl.cpu_reference(3.0, nth)
         vals.append(v)
     value = float(np.median(vals))
+    cfg, _ = wl.describe()
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
-        "data": "synthetic", "scaling": "weak", "vs_baseline": None,
-        "config": {"workload": "mlp n=64 width=64 (~25k-slot tape), gradient+HVP per point, batch 65536",
-                   "batch": BATCH},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port",
-                         "sample": f"{n} points of the batch per step, oracle gradient + per-point HVP (f64)"},
+        "data": "synthetic", "scaling": "weak", "vs_baseline": None, "config": cfg,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -172,6 +400,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--workload", default="mlp", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -181,7 +410,7 @@ def main():
     import torch
     import torch.distributed as dist
     from echidna_b200 import _lib
-    from echidna_b200.gpu import CudaContext, GpuTapeData
+    from echidna_b200.gpu import CudaContext
     from echidna_b200.multi import max_over_ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -195,33 +424,19 @@ def main():
     ctx = CudaContext.new(local)
     assert ctx is not None, "no CUDA device"
 
-    tape, X, V = _workload(np.float32, rank, world)
-    gt = ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(tape))
+    wl = WORKLOADS[args.workload](rank, world)
     # a dedicated stream: the events below and the engine's launches must share it
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
     assert sp != 0
-    dX = torch.from_numpy(X).cuda()
-    dV = torch.from_numpy(V).cuda()
-    d_out = torch.empty(BATCH, device="cuda")
-    d_g = torch.empty(BATCH * N_IN, device="cuda")
-    d_g2 = torch.empty(BATCH * N_IN, device="cuda")
-    d_h = torch.empty(BATCH * N_IN, device="cuda")
-    flush = torch.empty(256 * 1024 * 1024 // 4, device="cuda")
-
-    def grad():
-        st = lib.ech_gradient_batch_device(ctx._h, gt._h, 0, dX.data_ptr(), BATCH, d_out.data_ptr(), d_g.data_ptr(), sp)
-        assert st == 0, _lib.last_error()
-
-    def hvp():
-        st = lib.ech_hvp_batch_device(ctx._h, gt._h, 0, dX.data_ptr(), 1, dV.data_ptr(), BATCH, d_g2.data_ptr(),
-                                      d_h.data_ptr(), sp)
-        assert st == 0, _lib.last_error()
+    wl.setup(ctx, lib, torch, sp)
+    kernels = wl.kernels()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, device="cuda")
 
     for _ in range(args.warmup):
-        grad()
-        hvp()
+        for _, k in kernels:
+            k()
     torch.cuda.synchronize()
     assert lib.ech_ctx_synchronize(ctx._h) == 0, _lib.last_error()
 
@@ -231,107 +446,77 @@ def main():
         torch.cuda.synchronize()
 
     # device-resident timing, per kernel, L2 flushed between steps
-    t_grad, t_hvp = [], []
+    times = {name: [] for name, _ in kernels}
     barrier()
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             flush.zero_()
-            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-            e0.record(stream)
-            grad()
-            e1.record(stream)
-            hvp()
-            e2.record(stream)
-            e2.synchronize()
-            t_grad.append(e0.elapsed_time(e1))
-            t_hvp.append(e1.elapsed_time(e2))
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(kernels) + 1)]
+            ev[0].record(stream)
+            for i, (_, k) in enumerate(kernels):
+                k()
+                ev[i + 1].record(stream)
+            ev[-1].synchronize()
+            for i, (name, _) in enumerate(kernels):
+                times[name].append(ev[i].elapsed_time(ev[i + 1]))
         barrier()
     assert lib.ech_ctx_synchronize(ctx._h) == 0, _lib.last_error()
-    step_ms = float(np.sum(t_grad) + np.sum(t_hvp)) / args.steps
+    step_ms = float(sum(np.sum(v) for v in times.values())) / args.steps
     if world > 1:
         step_ms = max_over_ranks(step_ms, "cuda")
 
     # end-to-end through the host-buffer ABI (pinned host buffers)
-    hX = torch.from_numpy(X).pin_memory().numpy()
-    hV = torch.from_numpy(V).pin_memory().numpy()
-    ho = torch.empty(BATCH, pin_memory=True).numpy()
-    hg = torch.empty(BATCH * N_IN, pin_memory=True).numpy()
-    hg2 = torch.empty(BATCH * N_IN, pin_memory=True).numpy()
-    hh = torch.empty(BATCH * N_IN, pin_memory=True).numpy()
-    P = _lib.ptr
-
-    def e2e_step():
-        st = lib.ech_gradient_batch_f32(ctx._h, gt._h, P(hX), hX.size, BATCH, P(ho), ho.size, P(hg), hg.size)
-        assert st == 0, _lib.last_error()
-        st = lib.ech_hvp_batch_points_f32(ctx._h, gt._h, P(hX), hX.size, P(hV), hV.size, BATCH, P(hg2), hg2.size,
-                                          P(hh), hh.size)
-        assert st == 0, _lib.last_error()
-
-    e2e_step()
+    wl.e2e_step()
     barrier()
     e2e_ms = []
     for _ in range(max(3, args.steps // 2)):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        e2e_step()
+        wl.e2e_step()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e_step_ms = float(np.median(e2e_ms))
     if world > 1:
         e2e_step_ms = max_over_ranks(e2e_step_ms, "cuda")
 
     # roofline of the dominant kernel
-    sg = ctx.plan_stats(gt, "gradient")
-    sh = ctx.plan_stats(gt, "hvp")
-    s = 4
-    ni, no = N_IN, 1
-    grad_bytes = BATCH * (s * (2 * ni + no) + 2 * s * sg["traj_values"])
-    hvp_bytes = BATCH * (s * (4 * ni + no) + 2 * s * 2 * sh["traj_values"])
-    g_ms = float(np.mean(t_grad))
-    h_ms = float(np.mean(t_hvp))
-    if g_ms >= h_ms:
-        dom, dom_ms, dom_bytes, dom_flops = "gradient sweep", g_ms, grad_bytes, BATCH * (sg["flops_fwd"] + sg["flops_rev"])
-    else:
-        dom, dom_ms, dom_bytes, dom_flops = "hvp sweep", h_ms, hvp_bytes, BATCH * 4 * (sh["flops_fwd"] + sh["flops_rev"])
+    mean_ms = {name: float(np.mean(v)) for name, v in times.items()}
+    dom = max(mean_ms, key=mean_ms.get)
+    dom_bytes, dom_ops = wl.roofline_inputs(dom)
     peak, peak_kind = _peaks()
+    dom_ms = mean_ms[dom]
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
-            traffic = json.load(f).get(dom)
+            traffic = json.load(f).get(f"{wl.name}:{dom}")
 
-    value = world * BATCH / (step_ms * 1e-3)
-    e2e_value = world * BATCH / (e2e_step_ms * 1e-3)
+    cfg, dtype = wl.describe()
+    cfg.update({"l2": "flushed between steps (256 MiB write outside the events)",
+                "parallelism": f"points sharded, {world} rank(s)"})
+    h2d, d2h = wl.io_bytes()
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic",
-        "config": {"workload": "mlp n=64 width=64 (~25k-slot tape): gradient + per-point HVP, Rademacher v",
-                   "batch_per_gpu": BATCH, "l2": "flushed between steps (256 MiB write outside the events)",
-                   "parallelism": f"points sharded, {world} rank(s)"},
-        "gpu_launches": 2 * args.steps,
+        "metric": METRIC, "value": world * wl.batch / (step_ms * 1e-3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic", "config": cfg,
+        "gpu_launches": wl.launches_per_step * args.steps,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": dom_ms,
-                     "fp32_ops_per_launch": dom_flops, "fp32_tflops": dom_flops / (dom_ms * 1e-3) / 1e12},
-        "e2e": {"value": e2e_value, "unit": UNIT,
-                "h2d_bytes_per_step": int(hX.nbytes * 2 + hV.nbytes),
-                "d2h_bytes_per_step": int(ho.nbytes + hg.nbytes + hg2.nbytes + hh.nbytes)},
+                     "scalar_ops_per_launch": dom_ops, "scalar_tops": dom_ops / (dom_ms * 1e-3) / 1e12},
+        "e2e": {"value": world * wl.batch / (e2e_step_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
         "clocks": clk.summary(),
-        "detail": {"gradient_ms": g_ms, "hvp_ms": h_ms, "gradient_points_per_s": BATCH / (g_ms * 1e-3),
-                   "hvp_points_per_s": BATCH / (h_ms * 1e-3), "plan_gradient": sg, "plan_hvp": sh,
-                   "shape_gradient": ctx.launch_shape(gt, "gradient", BATCH),
-                   "shape_hvp": ctx.launch_shape(gt, "hvp", BATCH)},
+        "detail": {**{f"{k} ms": v for k, v in mean_ms.items()}, **wl.detail()},
     }
     if rank == 0 and not args.no_cpu_baseline:
         nth = os.cpu_count() or 1
-        v, n, dt = cpu_reference(tape, X, V, 10.0, nth)
-        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nth, "kind": "port",
-                                "sample": f"{n} points: oracle gradient + per-point HVP (f64), {dt:.1f} s"}
+        v, sample = wl.cpu_reference(10.0, nth)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    del gt
+    del wl
     ctx.close()
     if world > 1:
         dist.destroy_process_group()

@@ -929,6 +929,31 @@ static ech_status do_laplacian_batch(ech_ctx* ctx, const ech_tape* tc, const T* 
   return check_err_word(ctx);
 }
 
+ECH_API ech_status ech_laplacian_batch_device(ech_ctx* ctx, const ech_tape* tc, int f64, const void* xs, uint32_t B,
+                                              const void* dirs, uint32_t S, int dir_mode, uint64_t seed,
+                                              ech_estimator_result* results, void* stream) {
+  CHECK(common_checks(ctx, tc, f64 != 0));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(stde_checks(t, t->host.ni, "laplacian_batch", "Laplacian"));
+  CHECK(batch_args(t, B));
+  if (S == 0) return fail(ECH_ERR_OTHER, "no directions provided");
+  if (dir_mode < 0 || dir_mode > 2) return fail(ECH_ERR_INVALID_ARG, "dir_mode must be 0, 1 or 2");
+  if (!xs || !results || (dir_mode != 2 && !dirs)) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  cudaStream_t saved = ctx->stream;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->stream;  // stde_run enqueues on the context's stream
+  ech_status s;
+  if (f64)
+    s = stde_run<double>(ctx, t, (const double*)xs, false, B, S, (const double*)dirs, dir_mode, seed, true, nullptr,
+                         0.0, 0, results, nullptr, nullptr);
+  else
+    s = stde_run<float>(ctx, t, (const float*)xs, false, B, S, (const float*)dirs, dir_mode, seed, true, nullptr, 0.0,
+                        0, results, nullptr, nullptr);
+  ctx->stream = saved;
+  return s;
+}
+
 ECH_API ech_status ech_laplacian_batch_f32(ech_ctx* ctx, const ech_tape* t, const float* xs, size_t n_xs, uint32_t B,
                                            const float* dirs, size_t n_dirs, uint32_t S, int dir_mode, uint64_t seed,
                                            ech_estimator_result* res) {

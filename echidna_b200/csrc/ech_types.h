@@ -97,6 +97,7 @@ enum DOp : uint8_t {
   D_ADD_RR = 72, D_ADD_IR, D_ADD_RI, D_SUB_RR, D_SUB_IR, D_SUB_RI,
   D_MUL_RR, D_MUL_IR, D_MUL_RI, D_DIV_RR, D_DIV_IR, D_DIV_RI,  // .. 83
   D_CHAIN = 69,     // fused linear chain (forward and reverse)
+  D_CHAIN_LC = 70,  // fused chain whose terms are all c*x or x*c added to the running value
   D_FU_BASE = 96,   // forward unary fast form: 96 + (op - OP_NEG), a and dst smem
   D_RF_BASE = 128,  // reverse fast form: 128 + op, every adjoint location in smem
 };

@@ -413,6 +413,45 @@ template <class V, int P> struct FwdExec {
     }
   }
 
+  // Linear-combination chain: every term is Mul(c, x) or Mul(x, c) added to the
+  // running value, in tape order; two terms per iteration so their operand
+  // loads overlap.
+  __device__ __forceinline__ void chain_lc(uint32_t ma, uint32_t ao, double imm, uint32_t first, uint32_t n,
+                                           V (&acc)[P]) const {
+    ld(ma, ao, imm, acc);
+    const uint4* tp = reinterpret_cast<const uint4*>(kp.fterms + first);
+    uint32_t q = 0;
+#pragma unroll 1
+    for (; q + 2 <= n; q += 2) {
+      const uint4 a0 = __ldg(tp + 2 * q);
+      const uint2 a1 = __ldg(reinterpret_cast<const uint2*>(tp + 2 * q + 1));
+      const uint4 b0 = __ldg(tp + 2 * q + 2);
+      const uint2 b1 = __ldg(reinterpret_cast<const uint2*>(tp + 2 * q + 3));
+      V xa[P], xb[P];
+      ldv((a0.x >> 16) & 0xFFu, a0.y, xa);
+      ldv((b0.x >> 16) & 0xFFu, b0.y, xb);
+      const V ca = dm::VT<V>::cst(__hiloint2double((int)a1.y, (int)a1.x));
+      const V cb = dm::VT<V>::cst(__hiloint2double((int)b1.y, (int)b1.x));
+      const bool a_cx = (a0.x & 0xFFu) == CK_CX, b_cx = (b0.x & 0xFFu) == CK_CX;
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        const V ta = a_cx ? Kd::mul(ca, xa[p]) : Kd::mul(xa[p], ca);
+        const V tb = b_cx ? Kd::mul(cb, xb[p]) : Kd::mul(xb[p], cb);
+        acc[p] = Kd::add(Kd::add(acc[p], ta), tb);
+      }
+    }
+    if (q < n) {
+      const uint4 a0 = __ldg(tp + 2 * q);
+      const uint2 a1 = __ldg(reinterpret_cast<const uint2*>(tp + 2 * q + 1));
+      V xa[P];
+      ldv((a0.x >> 16) & 0xFFu, a0.y, xa);
+      const V ca = dm::VT<V>::cst(__hiloint2double((int)a1.y, (int)a1.x));
+      const bool a_cx = (a0.x & 0xFFu) == CK_CX;
+#pragma unroll
+      for (int p = 0; p < P; ++p) acc[p] = Kd::add(acc[p], a_cx ? Kd::mul(ca, xa[p]) : Kd::mul(xa[p], ca));
+    }
+  }
+
   __device__ __forceinline__ void operator()(const unsigned char* raw) const {
     const uint4 w0 = *reinterpret_cast<const uint4*>(raw);
     const uint4 w1 = *reinterpret_cast<const uint4*>(raw + 16);
@@ -438,6 +477,10 @@ template <class V, int P> struct FwdExec {
         return;
       case D_CHAIN:
         chain((w0.x >> 8) & 0xFFu, ao, imm, bo, (uint32_t)aux, r);
+        put(w0.x >> 24, dof, save, r);
+        return;
+      case D_CHAIN_LC:
+        chain_lc((w0.x >> 8) & 0xFFu, ao, imm, bo, (uint32_t)aux, r);
         put(w0.x >> 24, dof, save, r);
         return;
 #define ECH_FB(NAME, FN)                                                     \
@@ -606,6 +649,36 @@ template <class V, int P> struct RevExec {
     }
   }
 
+  // Reverse of a linear-combination chain (every term Mul(c, x) or Mul(x, c),
+  // op acc + term): for t = n..1 the Add (acc side, then the term side), then
+  // the Mul's contribution c * adj(term) to adj(x).  Both Add sides see the
+  // multiplier 1, so the running adjoint and the term's adjoint are the same
+  // value.
+  __device__ __forceinline__ void chain_lc(uint32_t flags, uint32_t ro, uint32_t ao, uint32_t first,
+                                           uint32_t n) const {
+    V adj[P], one[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) one[p] = Kd::c(1);
+    C::ld(loc(flags & RF_R_GLOB, ro), adj);
+    const uint4* tp = reinterpret_cast<const uint4*>(kp.rterms + first);
+#pragma unroll 1
+    for (uint32_t q = n; q-- > 0;) {
+      const uint4 w0 = __ldg(tp + 2 * q);
+      const uint4 w1 = __ldg(tp + 2 * q + 1);
+      const uint32_t tf = w0.x >> 16;
+      if (q == 0 && (flags & RF_HAS_A))
+        accumulate<false>(loc(flags & RF_A_GLOB, ao), (flags & RF_A_INIT) != 0, adj, one);
+      V t[P], c[P];
+      internal(adj, one, t);
+      const V cv = dm::VT<V>::cst(__hiloint2double((int)w1.w, (int)w1.z));
+#pragma unroll
+      for (int p = 0; p < P; ++p) c[p] = cv;
+      accumulate<false>(loc(tf & CF_X_GLOB, w0.y), (tf & CF_X_INIT) != 0, t, c);
+#pragma unroll
+      for (int p = 0; p < P; ++p) adj[p] = t[p];
+    }
+  }
+
   // One reverse op: adj(a) += da * adj(r), adj(b) += db * adj(r) with the
   // zero-adjoint skip and the zero-multiplier guard.  FAST: every adjoint
   // location is in shared memory.
@@ -644,6 +717,9 @@ template <class V, int P> struct RevExec {
       }
       case D_CHAIN:
         chain(flags, ro, ao, w1.x, (uint32_t)aux);
+        return;
+      case D_CHAIN_LC:
+        chain_lc(flags, ro, ao, w1.x, (uint32_t)aux);
         return;
       case D_STGRAD: {
         V g[P];

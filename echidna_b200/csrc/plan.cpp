@@ -821,6 +821,17 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
   return pl;
 }
 
+// A chain whose every term is c*x or x*c added to the running value runs the
+// specialised linear-combination loop (D_CHAIN_LC).
+static bool linear_combination(const Plan& p, uint32_t first, uint32_t n) {
+  if (n == 0) return false;
+  for (uint32_t q = first; q < first + n; ++q) {
+    const PTerm& t = p.terms[q];
+    if ((t.kind != CK_CX && t.kind != CK_XC) || t.op != 0) return false;
+  }
+  return true;
+}
+
 bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out, std::string& err) {
   const uint64_t row = (uint64_t)tile * vbytes;
   bool ok = true;
@@ -852,7 +863,7 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out,
     if (opc == XI_CHAIN) {
       d.b = in.b;  // first term (index into the term tables)
       d.mb = M_NONE;
-      d.opc = D_CHAIN;
+      d.opc = linear_combination(p, in.b, (uint32_t)in.aux) ? D_CHAIN_LC : D_CHAIN;
       out.fwd.push_back(d);
       continue;
     }
@@ -873,7 +884,7 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out,
     d.flags = in.flags;
     d.aux = in.aux;
     if (in.opc == XI_CHAIN) {
-      d.opc = D_CHAIN;
+      d.opc = linear_combination(p, in.va, (uint32_t)in.aux) ? D_CHAIN_LC : D_CHAIN;
       d.r = off(in.r);
       d.a = off(in.a);
       d.b = kNone;

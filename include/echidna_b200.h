@@ -192,6 +192,12 @@ ECH_API ech_status ech_hvp_batch_device(ech_ctx* ctx, const ech_tape* tape, int 
 ECH_API ech_status ech_taylor_batch_device(ech_ctx* ctx, const ech_tape* tape, int f64, const void* primals,
                                            const void* seeds, uint32_t batch_size, uint32_t order,
                                            void* coefficients, void* stream);
+/* Device-pointer form of ech_laplacian_batch_*: xs [B][n], dirs as dir_mode says,
+ * results[B] (device memory). */
+ECH_API ech_status ech_laplacian_batch_device(ech_ctx* ctx, const ech_tape* tape, int f64, const void* xs,
+                                              uint32_t batch_size, const void* dirs, uint32_t num_directions,
+                                              int dir_mode, uint64_t seed, ech_estimator_result* results,
+                                              void* stream);
 /* Waits for the context's stream and reports any device-side error word. */
 ECH_API ech_status ech_ctx_synchronize(ech_ctx* ctx);
 
