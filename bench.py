@@ -12,6 +12,10 @@ Workloads (``--workload``, default ``mlp``):
 * ``stde`` — f(x) = logsumexp(tanh(W x + b)), n=256, W in R^{512x256}; 16,384
   points, 64 Rademacher directions each from the device RNG, order-3 jets in FP32
   and a per-point Welford reduction in FP64; one step = one Laplacian batch.
+* ``uneven`` — 64 different tapes with uneven lengths, input sizes and point
+  counts; one step = gradient + per-point HVP of all of them in one persistent
+  launch (FP32), compared in ``detail`` with one launch per tape and with a
+  CUDA-graph replay of the persistent launch.
 
 Reported per line:
 
@@ -363,7 +367,132 @@ class StdeWorkload:
         return n / dt, f"{n} points x 64 directions: oracle stde::laplacian per point (f64), {dt:.1f} s"
 
 
-WORKLOADS = {"mlp": MlpWorkload, "rosenbrock": RosenbrockWorkload, "stde": StdeWorkload}
+class UnevenWorkload:
+    """64 different tapes (Rosenbrock, Ackley-type, random DAGs of 200-20,000 ops), input
+    sizes 2-512 and 1-100,000 points each: gradient + per-point HVP of all of them in one
+    persistent launch (FP32).  ``detail`` adds one launch per tape and a CUDA-graph replay."""
+    name = "uneven"
+    launches_per_step = 1
+
+    def __init__(self, rank, world):
+        from echidna_b200 import configs
+        self.seed = configs.SEEDS["uneven"]
+        self.suite = configs.uneven_suite(64, self.seed)
+        rng = np.random.default_rng([self.seed, rank])
+        self.data = []
+        for _, tape, n in self.suite:
+            ni = tape.num_inputs
+            self.data.append((rng.uniform(-1.0, 1.0, size=(n, ni)).astype(np.float32),
+                              rng.choice([-1.0, 1.0], size=(n, ni)).astype(np.float32)))
+        self.batch = sum(n for _, _, n in self.suite)
+
+    def describe(self):
+        return {"workload": "uneven batch: 64 tapes (Rosenbrock / Ackley-type / random DAGs 200-20k ops), "
+                            "dims 2-512, 1-100k points each; gradient + per-point HVP in one persistent launch",
+                "points_per_gpu": self.batch, "tapes": len(self.suite)}, "f32"
+
+    def setup(self, ctx, lib, torch, sp):
+        from echidna_b200.gpu import GpuTapeData, MultiTapeHvp
+        self.ctx, self.lib, self.sp, self.torch = ctx, lib, sp, torch
+        self.jobs = []
+        for (_, tape, n), (x, v) in zip(self.suite, self.data):
+            gt = ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(tape))
+            dx, dv = torch.from_numpy(x).cuda(), torch.from_numpy(v).cuda()
+            g, h = torch.empty_like(dx), torch.empty_like(dx)
+            hx, hv = _pinned(torch, x), _pinned(torch, v)
+            hg, hh = _pinned(torch, np.empty_like(x)), _pinned(torch, np.empty_like(x))
+            self.jobs.append((tape, gt, n, dx, dv, g, h, hx, hv, hg, hh))
+        torch.cuda.synchronize()
+        self.multi = MultiTapeHvp(ctx, [(gt, dx.data_ptr(), dv.data_ptr(), n, g.data_ptr(), h.data_ptr())
+                                        for _, gt, n, dx, dv, g, h, *_ in self.jobs], f64=False, autotune=True)
+
+    def kernels(self):
+        return [("multi-tape launch", lambda: self.multi.launch(self.sp))]
+
+    def per_tape(self):
+        from echidna_b200 import _lib
+        for _, gt, n, dx, dv, g, h, *_ in self.jobs:
+            st = self.lib.ech_hvp_batch_device(self.ctx._h, gt._h, 0, dx.data_ptr(), 1, dv.data_ptr(), n,
+                                               g.data_ptr(), h.data_ptr(), self.sp)
+            assert st == 0, _lib.last_error()
+
+    def extra(self, torch, stream, flush, steps):
+        """One launch per tape, and the multi launch replayed from a CUDA graph."""
+        for _ in range(3):
+            self.per_tape()
+        torch.cuda.synchronize()
+        t_per = []
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            self.per_tape()
+            e1.record(stream)
+            e1.synchronize()
+            t_per.append(e0.elapsed_time(e1))
+        graph = torch.cuda.CUDAGraph()
+        cap = torch.cuda.Stream()
+        with torch.cuda.graph(graph, stream=cap, capture_error_mode="thread_local"):
+            self.multi.launch(cap.cuda_stream)
+        graph.replay()
+        torch.cuda.synchronize()
+        t_graph = []
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            graph.replay()
+            e1.record(stream)
+            e1.synchronize()
+            t_graph.append(e0.elapsed_time(e1))
+        del graph
+        return {"one launch per tape ms": float(np.mean(t_per)), "graph replay ms": float(np.mean(t_graph)),
+                "multi_shape": self.multi.info()}
+
+    def e2e_step(self):
+        from echidna_b200 import _lib
+        P = _lib.ptr
+        for _, gt, n, *_, hx, hv, hg, hh in self.jobs:
+            st = self.lib.ech_hvp_batch_points_f32(self.ctx._h, gt._h, P(hx), hx.size, P(hv), hv.size, n, P(hg),
+                                                   hg.size, P(hh), hh.size)
+            assert st == 0, _lib.last_error()
+
+    def io_bytes(self):
+        h2d = sum(j[7].nbytes + j[8].nbytes for j in self.jobs)
+        d2h = sum(j[9].nbytes + j[10].nbytes for j in self.jobs)
+        return int(h2d), int(d2h)
+
+    def roofline_inputs(self, kernel):
+        s, total_b, total_f = 4, 0, 0
+        for tape, gt, n, *_ in self.jobs:
+            st = self.ctx.plan_stats(gt, "hvp")
+            ni = tape.num_inputs
+            total_b += n * (s * (4 * ni + 1) + 2 * s * 2 * st["traj_values"])
+            total_f += n * 4 * (st["flops_fwd"] + st["flops_rev"])
+        return total_b, total_f
+
+    def detail(self):
+        return {}
+
+    def cpu_reference(self, budget_s, nthreads):
+        from oracle.oracle import OracleTape
+        orcs = [OracleTape(tape) for _, tape, _ in self.suite]
+
+        def run(k):
+            pts = 0
+            t0 = time.perf_counter()
+            for o, (x, v), (_, _, n) in zip(orcs, self.data, self.suite):
+                m = min(n, k)
+                o.hvp(x[:m].astype(np.float64), v[:m].astype(np.float64), nthreads)
+                pts += m
+            return pts, time.perf_counter() - t0
+        pts, dt = run(4)
+        k = int(max(4, 4 * budget_s / max(dt, 1e-6)))
+        pts, dt = run(k)
+        return pts / dt, f"{pts} points (up to {k} per tape): oracle gradient + per-point HVP (f64), {dt:.1f} s"
+
+
+WORKLOADS = {"mlp": MlpWorkload, "rosenbrock": RosenbrockWorkload, "stde": StdeWorkload, "uneven": UnevenWorkload}
 
 
 # ───────────────────────────── arms ──────────────────────────────────────────
@@ -465,6 +594,8 @@ def main():
     if world > 1:
         step_ms = max_over_ranks(step_ms, "cuda")
 
+    extra = wl.extra(torch, stream, flush, args.steps) if hasattr(wl, "extra") else {}
+
     # end-to-end through the host-buffer ABI (pinned host buffers)
     wl.e2e_step()
     barrier()
@@ -508,7 +639,7 @@ def main():
         "e2e": {"value": world * wl.batch / (e2e_step_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "clocks": clk.summary(),
-        "detail": {**{f"{k} ms": v for k, v in mean_ms.items()}, **wl.detail()},
+        "detail": {**{f"{k} ms": v for k, v in mean_ms.items()}, **wl.detail(), **extra},
     }
     if rank == 0 and not args.no_cpu_baseline:
         nth = os.cpu_count() or 1
@@ -516,7 +647,7 @@ def main():
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    del wl
+    del kernels, wl
     ctx.close()
     if world > 1:
         dist.destroy_process_group()

@@ -77,6 +77,10 @@ _SIGS = {
     "ech_hvp_batch_device": ([_P, _P, _I, _P, _I, _P, _U32, _P, _P, _P], _I),
     "ech_taylor_batch_device": ([_P, _P, _I, _P, _P, _U32, _U32, _P, _P], _I),
     "ech_noalloc_region_bytes": ([], _SZ),
+    "ech_multi_create": ([_P, _I, _P, _U32, _I, _P], _I),
+    "ech_multi_launch": ([_P, _P], _I),
+    "ech_multi_info": ([_P, ctypes.POINTER(_U64)], _I),
+    "ech_multi_destroy": ([_P], None),
     "ech_laplacian_batch_device": ([_P, _P, _I, _P, _U32, _P, _U32, _I, _U64, _P, _P], _I),
     "ech_diagonal_kth_order_stochastic_f32": ([_P, _P, _P, _SZ, _U32, _P, _SZ, _P], _I),
     "ech_diagonal_kth_order_stochastic_f64": ([_P, _P, _P, _SZ, _U32, _P, _SZ, _P], _I),

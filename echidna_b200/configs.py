@@ -169,3 +169,45 @@ def random_dag(n: int, length: int, seed: int, dtype=np.float64):
     x0 = list(np.linspace(-0.5, 0.5, n))
     tape, _ = record(f, x0, dtype=dtype)
     return tape
+
+
+def ackley_fn(x):
+    n = float(len(x))
+    s2 = constant(0.0)
+    sc = constant(0.0)
+    for xi in x:
+        s2 = s2 + xi * xi
+        sc = sc + (xi * (2.0 * np.pi)).cos()
+    return -20.0 * (-0.2 * (s2 / n).sqrt()).exp() - (sc / n).exp() + 20.0 + float(np.e)
+
+
+def ackley(n: int, dtype=np.float64):
+    """Ackley-type sum of exp / cos terms over ``n`` inputs."""
+    tape, _ = record(ackley_fn, list(np.linspace(-0.5, 0.5, n)), dtype=dtype)
+    return tape
+
+
+def uneven_suite(count: int = 64, seed: int = SEEDS["uneven"], max_points: int = 100_000, max_len: int = 20_000,
+                 max_dim: int = 512):
+    """The uneven multi-tape batch: ``count`` (name, tape, n_points) triples.
+
+    Tapes cycle through Rosenbrock, Ackley-type and random DAGs over
+    {add, mul, sin, exp, log, tanh}; input dimensions are log-uniform in
+    [2, max_dim], DAG lengths log-uniform in [200, max_len] ops and point counts
+    log-uniform in [1, max_points].
+    """
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(2), np.log(max_dim)))))
+        pts = int(round(np.exp(rng.uniform(0.0, np.log(max_points)))))
+        kind = k % 3
+        if kind == 0:
+            name, tape = f"rosenbrock{n}", rosenbrock(n)
+        elif kind == 1:
+            name, tape = f"ackley{n}", ackley(n)
+        else:
+            length = int(round(np.exp(rng.uniform(np.log(200), np.log(max_len)))))
+            name, tape = f"dag{n}x{length}", random_dag(n, length, seed=seed + k)
+        out.append((name, tape, max(1, pts)))
+    return out

@@ -394,7 +394,7 @@ static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_
 }
 
 // Autotuning applies from this many units up; smaller batches use the fixed shape.
-static constexpr uint64_t kTuneMinUnits = 16384;
+static constexpr uint64_t kTuneMinUnits = 512;
 
 static int size_bucket(uint64_t n) {
   int b = 0;
@@ -404,9 +404,12 @@ static int size_bucket(uint64_t n) {
 
 // Candidate shapes, timed on the call's own inputs (every shape computes
 // bit-identical results: a point's arithmetic does not depend on the launch).
+// The narrow shapes (32 / 64 threads) spread batches of fewer than two
+// 128-point tiles per SM over more SMs; they are only tried for such batches.
 static const Shape kShapes[] = {
     {128, 1, 1}, {128, 1, 2}, {128, 1, 3}, {128, 1, 4}, {128, 2, 1}, {128, 2, 2},
     {128, 2, 3}, {128, 4, 1}, {128, 4, 2}, {256, 1, 1}, {256, 1, 2}, {64, 2, 4},
+    {64, 1, 2}, {64, 1, 4}, {32, 1, 2}, {32, 1, 4},
 };
 
 static ech_status tune(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n_units, const SweepIO& io,
@@ -417,7 +420,9 @@ static ech_status tune(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n_un
   float best_ms = -1.0f;
   ech_status first_err = ECH_OK;
   std::string first_msg;
+  const bool small_batch = n_units < (uint64_t)2 * 128 * ctx->sm_count;
   for (const Shape& sh : kShapes) {
+    if (sh.threads * sh.P < 128 && !small_batch) continue;
     const LaunchCfg c = cfg_for(ctx, t, kind, K, sh);
     if (c.cap < 1 || kRingBytes + (size_t)c.tile * c.vbytes > ctx->smem_optin) continue;
     ech_status s = launch_cfg(ctx, t, kind, K, n_units, io, st, c);  // warm: plan build + upload
@@ -1124,6 +1129,205 @@ size_t value_bytes(const LaunchReq& r) {
   return s;
 }
 }  // namespace ech
+
+// ───────────────────────────── many tapes, one launch ───────────────────────
+// A prepared many-tape gradient + per-point HVP launch over caller-owned device
+// buffers (extension; the uneven-batch workload).  Preparation lowers every
+// tape for one launch shape, orders the jobs by cost, uploads the job table and
+// sizes the scratch; a launch is then a counter reset plus one kernel.
+struct ech_multi {
+  ech_ctx* ctx = nullptr;  // must outlive the handle
+  int device = 0;
+  bool f64 = false;
+  std::vector<ech_multi_item> items;
+  Shape shape;
+  LaunchCfg cfg;
+  DevBuf jobs, next, scratch;
+  uint32_t n_jobs = 0;
+  uint32_t total_tiles = 0;
+  uint64_t stride = 0;
+  int grid = 0;
+  bool tuned = false;
+};
+
+static ech_status multi_prepare(ech_multi* m, Shape sh) {
+  ech_ctx* ctx = m->ctx;
+  CU(cudaStreamSynchronize(ctx->stream));  // no earlier launch may still read the job table or scratch
+  LaunchCfg c = cfg_for(ctx, m->items[0].tape, 2, 0, sh);
+  if (c.cap < 1 || kRingBytes + (size_t)c.tile * c.vbytes > ctx->smem_optin)
+    return fail(ECH_ERR_OTHER, "launch shape does not fit shared memory");
+  struct J {
+    MultiJob job;
+    uint64_t cost, tiles;
+  };
+  std::vector<J> js;
+  uint32_t regs = 1;
+  uint64_t slots = 0;
+  for (const ech_multi_item& it : m->items) {
+    if (it.n_points == 0) continue;
+    ech_tape* t = const_cast<ech_tape*>(it.tape);
+    DevPlan* dp = nullptr;
+    CHECK(get_plan(t, 2, 0, c.cap, c.tile, (uint32_t)c.vbytes, &dp));
+    const Plan& p = dp->host;
+    regs = std::max<uint32_t>(regs, p.smem_regs);
+    slots = std::max<uint64_t>(slots, (uint64_t)p.far_slots + p.traj_slots);
+    J j{};
+    KParams& kp = j.job.kp;
+    kp.fwd = dp->d_fwd;
+    kp.n_fwd = (uint32_t)p.fwd.size();
+    kp.rev = dp->d_rev;
+    kp.n_rev = (uint32_t)p.rev.size();
+    kp.fterms = dp->d_fterms;
+    kp.rterms = dp->d_rterms;
+    kp.far_slots = p.far_slots;
+    kp.tile = c.tile;
+    kp.n_units = it.n_points;
+    kp.ni = t->host.ni;
+    kp.no = (uint32_t)t->host.outs.size();
+    kp.x = it.xs;
+    kp.v = it.dirs;
+    kp.x_bcast = 0;
+    kp.out2 = it.grads;
+    kp.out3 = it.hvps;
+    kp.err = ctx->d_err;
+    j.tiles = (it.n_points + c.tile - 1) / c.tile;
+    j.cost = (uint64_t)p.fwd.size() + p.rev.size();
+    js.push_back(j);
+  }
+  if (js.empty()) return fail(ECH_ERR_OTHER, "batch_size must be non-zero");
+  // most expensive tiles first, so the tail of the dynamic schedule is short work
+  std::stable_sort(js.begin(), js.end(), [](const J& a, const J& b) { return a.cost > b.cost; });
+  uint64_t first = 0;
+  std::vector<MultiJob> h(js.size());
+  for (size_t k = 0; k < js.size(); ++k) {
+    h[k] = js[k].job;
+    h[k].kp.smem_regs = regs;
+    h[k].first_tile = first;
+    first += js[k].tiles;
+  }
+  if (first >= 0xFFFFFFFFull) return fail(ECH_ERR_OTHER, "too many tiles for one launch");
+  c.smem = kRingBytes + (size_t)regs * c.tile * c.vbytes;
+  uint64_t stride = slots * c.tile * c.vbytes;
+  stride = (stride + 255) & ~(uint64_t)255;
+  MultiParams mp{};
+  int bps = 0;
+  cudaError_t e = launch_multi_hvp(m->f64, c.req.P, mp, 0, c.threads, c.smem, nullptr, &bps);
+  if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+  if (bps <= 0) return fail(ECH_ERR_OTHER, "tape live set does not fit the shared-memory slot file");
+  const uint64_t grid = std::min<uint64_t>(first, (uint64_t)bps * ctx->sm_count);
+  CU(m->jobs.ensure(h.size() * sizeof(MultiJob)));
+  CU(m->next.ensure(sizeof(uint32_t)));
+  CU(m->scratch.ensure(std::max<uint64_t>(stride * grid, 256)));
+  for (MultiJob& j : h) {
+    j.kp.scratch = m->scratch.p;
+    j.kp.scratch_stride_bytes = stride;
+  }
+  CU(cudaMemcpy(m->jobs.p, h.data(), h.size() * sizeof(MultiJob), cudaMemcpyHostToDevice));
+  m->shape = sh;
+  m->cfg = c;
+  m->n_jobs = (uint32_t)h.size();
+  m->total_tiles = (uint32_t)first;
+  m->stride = stride;
+  m->grid = (int)grid;
+  return ECH_OK;
+}
+
+static ech_status multi_enqueue(ech_multi* m, cudaStream_t st) {
+  MultiParams mp{};
+  mp.jobs = (const MultiJob*)m->jobs.p;
+  mp.n_jobs = m->n_jobs;
+  mp.total_tiles = m->total_tiles;
+  mp.next_tile = (uint32_t*)m->next.p;
+  mp.scratch = m->scratch.p;
+  mp.stride = m->stride;
+  CU(cudaMemsetAsync(m->next.p, 0, sizeof(uint32_t), st));
+  int bps = 0;
+  cudaError_t e = launch_multi_hvp(m->f64, m->cfg.req.P, mp, m->grid, m->cfg.threads, m->cfg.smem, st, &bps);
+  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  return ECH_OK;
+}
+
+extern "C" {
+
+ECH_API ech_status ech_multi_create(ech_ctx* ctx, int f64, const ech_multi_item* items, uint32_t n_items,
+                                    int autotune, ech_multi** out) {
+  if (!ctx || !out || (n_items && !items)) return fail(ECH_ERR_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (n_items == 0) return fail(ECH_ERR_OTHER, "batch_size must be non-zero");
+  uint64_t total_points = 0;
+  for (uint32_t k = 0; k < n_items; ++k) {
+    const ech_multi_item& it = items[k];
+    if (!it.tape) return fail(ECH_ERR_INVALID_ARG, "null tape");
+    if (it.tape->ctx != ctx) return fail(ECH_ERR_INVALID_ARG, "tape belongs to another context");
+    if (it.tape->f64 != (f64 != 0)) return fail(ECH_ERR_INVALID_ARG, "tape precision does not match the call");
+    if (it.tape->host.ni == 0) return fail(ECH_ERR_OTHER, "tape has no inputs");
+    if (it.n_points && (!it.xs || !it.dirs || !it.grads || !it.hvps))
+      return fail(ECH_ERR_INVALID_ARG, "null device buffer");
+    total_points += it.n_points;
+  }
+  if (total_points == 0) return fail(ECH_ERR_OTHER, "batch_size must be non-zero");
+  std::unique_ptr<ech_multi> m(new ech_multi());
+  m->ctx = ctx;
+  m->device = ctx->device;
+  m->f64 = f64 != 0;
+  m->items.assign(items, items + n_items);
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  Shape best;
+  if (autotune) {
+    cudaEvent_t e0, e1;
+    CU(cudaEventCreate(&e0));
+    CU(cudaEventCreate(&e1));
+    float best_ms = -1.0f;
+    for (const Shape& sh : kShapes) {
+      if (sh.threads * sh.P < 128) continue;
+      if (multi_prepare(m.get(), sh) != ECH_OK) continue;
+      if (multi_enqueue(m.get(), ctx->stream) != ECH_OK) continue;  // warm
+      cudaEventRecord(e0, ctx->stream);
+      const ech_status s = multi_enqueue(m.get(), ctx->stream);
+      cudaEventRecord(e1, ctx->stream);
+      if (s != ECH_OK || cudaEventSynchronize(e1) != cudaSuccess) continue;
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (best_ms < 0.0f || ms < best_ms) {
+        best_ms = ms;
+        best = sh;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CHECK(check_err_word(ctx));
+    if (best_ms < 0.0f) return fail(ECH_ERR_OTHER, "no launch shape fits");
+    m->tuned = true;
+  }
+  CHECK(multi_prepare(m.get(), best));
+  *out = m.release();
+  return ECH_OK;
+}
+
+ECH_API ech_status ech_multi_launch(ech_multi* m, void* stream) {
+  if (!m) return fail(ECH_ERR_INVALID_ARG, "null multi");
+  std::lock_guard<std::mutex> lk(m->ctx->mu);
+  CU(cudaSetDevice(m->ctx->device));
+  return multi_enqueue(m, stream ? (cudaStream_t)stream : m->ctx->stream);
+}
+
+ECH_API ech_status ech_multi_info(const ech_multi* m, uint64_t* info) {
+  if (!m || !info) return fail(ECH_ERR_INVALID_ARG, "null argument");
+  uint64_t v[9] = {m->shape.threads, m->shape.P, m->shape.ctas, m->cfg.cap, (uint64_t)m->grid, m->total_tiles,
+                   m->n_jobs, m->stride, m->tuned ? 1u : 0u};
+  memcpy(info, v, sizeof v);
+  return ECH_OK;
+}
+
+ECH_API void ech_multi_destroy(ech_multi* m) {
+  if (!m) return;
+  // only the device is needed here (its buffers' cudaFree waits for work that uses them)
+  cudaSetDevice(m->device);
+  delete m;
+}
+
+}  // extern "C"
 
 // ───────────────────────────── internal hooks ───────────────────────────────
 namespace ech {

@@ -750,7 +750,31 @@ template <class V, int P> struct RevExec {
   }
 };
 
-// ───────────────────────────── the sweep kernel ─────────────────────────────
+// ───────────────────────────── the sweep kernels ────────────────────────────
+// One tile of `kp.tile` units: the forward program (with trajectory saves when
+// REV), then the reverse program.  `gbase` is the CTA's global scratch region.
+// Returns false when a bounded wait gave up (every thread sees the same value).
+template <class V, int P, bool REV>
+__device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned char* sm, unsigned char* gbase,
+                                           uint64_t t) {
+  const uint32_t tile = kp.tile;
+  const size_t colb = (size_t)threadIdx.x * P * sizeof(V);
+  unsigned char* gs = gbase + colb;
+  unsigned char* tj = gbase + (size_t)kp.far_slots * tile * sizeof(V) + colb;
+  const uint64_t unit0 = t * tile + (uint64_t)threadIdx.x * P;
+  FwdExec<V, P> fx{kp, sm, gs, tj, unit0, {}};
+#pragma unroll
+  for (int p = 0; p < P; ++p) fx.valid[p] = unit0 + p < kp.n_units;
+  if (!run_program<32>(rg, reinterpret_cast<const unsigned char*>(kp.fwd), kp.n_fwd, kp.err, fx)) return false;
+  if (REV) {
+    RevExec<V, P> rx{kp, sm, gs, tj, unit0, {}};
+#pragma unroll
+    for (int p = 0; p < P; ++p) rx.valid[p] = fx.valid[p];
+    if (!run_program<48>(rg, reinterpret_cast<const unsigned char*>(kp.rev), kp.n_rev, kp.err, rx)) return false;
+  }
+  return true;
+}
+
 // REV = false: forward program only (forward values, JVP, Taylor jets).
 // REV = true : forward program with trajectory saves, then the reverse program
 //              (gradient for plain values, HVP for Dual values).
@@ -764,25 +788,69 @@ __global__ void __launch_bounds__(256) sweep_kernel(KParams kp) {
   }
   __syncthreads();
   Ring rg{smem_dyn, full, 0u, 0u};
-  const uint32_t tile = kp.tile;
-  const size_t colb = (size_t)threadIdx.x * P * sizeof(V);
-  unsigned char* sm = smem_dyn + kRingBytes + colb;
+  unsigned char* sm = smem_dyn + kRingBytes + (size_t)threadIdx.x * P * sizeof(V);
   unsigned char* gbase = reinterpret_cast<unsigned char*>(kp.scratch) + blockIdx.x * kp.scratch_stride_bytes;
-  unsigned char* gs = gbase + colb;
-  unsigned char* tj = gbase + (size_t)kp.far_slots * tile * sizeof(V) + colb;
-  const uint64_t ntiles = (kp.n_units + tile - 1) / tile;
-  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const uint64_t unit0 = t * tile + (uint64_t)threadIdx.x * P;
-    FwdExec<V, P> fx{kp, sm, gs, tj, unit0, {}};
-#pragma unroll
-    for (int p = 0; p < P; ++p) fx.valid[p] = unit0 + p < kp.n_units;
-    if (!run_program<32>(rg, reinterpret_cast<const unsigned char*>(kp.fwd), kp.n_fwd, kp.err, fx)) return;
-    if (REV) {
-      RevExec<V, P> rx{kp, sm, gs, tj, unit0, {}};
-#pragma unroll
-      for (int p = 0; p < P; ++p) rx.valid[p] = fx.valid[p];
-      if (!run_program<48>(rg, reinterpret_cast<const unsigned char*>(kp.rev), kp.n_rev, kp.err, rx)) return;
+  const uint64_t ntiles = (kp.n_units + kp.tile - 1) / kp.tile;
+  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x)
+    if (!sweep_tile<V, P, REV>(kp, rg, sm, gbase, t)) return;
+}
+
+// ───────────────────────────── many tapes, one launch ───────────────────────
+// Uneven batches of tapes (different programs, input sizes and point counts)
+// as one persistent launch: the global tile list is the concatenation of every
+// job's tiles (jobs ordered by the host, most expensive tile first), and CTAs
+// take tiles from a global counter, so long and short tapes balance across
+// SMs.  Each job is a complete parameter block; all jobs share the launch's
+// tile size, shared-register budget and per-CTA scratch stride.
+struct MultiJob {
+  KParams kp;
+  uint64_t first_tile;   // global id of the job's first tile
+  uint64_t pad;
+};
+
+struct MultiParams {
+  const MultiJob* jobs;
+  uint32_t n_jobs;
+  uint32_t total_tiles;
+  uint32_t* next_tile;   // tile counter, zero at launch
+  void* scratch;
+  uint64_t stride;       // scratch bytes per CTA
+};
+
+template <class V, int P>
+__global__ void __launch_bounds__(256) multi_sweep_kernel(MultiParams mp) {
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  __shared__ __align__(8) uint64_t full[kStages];
+  __shared__ __align__(16) KParams job;
+  __shared__ uint32_t s_tile;
+  __shared__ uint64_t s_local;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  Ring rg{smem_dyn, full, 0u, 0u};
+  unsigned char* sm = smem_dyn + kRingBytes + (size_t)threadIdx.x * P * sizeof(V);
+  unsigned char* gbase = reinterpret_cast<unsigned char*>(mp.scratch) + blockIdx.x * mp.stride;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const uint32_t g = atomicAdd(mp.next_tile, 1u);
+      s_tile = g;
+      if (g < mp.total_tiles) {
+        uint32_t lo = 0, hi = mp.n_jobs - 1;   // last job with first_tile <= g
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi + 1) / 2;
+          if (mp.jobs[mid].first_tile <= g) lo = mid;
+          else hi = mid - 1;
+        }
+        job = mp.jobs[lo].kp;
+        s_local = g - mp.jobs[lo].first_tile;
+      }
     }
+    __syncthreads();
+    if (s_tile >= mp.total_tiles) break;
+    if (!sweep_tile<V, P, true>(job, rg, sm, gbase, s_local)) return;
+    __syncthreads();  // every thread is done with `job` before thread 0 replaces it
   }
 }
 

@@ -7,6 +7,7 @@
 
 namespace ech {
 struct KParams;
+struct MultiParams;
 
 enum class VKind { Plain, Dual, Jet };
 
@@ -37,6 +38,10 @@ inline cudaError_t launch_sweep(const LaunchReq& r, const KParams& kp, int grid,
   }
   return cudaErrorInvalidValue;
 }
+
+// Many-tape persistent gradient + per-point HVP launch (grid == 0: occupancy query).
+cudaError_t launch_multi_hvp(bool f64, int P, const MultiParams& mp, int grid, int block, size_t smem,
+                             cudaStream_t st, int* blocks_per_sm);
 
 // STDE per-point reduction of scale*c_k samples (Welford in direction order);
 // acc64 selects a double accumulator for f32 samples.

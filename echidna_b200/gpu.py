@@ -197,6 +197,7 @@ class CudaContext:
 
     def __init__(self, handle):
         self._h = handle
+        self._children = []  # handles that must be released before the context
 
     @staticmethod
     def new(device: int = 0) -> Optional["CudaContext"]:
@@ -208,6 +209,9 @@ class CudaContext:
         return CudaContext(h)
 
     def close(self):
+        for c in getattr(self, "_children", []):
+            c.close()
+        self._children = []
         if getattr(self, "_h", None):
             _lib.load().ech_ctx_destroy(self._h)
             self._h = None
@@ -411,3 +415,54 @@ class CudaContext:
     def sparse_hessian_f64(self, tape: CudaTapeBuffersF64, tape_cpu: BytecodeTape, x):
         from .sparse import sparse_hessian_gpu
         return sparse_hessian_gpu(self, tape, tape_cpu, x, np.float64)
+
+
+class _MultiItem(ctypes.Structure):
+    _fields_ = [("tape", ctypes.c_void_p), ("xs", ctypes.c_void_p), ("dirs", ctypes.c_void_p),
+                ("n_points", ctypes.c_uint32), ("pad", ctypes.c_uint32), ("grads", ctypes.c_void_p),
+                ("hvps", ctypes.c_void_p)]
+
+
+class MultiTapeHvp:
+    """Gradient + per-point HVP of many tapes in one persistent launch (extension).
+
+    ``items``: sequence of ``(tape, xs_ptr, dirs_ptr, n_points, grads_ptr, hvps_ptr)``
+    with device pointers (``[n_points][num_inputs]`` each).  The buffers are bound
+    to the launch; ``launch(stream)`` enqueues it without synchronising, so it can
+    be captured in a CUDA graph once created.
+    """
+
+    def __init__(self, ctx: "CudaContext", items, f64: bool = False, autotune: bool = True):
+        lib = _lib.load()
+        arr = (_MultiItem * len(items))()
+        for k, (tape, xs, dirs, n, g, h) in enumerate(items):
+            arr[k] = _MultiItem(tape._h, xs, dirs, int(n), 0, g, h)
+        self._items = arr
+        self._tapes = [it[0] for it in items]
+        self._ctx = ctx
+        h = ctypes.c_void_p()
+        _check(lib.ech_multi_create(ctx._h, 1 if f64 else 0, ctypes.cast(arr, ctypes.c_void_p), len(items),
+                                    1 if autotune else 0, ctypes.byref(h)))
+        self._h = h
+        ctx._children.append(self)
+
+    def launch(self, stream: int = 0):
+        _check(_lib.load().ech_multi_launch(self._h, ctypes.c_void_p(stream)))
+
+    def info(self) -> dict:
+        buf = (ctypes.c_uint64 * 9)()
+        _check(_lib.load().ech_multi_info(self._h, buf))
+        keys = ["threads", "points_per_thread", "ctas_per_sm", "smem_reg_cap", "grid", "tiles", "jobs",
+                "scratch_bytes_per_cta", "tuned"]
+        return dict(zip(keys, [int(v) for v in buf]))
+
+    def close(self):
+        if getattr(self, "_h", None) and getattr(self._ctx, "_h", None):
+            _lib.load().ech_multi_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

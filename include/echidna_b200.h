@@ -234,6 +234,37 @@ ECH_API ech_status ech_diagonal_kth_order_stochastic_f64(ech_ctx* ctx, const ech
                                                          size_t n, uint32_t k, const uint32_t* sampled_indices,
                                                          size_t n_indices, ech_estimator_result* out);
 
+/* ── many tapes in one launch (extension, no reference counterpart) ─────────
+ * Gradient + per-point HVP for a batch of different tapes with uneven input
+ * sizes and point counts, as one persistent launch.  Every pointer in an item is
+ * a device pointer: xs and dirs [n_points][num_inputs], grads and hvps
+ * [n_points][num_inputs].  All tapes belong to `ctx` and share the precision
+ * `f64`.  ech_multi_create lowers every tape for one launch shape (with
+ * autotune != 0 it times the candidate shapes on the items' own buffers and
+ * waits for them), orders the work by cost and sizes the scratch; the buffers
+ * are bound to the handle.  ech_multi_launch enqueues a counter reset and one
+ * kernel on `stream` (NULL = the context's) and returns without synchronising;
+ * device-side errors surface at ech_ctx_synchronize.  Results equal
+ * ech_hvp_batch_device with x_per_point = 1 on each item.  Destroy the handle
+ * before its context. */
+typedef struct ech_multi ech_multi;
+typedef struct ech_multi_item {
+  const ech_tape* tape;
+  const void* xs;
+  const void* dirs;
+  uint32_t n_points;
+  uint32_t pad;
+  void* grads;
+  void* hvps;
+} ech_multi_item;
+ECH_API ech_status ech_multi_create(ech_ctx* ctx, int f64, const ech_multi_item* items, uint32_t n_items,
+                                    int autotune, ech_multi** out);
+ECH_API ech_status ech_multi_launch(ech_multi* multi, void* stream);
+/* info[9]: threads, points per thread, CTAs per SM, shared-register cap, grid,
+ * tiles, jobs, scratch bytes per CTA, tuned (1/0). */
+ECH_API ech_status ech_multi_info(const ech_multi* multi, uint64_t* info);
+ECH_API void ech_multi_destroy(ech_multi* multi);
+
 /* ── structural sparsity and coloring (host only, no device needed) ──────────
  * Used by the sparse Jacobian / Hessian drop-ins (src/gpu/cuda_backend.rs:306-441),
  * which seed the tangent / HVP sweeps with one row per color.  Two-call
@@ -283,7 +314,7 @@ ECH_API ech_status ech_plan_dump(const uint32_t* opcodes, const uint32_t* arg0, 
 ECH_API ech_status ech_ctx_set_launch(ech_ctx* ctx, uint32_t threads, uint32_t points_per_thread,
                                       uint32_t smem_reg_cap);
 /* Launch-shape autotuning (default on).  Without overrides, the first sweep of
- * a (tape, kind, order, batch-size octave) with at least 16,384 units times a
+ * a (tape, kind, order, batch-size octave) with at least 512 units times a
  * fixed set of shapes (threads per CTA, points per thread, CTAs per SM) on the
  * call's own inputs and keeps the fastest; every shape computes bit-identical
  * results.  That first call waits for its timing runs; calls made while the
