@@ -661,8 +661,61 @@ template <class V, int P> struct RevExec {
     for (int p = 0; p < P; ++p) one[p] = Kd::c(1);
     C::ld(loc(flags & RF_R_GLOB, ro), adj);
     const uint4* tp = reinterpret_cast<const uint4*>(kp.rterms + first);
+    uint32_t q = n;
 #pragma unroll 1
-    for (uint32_t q = n; q-- > 0;) {
+    while (q >= 3) {
+      // terms q-1 and q-2 (neither is the first term): when their adjoint
+      // targets differ the two read-modify-writes are independent, so both
+      // loads are issued before either store
+      const uint4 a0 = __ldg(tp + 2 * (q - 1));
+      const uint4 a1 = __ldg(tp + 2 * (q - 1) + 1);
+      const uint4 b0 = __ldg(tp + 2 * (q - 2));
+      const uint4 b1 = __ldg(tp + 2 * (q - 2) + 1);
+      const uint32_t fa = a0.x >> 16, fb = b0.x >> 16;
+      unsigned char* pa = loc(fa & CF_X_GLOB, a0.y);
+      unsigned char* pb = loc(fb & CF_X_GLOB, b0.y);
+      V ta[P], tb[P];
+      internal(adj, one, ta);
+      if (pa == pb) {
+        const V ca = dm::VT<V>::cst(__hiloint2double((int)a1.w, (int)a1.z));
+        V c[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) c[p] = ca;
+        accumulate<false>(pa, (fa & CF_X_INIT) != 0, ta, c);
+#pragma unroll
+        for (int p = 0; p < P; ++p) adj[p] = ta[p];
+        q -= 1;
+        continue;
+      }
+      internal(ta, one, tb);
+      V cura[P], curb[P];
+      if (fa & CF_X_INIT) {
+#pragma unroll
+        for (int p = 0; p < P; ++p) cura[p] = Kd::c(0);
+      } else {
+        C::ld(pa, cura);
+      }
+      if (fb & CF_X_INIT) {
+#pragma unroll
+        for (int p = 0; p < P; ++p) curb[p] = Kd::c(0);
+      } else {
+        C::ld(pb, curb);
+      }
+      const V ca = dm::VT<V>::cst(__hiloint2double((int)a1.w, (int)a1.z));
+      const V cb = dm::VT<V>::cst(__hiloint2double((int)b1.w, (int)b1.z));
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        if (!Kd::all_zero(ta[p]) && !Kd::all_zero(ca)) cura[p] = Kd::add(cura[p], Kd::mul(ca, ta[p]));
+        if (!Kd::all_zero(tb[p]) && !Kd::all_zero(cb)) curb[p] = Kd::add(curb[p], Kd::mul(cb, tb[p]));
+      }
+      C::st(pa, cura);
+      C::st(pb, curb);
+#pragma unroll
+      for (int p = 0; p < P; ++p) adj[p] = tb[p];
+      q -= 2;
+    }
+#pragma unroll 1
+    while (q-- > 0) {
       const uint4 w0 = __ldg(tp + 2 * q);
       const uint4 w1 = __ldg(tp + 2 * q + 1);
       const uint32_t tf = w0.x >> 16;

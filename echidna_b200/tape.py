@@ -379,20 +379,43 @@ class BytecodeTape:
 
     @classmethod
     def from_json(cls, text: str, dtype=np.float64) -> "BytecodeTape":
+        """Deserialize (``src/bytecode_tape/serde_support.rs:35-100``): custom ops and their
+        side table are refused, ``num_variables`` must equal the entry count, and the
+        whole tape is validated; every corrupt payload raises ``TapeValidationError``."""
         d = json.loads(text)
+        try:
+            ops = [int(OpCode[o]) if isinstance(o, str) else int(o) for o in d["opcodes"]]
+            args = [[int(a[0]), int(a[1])] for a in d["arg_indices"]]
+            values = list(d["values"])
+            num_inputs = int(d["num_inputs"])
+            num_variables = int(d["num_variables"])
+            output_index = int(d["output_index"])
+            output_indices = [int(i) for i in d.get("output_indices", [])]
+            custom_second_args = d.get("custom_second_args", {}) or {}
+        except (KeyError, TypeError, ValueError, IndexError) as e:
+            raise TapeValidationError(f"malformed tape payload: {e}") from e
+        if OpCode.Custom in ops:
+            i = ops.index(OpCode.Custom)
+            raise TapeValidationError(f"opcodes[{i}] is Custom, which cannot be deserialized "
+                                      "(custom ops have no serializable callback)")
+        if custom_second_args:
+            raise TapeValidationError("custom_second_args must be empty: custom ops cannot be deserialized")
+        if num_variables != len(ops):
+            raise TapeValidationError(f"num_variables ({num_variables}) != opcodes.len() ({len(ops)})")
+        if len(args) != len(ops):
+            raise TapeValidationError(f"invalid bytecode tape: arg_indices.len() ({len(args)}) != "
+                                      f"opcodes.len() ({len(ops)})")
+        if len(values) != len(ops):
+            raise TapeValidationError(f"invalid bytecode tape: values.len() ({len(values)}) != "
+                                      f"opcodes.len() ({len(ops)})")
         t = cls(dtype)
-        ops = d["opcodes"]
-        t.opcodes = [int(OpCode[o]) if isinstance(o, str) else int(o) for o in ops]
-        t.arg0 = [int(a[0]) for a in d["arg_indices"]]
-        t.arg1 = [int(a[1]) for a in d["arg_indices"]]
-        t.values = [t._s.c(v) for v in d["values"]]
-        t.num_inputs = int(d["num_inputs"])
-        t.output_index = int(d["output_index"])
-        t.output_indices = [int(i) for i in d.get("output_indices", [])]
-        if d.get("custom_second_args"):
-            t.has_custom_ops = True
-        if int(d.get("num_variables", len(t.values))) != len(t.values):
-            raise TapeValidationError("num_variables does not match values length")
+        t.opcodes = ops
+        t.arg0 = [a[0] for a in args]
+        t.arg1 = [a[1] for a in args]
+        t.values = [t._s.c(v) for v in values]
+        t.num_inputs = num_inputs
+        t.output_index = output_index
+        t.output_indices = output_indices
         t.validate()
         return t
 
