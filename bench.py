@@ -617,6 +617,15 @@ def main():
     peak, peak_kind = _peaks()
     dom_ms = mean_ms[dom]
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    # the interpreted sweeps are issue / latency bound: the scalar pipe is the
+    # compute roof (each +, -, *, / and libm call counted once; -fmad=false)
+    sm_mhz = 1965.0
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            sm_mhz = float(json.load(f).get("sm_max_mhz", sm_mhz))
+    except OSError:
+        pass
+    pipe_peak = 148 * 128 * sm_mhz * 1e6 / 1e12 * (0.5 if wl.describe()[1] == "f64" else 1.0)
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
@@ -635,7 +644,10 @@ def main():
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": dom_ms,
-                     "scalar_ops_per_launch": dom_ops, "scalar_tops": dom_ops / (dom_ms * 1e-3) / 1e12},
+                     "scalar_ops_per_launch": dom_ops, "scalar_tops": dom_ops / (dom_ms * 1e-3) / 1e12,
+                     "scalar_pipe_peak_tops": pipe_peak, "scalar_pipe_frac": dom_ops / (dom_ms * 1e-3) / 1e12 / pipe_peak,
+                     "scalar_pipe_peak_source": "nominal: 148 SMs x 128 FP32 lanes x max SM clock "
+                                                "(FP64: x 1/2); one op per lane per clock, no FMA"},
         "e2e": {"value": world * wl.batch / (e2e_step_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "clocks": clk.summary(),
