@@ -1334,6 +1334,14 @@ namespace ech {
 
 ech_status set_error(ech_status st, const std::string& msg) { return fail(st, msg); }
 
+ech_status ctx_basics(ech_ctx* ctx, int* device, cudaStream_t* stream, uint32_t** err) {
+  if (!ctx) return fail(ECH_ERR_INVALID_ARG, "ctx is null");
+  *device = ctx->device;
+  *stream = ctx->stream;
+  *err = ctx->d_err;
+  return ECH_OK;
+}
+
 ech_status prepare_gradient_host(ech_ctx* ctx, const ech_tape* tc, int f64, uint32_t B, HostSweep* out) {
   CHECK(common_checks(ctx, tc, f64 != 0));
   CHECK(batch_args(tc, B));

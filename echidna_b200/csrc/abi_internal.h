@@ -35,5 +35,7 @@ struct HostSweep {
 // Argument checks of the gradient entry points, then the host-side plan.
 ech_status prepare_gradient_host(ech_ctx* ctx, const ech_tape* t, int f64, uint32_t batch, HostSweep* out);
 ech_status set_error(ech_status st, const std::string& msg);
+// The context's device, stream and device-side error word.
+ech_status ctx_basics(ech_ctx* ctx, int* device, cudaStream_t* stream, uint32_t** err);
 
 }  // namespace ech

@@ -265,6 +265,28 @@ ECH_API ech_status ech_multi_launch(ech_multi* multi, void* stream);
 ECH_API ech_status ech_multi_info(const ech_multi* multi, uint64_t* info);
 ECH_API void ech_multi_destroy(ech_multi* multi);
 
+/* ── learned sampling proposal for sparse STDE (extension, no reference counterpart) ──
+ * A softmax MLP n_in -> hidden -> hidden -> n_out (ReLU), trained on the GPU with
+ * BF16 tensor-core GEMMs (tcgen05, FP32 accumulation) and Adam on FP32 master
+ * weights.  Sizes are multiples of 64; weights are row-major [out][in]. */
+typedef struct ech_mlp ech_mlp;
+ECH_API ech_status ech_mlp_create(ech_ctx* ctx, int n_in, int hidden, int n_out, const float* w1, const float* b1,
+                                  const float* w2, const float* b2, const float* w3, const float* b3,
+                                  ech_mlp** out);
+/* x [B][n_in], q [B][n_out] (rows of target probabilities) in device memory;
+ * B a positive multiple of 64; synchronous; *loss_out = mean cross-entropy. */
+ECH_API ech_status ech_mlp_train_step(ech_mlp* mlp, const float* x, const float* q, int batch, float lr,
+                                      float* loss_out);
+/* probs [B][n_out] = softmax(MLP(x)), device arrays, enqueued on `stream`. */
+ECH_API ech_status ech_mlp_forward(ech_mlp* mlp, const float* x, int batch, float* probs, void* stream);
+ECH_API ech_status ech_mlp_get_weights(ech_mlp* mlp, float* w1, float* b1, float* w2, float* b2, float* w3,
+                                       float* b3);
+ECH_API void ech_mlp_destroy(ech_mlp* mlp);
+/* The GEMM the MLP uses: C[M][N] (fp32) = A[M][K] * B[N][K]^T (+ bias[N]), A and B
+ * bf16 row-major device arrays, K a multiple of 64, lda/ldb multiples of 8. */
+ECH_API ech_status ech_gemm_bf16(ech_ctx* ctx, const void* A, const void* B, float* C, const float* bias, int M,
+                                 int N, int K, int lda, int ldb, int ldc, void* stream);
+
 /* ── structural sparsity and coloring (host only, no device needed) ──────────
  * Used by the sparse Jacobian / Hessian drop-ins (src/gpu/cuda_backend.rs:306-441),
  * which seed the tangent / HVP sweeps with one row per color.  Two-call
