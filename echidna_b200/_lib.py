@@ -77,6 +77,8 @@ _SIGS = {
     "ech_hvp_batch_device": ([_P, _P, _I, _P, _I, _P, _U32, _P, _P, _P], _I),
     "ech_taylor_batch_device": ([_P, _P, _I, _P, _P, _U32, _U32, _P, _P], _I),
     "ech_noalloc_region_bytes": ([], _SZ),
+    "ech_hessian_diagonal_batch_device": ([_P, _P, _I, _P, _U32, _P, _P], _I),
+    "ech_sparse_trace_batch_device": ([_P, _P, _I, _P, _U32, _P, _U32, _U64, _P, _P], _I),
     "ech_gemm_bf16": ([_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P], _I),
     "ech_mlp_create": ([_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P], _I),
     "ech_mlp_train_step": ([_P, _P, _P, _I, ctypes.c_float, _P], _I),

@@ -803,7 +803,7 @@ template <class T>
 static ech_status stde_run(ech_ctx* ctx, ech_tape* t, const T* d_x, bool x_bcast, uint64_t npoints, uint32_t S,
                            const T* d_dirs, int dir_mode, uint64_t seed, bool acc64, const T* d_cv, double trace,
                            int control, ech_estimator_result* d_res, T* d_c0_out, T* d_c2_out, int K = 3,
-                           int kk = 2, double scale = 2.0) {
+                           int kk = 2, double scale = 2.0, const T* d_wmul = nullptr) {
   const uint64_t units = npoints * S;
   CU(ctx->stde_tmp.ensure(units * (uint64_t)K * sizeof(T)));
   SweepIO io;
@@ -818,7 +818,7 @@ static ech_status stde_run(ech_ctx* ctx, ech_tape* t, const T* d_x, bool x_bcast
   const T* c0 = (const T*)ctx->stde_tmp.p;
   const T* c2 = c0 + (uint64_t)kk * units;
   if (d_res) {
-    CU(launch_stde_reduce_t(sizeof(T) == 8, acc64, c0, c2, scale, npoints, S, d_cv, trace, control, d_res,
+    CU(launch_stde_reduce_t(sizeof(T) == 8, acc64, c0, c2, scale, npoints, S, d_cv, trace, control, d_wmul, d_res,
                             ctx->stream));
   }
   if (d_c0_out) CU(cudaMemcpyAsync(d_c0_out, c0, units * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
@@ -955,6 +955,72 @@ ECH_API ech_status ech_laplacian_batch_device(ech_ctx* ctx, const ech_tape* tc, 
   else
     s = stde_run<float>(ctx, t, (const float*)xs, false, B, S, (const float*)dirs, dir_mode, seed, true, nullptr, 0.0,
                         0, results, nullptr, nullptr);
+  ctx->stream = saved;
+  return s;
+}
+
+// Exact Hessian diagonals of many points: order-3 jets along every basis
+// direction (dir_mode 3), diag[b][j] = 2 * c2.
+ECH_API ech_status ech_hessian_diagonal_batch_device(ech_ctx* ctx, const ech_tape* tc, int f64, const void* xs,
+                                                     uint32_t B, void* diag, void* stream) {
+  CHECK(common_checks(ctx, tc, f64 != 0));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(stde_checks(t, t->host.ni, "hessian_diagonal_batch", "Hessian diagonal"));
+  CHECK(batch_args(t, B));
+  if (!xs || !diag) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  cudaStream_t saved = ctx->stream;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->stream;
+  const uint32_t n = t->host.ni;
+  ech_status s;
+  if (f64)
+    s = stde_run<double>(ctx, t, (const double*)xs, false, B, n, nullptr, 3, 0, true, nullptr, 0.0, 0, nullptr,
+                         nullptr, (double*)diag);
+  else
+    s = stde_run<float>(ctx, t, (const float*)xs, false, B, n, nullptr, 3, 0, true, nullptr, 0.0, 0, nullptr,
+                        nullptr, (float*)diag);
+  if (s == ECH_OK) {
+    cudaError_t e = launch_scale(f64 != 0, diag, 2.0, (size_t)B * n, ctx->stream);
+    if (e != cudaSuccess) s = cuda_fail(e, "scale");
+  }
+  ctx->stream = saved;
+  return s;
+}
+
+// Sparse STDE trace estimator over many points: per point S coordinates drawn
+// from `probs` [B][n] (fp32 rows, e.g. the learned proposal) or uniformly
+// (probs == NULL), one order-3 jet along each sampled e_j, samples 2*c2 / p_j,
+// FP64 Welford per point.  The estimate is unbiased for sum_j H_jj.
+ECH_API ech_status ech_sparse_trace_batch_device(ech_ctx* ctx, const ech_tape* tc, int f64, const void* xs,
+                                                 uint32_t B, const float* probs, uint32_t S, uint64_t seed,
+                                                 ech_estimator_result* results, void* stream) {
+  CHECK(common_checks(ctx, tc, f64 != 0));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(stde_checks(t, t->host.ni, "sparse_trace_batch", "trace"));
+  CHECK(batch_args(t, B));
+  if (S == 0) return fail(ECH_ERR_OTHER, "sampled_indices must not be empty");
+  if (!xs || !results) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  const uint64_t units = (uint64_t)B * S;
+  const size_t vb = f64 ? 8 : 4;
+  CU(ctx->io_in2.ensure(units * (sizeof(uint32_t) + vb) + 256));
+  uint32_t* d_idx = (uint32_t*)ctx->io_in2.p;
+  void* d_w = (unsigned char*)ctx->io_in2.p + ((units * sizeof(uint32_t) + 255) & ~(uint64_t)255);
+  cudaStream_t saved = ctx->stream;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->stream;
+  ech_status s = ECH_OK;
+  cudaError_t e = launch_sample_coords(f64 != 0, probs, t->host.ni, B, S, seed, d_idx, d_w, ctx->stream);
+  if (e != cudaSuccess) s = cuda_fail(e, "coordinate sampling");
+  if (s == ECH_OK) {
+    if (f64)
+      s = stde_run<double>(ctx, t, (const double*)xs, false, B, S, (const double*)(const void*)d_idx, 4, seed, true,
+                           nullptr, 0.0, 0, results, nullptr, nullptr, 3, 2, 2.0, (const double*)d_w);
+    else
+      s = stde_run<float>(ctx, t, (const float*)xs, false, B, S, (const float*)(const void*)d_idx, 4, seed, true,
+                          nullptr, 0.0, 0, results, nullptr, nullptr, 3, 2, 2.0, (const float*)d_w);
+  }
   ctx->stream = saved;
   return s;
 }

@@ -22,6 +22,7 @@
 #include <stdint.h>
 #include "ech_types.h"
 #include "device_math.cuh"
+#include "rng.cuh"
 
 namespace ech {
 
@@ -51,7 +52,8 @@ struct KParams {
   uint32_t* err;         // error word (KErr bits)
   // STDE: units = points * S; directions from host or device RNG
   uint32_t S;            // directions per point (0 = not STDE)
-  int dir_mode;          // 0: v per unit, 1: v shared [S][ni], 2: device Rademacher, 3: basis e_s
+  int dir_mode;          // 0: v per unit, 1: v shared [S][ni], 2: device Rademacher, 3: basis e_s,
+                         // 4: basis e_{v[u]} (v: one uint32 coordinate per unit)
   uint64_t seed;
 };
 
@@ -256,23 +258,6 @@ template <class T> struct Lane<dm::Dual<T>> {
   }
 };
 
-// Philox-4x32-10 (Salmon et al., SC'11) keyed by `seed`; counter (point, dir, i).
-__device__ __forceinline__ uint32_t philox_bits(uint64_t seed, uint64_t point, uint32_t dir, uint32_t i) {
-  uint32_t c0 = (uint32_t)point, c1 = (uint32_t)(point >> 32), c2 = dir, c3 = i;
-  uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-#pragma unroll
-  for (int r = 0; r < 10; ++r) {
-    const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
-    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
-    const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
-    const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
-    const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
-    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
-    k0 += 0x9E3779B9u;
-    k1 += 0xBB67AE85u;
-  }
-  return c0;
-}
 
 // Direction component for Taylor units; STDE units are (point = u / S, dir = u % S).
 template <class T, int K> struct Lane<dm::Jet<T, K>> {
@@ -283,6 +268,7 @@ template <class T, int K> struct Lane<dm::Jet<T, K>> {
     const uint32_t s = (uint32_t)(u - pt * kp.S);
     if (kp.dir_mode == 1) return v[(uint64_t)s * kp.ni + i];
     if (kp.dir_mode == 3) return (i == s) ? T(1) : T(0);
+    if (kp.dir_mode == 4) return (i == reinterpret_cast<const uint32_t*>(kp.v)[u]) ? T(1) : T(0);
     return (philox_bits(kp.seed, pt, s, i) & 1u) ? T(1) : T(-1);
   }
   static __device__ __forceinline__ dm::Jet<T, K> make_input(const KParams& kp, uint64_t u, uint32_t i, bool valid) {

@@ -46,8 +46,13 @@ cudaError_t launch_multi_hvp(bool f64, int P, const MultiParams& mp, int grid, i
 // STDE per-point reduction of scale*c_k samples (Welford in direction order);
 // acc64 selects a double accumulator for f32 samples.
 cudaError_t launch_stde_reduce_t(bool f64, bool acc64, const void* c0, const void* ck, double scale, uint64_t npoints,
-                                 uint32_t S, const void* cv, double trace, int control, void* results,
-                                 cudaStream_t st);
+                                 uint32_t S, const void* cv, double trace, int control, const void* wmul,
+                                 void* results, cudaStream_t st);
+// S coordinates per point from probability rows (or uniform when probs is null),
+// with their importance weights; y *= a.
+cudaError_t launch_sample_coords(bool f64, const float* probs, uint32_t n, uint64_t npoints, uint32_t S,
+                                 uint64_t seed, uint32_t* idx, void* wmul, cudaStream_t st);
+cudaError_t launch_scale(bool f64, void* y, double a, size_t n, cudaStream_t st);
 cudaError_t launch_control_term(bool f64, const void* dirs, const void* diag, uint32_t S, uint32_t n, void* cv,
                                 cudaStream_t st);
 

@@ -15,6 +15,7 @@
 
 #include "../../include/echidna_b200.h"
 #include "launch.h"
+#include "rng.cuh"
 
 namespace ech {
 
@@ -55,14 +56,17 @@ struct Welford {
 // One thread per point: samples scale*c_k of units [p*S, (p+1)*S) (scale 2,
 // k = 2 for the Laplacian; k!, k for k-th order diagonals), optionally minus a
 // control term cv[s] plus `trace` (laplacian_with_control).
+// With `wmul`, each sample is also multiplied by its unit's weight (importance
+// sampling: 1 / p of the sampled coordinate).
 template <class T, class Acc>
 __global__ void stde_reduce_kernel(const T* c0, const T* ck, T scale, uint64_t npoints, uint32_t S, const T* cv,
-                                   T trace, int control, ech_estimator_result* out) {
+                                   T trace, int control, const T* wmul, ech_estimator_result* out) {
   const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npoints) return;
   Welford<Acc> acc;
   for (uint32_t s = 0; s < S; ++s) {
-    const T vhv = scale * ck[p * S + s];
+    T vhv = scale * ck[p * S + s];
+    if (wmul) vhv = vhv * wmul[p * S + s];
     if (control) acc.update((Acc)(vhv - cv[s]));
     else acc.update((Acc)vhv);
   }
@@ -93,24 +97,24 @@ __global__ void control_term_kernel(const T* dirs, const T* diag, uint32_t S, ui
 }
 
 cudaError_t launch_stde_reduce_t(bool f64, bool acc64, const void* c0, const void* c2, double scale, uint64_t npoints,
-                                 uint32_t S, const void* cv, double trace, int control, void* results,
-                                 cudaStream_t st) {
+                                 uint32_t S, const void* cv, double trace, int control, const void* wmul,
+                                 void* results, cudaStream_t st) {
   const int threads = 128;
   const unsigned blocks = (unsigned)((npoints + threads - 1) / threads);
   if (blocks == 0) return cudaSuccess;
   if (f64) {
     stde_reduce_kernel<double, double><<<blocks, threads, 0, st>>>((const double*)c0, (const double*)c2, scale, npoints, S,
-                                                                   (const double*)cv, trace, control,
+                                                                   (const double*)cv, trace, control, (const double*)wmul,
                                                                    (ech_estimator_result*)results);
   } else if (acc64) {
     stde_reduce_kernel<float, double><<<blocks, threads, 0, st>>>((const float*)c0, (const float*)c2, (float)scale,
                                                                   npoints, S,
-                                                                  (const float*)cv, (float)trace, control,
+                                                                  (const float*)cv, (float)trace, control, (const float*)wmul,
                                                                   (ech_estimator_result*)results);
   } else {
     stde_reduce_kernel<float, float><<<blocks, threads, 0, st>>>((const float*)c0, (const float*)c2, (float)scale,
                                                                  npoints, S,
-                                                                 (const float*)cv, (float)trace, control,
+                                                                 (const float*)cv, (float)trace, control, (const float*)wmul,
                                                                  (ech_estimator_result*)results);
   }
   return cudaGetLastError();
@@ -125,6 +129,82 @@ cudaError_t launch_control_term(bool f64, const void* dirs, const void* diag, ui
     control_term_kernel<double><<<blocks, threads, 0, st>>>((const double*)dirs, (const double*)diag, S, n, (double*)cv);
   else
     control_term_kernel<float><<<blocks, threads, 0, st>>>((const float*)dirs, (const float*)diag, S, n, (float*)cv);
+  return cudaGetLastError();
+}
+
+// Coordinate sampling for sparse STDE: one block per point draws S coordinates
+// from the row of `probs` (inverse CDF of the row's prefix sums) or uniformly
+// (probs == nullptr), with Philox uniforms keyed by (seed, point, sample), and
+// records each sample's importance weight total / p_j (n for uniform draws).
+template <class T>
+__global__ void sample_coords_kernel(const float* probs, uint32_t n, uint64_t npoints, uint32_t S, uint64_t seed,
+                                     uint32_t* idx, T* wmul) {
+  extern __shared__ double cdf[];
+  const uint64_t pt = blockIdx.x;
+  if (pt >= npoints) return;
+  const float* row = probs ? probs + pt * n : nullptr;
+  if (row && threadIdx.x == 0) {
+    double acc = 0.0;
+    for (uint32_t j = 0; j < n; ++j) {
+      acc += (double)row[j];
+      cdf[j] = acc;
+    }
+  }
+  __syncthreads();
+  const double total = row ? cdf[n - 1] : 1.0;
+  for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
+    const double u = (double)philox_uniform(seed, pt, s, 0);
+    uint32_t j;
+    T w;
+    if (row) {
+      const double target = u * total;
+      uint32_t lo = 0, hi = n - 1;  // first j with cdf[j] > target
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (cdf[mid] > target) hi = mid;
+        else lo = mid + 1;
+      }
+      j = lo;
+      const double pj = fmax((double)row[j], 1e-30) / total;
+      w = (T)(1.0 / pj);
+    } else {
+      j = min((uint32_t)(u * (double)n), n - 1);
+      w = (T)n;
+    }
+    idx[pt * S + s] = j;
+    wmul[pt * S + s] = w;
+  }
+}
+
+template <class T>
+__global__ void scale_kernel(T* y, T a, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = a * y[i];
+}
+
+cudaError_t launch_sample_coords(bool f64, const float* probs, uint32_t n, uint64_t npoints, uint32_t S,
+                                 uint64_t seed, uint32_t* idx, void* wmul, cudaStream_t st) {
+  if (npoints == 0) return cudaSuccess;
+  const size_t smem = probs ? (size_t)n * sizeof(double) : 0;
+  if (smem > 48 * 1024) {
+    cudaError_t e = f64 ? cudaFuncSetAttribute(sample_coords_kernel<double>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                        : cudaFuncSetAttribute(sample_coords_kernel<float>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  if (f64)
+    sample_coords_kernel<double><<<(unsigned)npoints, 128, smem, st>>>(probs, n, npoints, S, seed, idx, (double*)wmul);
+  else
+    sample_coords_kernel<float><<<(unsigned)npoints, 128, smem, st>>>(probs, n, npoints, S, seed, idx, (float*)wmul);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scale(bool f64, void* y, double a, size_t n, cudaStream_t st) {
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  if (blocks == 0) return cudaSuccess;
+  if (f64) scale_kernel<double><<<blocks, 256, 0, st>>>((double*)y, a, n);
+  else scale_kernel<float><<<blocks, 256, 0, st>>>((float*)y, (float)a, n);
   return cudaGetLastError();
 }
 

@@ -46,14 +46,16 @@ class ProposalMLP:
                                               ctypes.c_float(lr), ctypes.byref(loss)))
         return float(loss.value)
 
-    def probs(self, x, out=None, stream: int = 0):
+    def probs(self, x, out=None, stream=None):
+        """softmax(MLP(x)) for a device tensor x [B, n_in], on torch's current stream
+        unless ``stream`` is given."""
         import torch
         B = int(x.shape[0])
         if out is None:
             out = torch.empty((B, self.n_out), dtype=torch.float32, device=x.device)
+        if stream is None:
+            stream = torch.cuda.current_stream().cuda_stream
         _check(_lib.load().ech_mlp_forward(self._h, x.data_ptr(), B, out.data_ptr(), ctypes.c_void_p(stream)))
-        if stream == 0:
-            torch.cuda.synchronize()
         return out
 
     def weights(self):
@@ -71,3 +73,108 @@ class ProposalMLP:
             self.close()
         except Exception:
             pass
+
+
+_RESULT_DTYPE = [("value", "f8"), ("estimate", "f8"), ("sample_variance", "f8"), ("standard_error", "f8"),
+                 ("num_samples", "u8")]
+
+
+def _stream(stream):
+    """The CUDA stream to enqueue on: torch's current stream unless one is given,
+    so the engine's work is ordered with the torch ops around it."""
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return stream
+
+
+def _settle(ctx, stream):
+    """Stream handle 0 means the context's own stream to the C ABI; wait for it so
+    that later work on torch's default stream sees the results."""
+    if stream == 0:
+        _check(_lib.load().ech_ctx_synchronize(ctx._h))
+
+
+def hessian_diagonals(ctx, tape, X, stream=None):
+    """Exact Hessian diagonals of every row of the device tensor X [B, n]
+    (``ech_hessian_diagonal_batch_device``); returns a device tensor [B, n]."""
+    import torch
+    out = torch.empty_like(X)
+    st = _stream(stream)
+    _check(_lib.load().ech_hessian_diagonal_batch_device(ctx._h, tape._h, int(tape.f64), X.data_ptr(), X.shape[0],
+                                                         out.data_ptr(), ctypes.c_void_p(st)))
+    _settle(ctx, st)
+    return out
+
+
+def sparse_trace(ctx, tape, X, probs, num_samples: int, seed: int, results=None, stream=None):
+    """Per-row sparse STDE trace estimates (``ech_sparse_trace_batch_device``): coordinates
+    drawn from ``probs`` [B, n] (fp32 device tensor) or uniformly (``probs=None``).
+    Returns a device tensor of B estimator records (5 float64 words each)."""
+    import torch
+    B = int(X.shape[0])
+    if results is None:
+        results = torch.empty((B, 5), dtype=torch.float64, device=X.device)
+    st = _stream(stream)
+    _check(_lib.load().ech_sparse_trace_batch_device(
+        ctx._h, tape._h, int(tape.f64), X.data_ptr(), B, None if probs is None else probs.data_ptr(),
+        int(num_samples), ctypes.c_uint64(seed & 0xFFFFFFFFFFFFFFFF), results.data_ptr(), ctypes.c_void_p(st)))
+    _settle(ctx, st)
+    return results
+
+
+def as_records(results) -> np.ndarray:
+    """Device result tensor -> structured numpy array (value, estimate, ..., num_samples)."""
+    raw = results.cpu().numpy()
+    out = np.zeros(raw.shape[0], dtype=_RESULT_DTYPE)
+    for k, (name, _) in enumerate(_RESULT_DTYPE[:4]):
+        out[name] = raw[:, k]
+    out["num_samples"] = raw[:, 4].view(np.uint64)
+    return out
+
+
+def target_distribution(diag):
+    """q_j = |H_jj| / sum_k |H_kk| per row (device tensors)."""
+    a = diag.abs().double()
+    return (a / a.sum(dim=1, keepdim=True).clamp_min(1e-300)).float()
+
+
+def samples_to_tolerance(diag, probs, rel: float = 0.01):
+    """Samples an importance-sampled trace estimator needs for a relative standard
+    error of ``rel``: per-sample variance sum_j d_j^2 / p_j - T^2 over (rel*T)^2.
+    ``probs=None`` is the uniform proposal (p_j = 1/n).  Rows of float64 numpy arrays."""
+    d = np.asarray(diag, dtype=np.float64)
+    n = d.shape[1]
+    T = d.sum(axis=1)
+    if probs is None:
+        second = n * (d * d).sum(axis=1)
+    else:
+        p = np.asarray(probs, dtype=np.float64)
+        p = p / p.sum(axis=1, keepdims=True)
+        second = (d * d / np.maximum(p, 1e-300)).sum(axis=1)
+    var = np.maximum(second - T * T, 0.0)
+    return var / (rel * T) ** 2, var, T
+
+
+def exact_diagonals(ctx, tape64, X64, chunk: int = 4096):
+    """Exact FP64 Hessian diagonals of the rows of X64 [N, n], in chunks."""
+    import torch
+    parts = [hessian_diagonals(ctx, tape64, X64[i:i + chunk].contiguous()) for i in range(0, X64.shape[0], chunk)]
+    return torch.cat(parts)
+
+
+def train_proposal(ctx, tape64, X64, hidden: int = 256, steps: int = 400, batch: int = 256, lr: float = 1e-3,
+                   seed: int = 0):
+    """Trains the proposal on exact diagonals of the training points X64 [N, n]
+    (FP64 labels from the tape's own jets); returns (mlp, losses)."""
+    import torch
+    n = int(X64.shape[1])
+    q = target_distribution(exact_diagonals(ctx, tape64, X64))
+    xf = X64.float()
+    mlp = ProposalMLP(ctx, n, hidden, n, seed=seed)
+    g = torch.Generator(device=X64.device).manual_seed(seed)
+    losses = []
+    for _ in range(steps):
+        rows = torch.randint(0, X64.shape[0], (batch,), device=X64.device, generator=g)
+        losses.append(mlp.train_step(xf[rows].contiguous(), q[rows].contiguous(), lr=lr))
+    return mlp, losses

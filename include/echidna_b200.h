@@ -265,6 +265,21 @@ ECH_API ech_status ech_multi_launch(ech_multi* multi, void* stream);
 ECH_API ech_status ech_multi_info(const ech_multi* multi, uint64_t* info);
 ECH_API void ech_multi_destroy(ech_multi* multi);
 
+/* Extension: exact Hessian diagonals of many points (device arrays): xs [B][n]
+ * -> diag [B][n] = 2 * c2 of order-3 jets along every e_j (the batched form of
+ * hessian_diagonal_gpu, src/gpu/stde_gpu.rs:103-129, with the values on the GPU). */
+ECH_API ech_status ech_hessian_diagonal_batch_device(ech_ctx* ctx, const ech_tape* tape, int f64, const void* xs,
+                                                     uint32_t batch_size, void* diag, void* stream);
+/* Extension: sparse STDE trace estimate sum_j H_jj for many points (device
+ * arrays).  Per point, S coordinates are drawn from the fp32 probability row
+ * probs[b][*] (NULL: uniform, as stde::diagonal_kth_order_stochastic with k = 2)
+ * with a device Philox stream keyed by `seed`; each sample is 2*c2 / p_j of an
+ * order-3 jet along e_j; results[B] are FP64 Welford statistics of the samples
+ * (estimate = their mean, unbiased for the trace). */
+ECH_API ech_status ech_sparse_trace_batch_device(ech_ctx* ctx, const ech_tape* tape, int f64, const void* xs,
+                                                 uint32_t batch_size, const float* probs, uint32_t num_samples,
+                                                 uint64_t seed, ech_estimator_result* results, void* stream);
+
 /* ── learned sampling proposal for sparse STDE (extension, no reference counterpart) ──
  * A softmax MLP n_in -> hidden -> hidden -> n_out (ReLU), trained on the GPU with
  * BF16 tensor-core GEMMs (tcgen05, FP32 accumulation) and Adam on FP32 master
