@@ -16,6 +16,9 @@ Workloads (``--workload``, default ``mlp``):
   counts; one step = gradient + per-point HVP of all of them in one persistent
   launch (FP32), compared in ``detail`` with one launch per tape and with a
   CUDA-graph replay of the persistent launch.
+* ``learned`` — sparse STDE of a 1,024-input softplus chain with the learned
+  proposal (BF16 tcgen05 MLP trained in setup on exact diagonals) vs uniform
+  sampling; ``detail`` has the samples and wall time to 1 % relative error.
 
 Reported per line:
 
@@ -492,7 +495,161 @@ class UnevenWorkload:
         return pts / dt, f"{pts} points (up to {k} per tape): oracle gradient + per-point HVP (f64), {dt:.1f} s"
 
 
-WORKLOADS = {"mlp": MlpWorkload, "rosenbrock": RosenbrockWorkload, "stde": StdeWorkload, "uneven": UnevenWorkload}
+class LearnedWorkload:
+    """C5: sparse STDE trace of f = sum a_i softplus(x_i x_{i+1}) + sum a_i cos x_i (n = 1,024,
+    a_i log-uniform in [1e-3, 1e3]) with the learned proposal vs uniform sampling.  Setup
+    labels training points with exact FP64 diagonals from the tape's jets and trains the
+    1024-256-256-1024 BF16 MLP on the GPU; the timed step is the learned estimator (MLP +
+    256 sampled jets per point, FP32 jets, FP64 Welford) over 1,024 held-out points.
+    ``detail`` gives the samples and wall time each proposal needs for 1 % relative error."""
+    name = "learned"
+    n = 1024
+    batch = 1024          # held-out points per timed step
+    S = 256               # samples per point in the timed step
+    launches_per_step = 10  # MLP: 3 conversions, 3 GEMMs, softmax; sampler, jet sweep, reduction
+    n_train = 16384
+    n_eval = 1024
+
+    def __init__(self, rank, world):
+        from echidna_b200 import configs
+        self.seed = configs.SEEDS["softplus_chain"]
+        self.tape = configs.softplus_chain(self.n)
+        rng = np.random.default_rng([self.seed, rank])
+        self.Xtr = rng.normal(size=(self.n_train, self.n))
+        self.Xev = rng.normal(size=(self.n_eval, self.n))
+
+    def describe(self):
+        return {"workload": "learned STDE proposal: softplus-chain n=1024, MLP 1024-256-256-1024 (BF16 tcgen05, "
+                            "FP32 accumulation) trained on exact FP64 diagonals; learned vs uniform sparse STDE",
+                "eval_points": self.batch, "samples_per_point_in_step": self.S,
+                "training_points": self.n_train}, "f32"
+
+    def setup(self, ctx, lib, torch, sp):
+        from echidna_b200 import learned
+        from echidna_b200.gpu import GpuTapeData
+        self.ctx, self.lib, self.sp, self.torch = ctx, lib, sp, torch
+        self.g64 = ctx.upload_tape_f64(self.tape)
+        self.g32 = ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(self.tape))
+        # labels and training run on the default stream, before the timed stream is used
+        with torch.cuda.stream(torch.cuda.default_stream()):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            xtr = torch.tensor(self.Xtr, device="cuda")
+            d = learned.exact_diagonals(ctx, self.g64, xtr)
+            torch.cuda.synchronize()
+            self.t_labels = time.perf_counter() - t0
+            q = learned.target_distribution(d)
+            t0 = time.perf_counter()
+            self.mlp = learned.ProposalMLP(ctx, self.n, 256, self.n, seed=self.seed)
+            g = torch.Generator(device="cuda").manual_seed(self.seed)
+            xf = xtr.float()
+            self.losses = []
+            for _ in range(1500):
+                rows = torch.randint(0, self.n_train, (512,), device="cuda", generator=g)
+                self.losses.append(self.mlp.train_step(xf[rows].contiguous(), q[rows].contiguous(), lr=1e-3))
+            torch.cuda.synchronize()
+            self.t_train = time.perf_counter() - t0
+            xev = torch.tensor(self.Xev, device="cuda")
+            self.d_eval = learned.exact_diagonals(ctx, self.g64, xev).cpu().numpy()
+            self.xev32 = xev.float().contiguous()
+            self.p_eval = self.mlp.probs(self.xev32).cpu().numpy()
+            torch.cuda.synchronize()
+        self.probs = torch.empty((self.batch, self.n), dtype=torch.float32, device="cuda")
+        self.res = torch.empty((self.batch, 5), dtype=torch.float64, device="cuda")
+        self.hX = _pinned(torch, self.Xev.astype(np.float32))
+        self.h_res = _pinned(torch, np.empty((self.batch, 5)))
+
+    def _learned(self, S):
+        from echidna_b200 import learned
+        self.mlp.probs(self.xev32, out=self.probs, stream=self.sp)
+        learned.sparse_trace(self.ctx, self.g32, self.xev32, self.probs, S, self.seed, self.res, stream=self.sp)
+
+    def _uniform(self, S):
+        from echidna_b200 import learned
+        learned.sparse_trace(self.ctx, self.g32, self.xev32, None, S, self.seed, self.res, stream=self.sp)
+
+    def kernels(self):
+        return [("learned estimator (MLP + sampled jets)", lambda: self._learned(self.S))]
+
+    def extra(self, torch, stream, flush, steps):
+        from echidna_b200 import learned
+        ev = lambda: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))  # noqa: E731
+        def timed(fn):
+            fn()
+            torch.cuda.synchronize()
+            ts = []
+            for _ in range(steps):
+                flush.zero_()
+                e0, e1 = ev()
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            return float(np.mean(ts))
+        t_learn = timed(lambda: self._learned(self.S))
+        t_unif = timed(lambda: self._uniform(self.S))
+        t_mlp = timed(lambda: self.mlp.probs(self.xev32, out=self.probs, stream=self.sp))
+        s_u, _, T = learned.samples_to_tolerance(self.d_eval, None)
+        s_l, _, _ = learned.samples_to_tolerance(self.d_eval, self.p_eval)
+        s_b, _, _ = learned.samples_to_tolerance(self.d_eval, np.abs(self.d_eval))
+        per_sample_l = (t_learn - t_mlp) / (self.batch * self.S)   # ms per sampled jet
+        per_sample_u = t_unif / (self.batch * self.S)
+        med_l, med_u = float(np.median(s_l)), float(np.median(s_u))
+        time_l = med_l * per_sample_l + t_mlp / self.batch
+        time_u = med_u * per_sample_u
+        # empirical check on 32 points at their own 1% sample counts (capped)
+        k = 32
+        S_chk = int(min(np.ceil(med_l), 200000))
+        x = self.xev32[:k].contiguous()
+        pr = self.mlp.probs(x)
+        r = learned.as_records(learned.sparse_trace(self.ctx, self.g32, x, pr, S_chk, self.seed + 1))
+        rel = np.abs(r["estimate"] - T[:k]) / np.abs(T[:k])
+        return {"samples_to_1pct_median": {"uniform": med_u, "learned": med_l, "best_possible": float(np.median(s_b))},
+                "time_to_1pct_ms_per_point_median": {"uniform": time_u, "learned": time_l,
+                                                     "learned_speedup": time_u / time_l},
+                "per_sample_jet_us": {"uniform": per_sample_u * 1e3, "learned": per_sample_l * 1e3},
+                "mlp_forward_ms_per_1024_points": t_mlp, "uniform_step_ms": t_unif,
+                "check_32_points_at_median_samples": {"samples": S_chk,
+                                                      "median_relative_error": float(np.median(rel))},
+                "labels_s": self.t_labels, "training_s": self.t_train, "loss_first_last": [self.losses[0],
+                                                                                          self.losses[-1]]}
+
+    def e2e_step(self):
+        torch = self.torch
+        x = torch.from_numpy(self.hX).to("cuda", non_blocking=True)
+        from echidna_b200 import learned
+        pr = self.mlp.probs(x, out=self.probs, stream=self.sp)
+        learned.sparse_trace(self.ctx, self.g32, x, pr, self.S, self.seed, self.res, stream=self.sp)
+        self.h_res_t = self.res.to("cpu", non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    def io_bytes(self):
+        return int(self.hX.nbytes), int(self.batch * 40)
+
+    def roofline_inputs(self, kernel):
+        st = self.ctx.plan_stats(self.g32, "taylor", 3)
+        units = self.batch * self.S
+        return int(units * 4 * (self.n / self.S + 3)), units * st["flops_fwd"]
+
+    def detail(self):
+        return {"plan_taylor3": self.ctx.plan_stats(self.g32, "taylor", 3)}
+
+    def cpu_reference(self, budget_s, nthreads):
+        """Uniform sparse STDE on the reference CPU path (diagonal_kth_order_stochastic, k=2)."""
+        from oracle.oracle import OracleTape
+        o = OracleTape(self.tape)
+        rng = np.random.default_rng(self.seed)
+        pts, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < budget_s / 4 and pts < 256:
+            o.diagonal_kth_order_stochastic(self.Xev[pts], 2, rng.integers(0, self.n, size=self.S))
+            pts += 1
+        dt = time.perf_counter() - t0
+        return pts / dt, f"{pts} points x {self.S} uniform samples: oracle diagonal_kth_order_stochastic (k=2, f64, 1 thread), {dt:.1f} s"
+
+
+WORKLOADS = {"mlp": MlpWorkload, "rosenbrock": RosenbrockWorkload, "stde": StdeWorkload, "uneven": UnevenWorkload,
+             "learned": LearnedWorkload}
 
 
 # ───────────────────────────── arms ──────────────────────────────────────────
