@@ -77,6 +77,16 @@ _SIGS = {
     "ech_hvp_batch_device": ([_P, _P, _I, _P, _I, _P, _U32, _P, _P, _P], _I),
     "ech_taylor_batch_device": ([_P, _P, _I, _P, _P, _U32, _U32, _P, _P], _I),
     "ech_noalloc_region_bytes": ([], _SZ),
+    "ech_laplacian_hutchpp_f32": ([_P, _P, _P, _SZ, _P, _U32, _P, _U32, _P], _I),
+    "ech_parabolic_diffusion_f32": ([_P, _P, _P, _SZ, _P, _U32, _P, _P], _I),
+    "ech_parabolic_diffusion_stochastic_f32": ([_P, _P, _P, _SZ, _P, _U32, _P, _U32, _P], _I),
+    "ech_dense_stde_2nd_f32": ([_P, _P, _P, _SZ, _P, _P, _U32, _P], _I),
+    "ech_divergence_f32": ([_P, _P, _P, _SZ, _P, _U32, _P, _P], _I),
+    "ech_laplacian_hutchpp_f64": ([_P, _P, _P, _SZ, _P, _U32, _P, _U32, _P], _I),
+    "ech_parabolic_diffusion_f64": ([_P, _P, _P, _SZ, _P, _U32, _P, _P], _I),
+    "ech_parabolic_diffusion_stochastic_f64": ([_P, _P, _P, _SZ, _P, _U32, _P, _U32, _P], _I),
+    "ech_dense_stde_2nd_f64": ([_P, _P, _P, _SZ, _P, _P, _U32, _P], _I),
+    "ech_divergence_f64": ([_P, _P, _P, _SZ, _P, _U32, _P, _P], _I),
     "ech_hessian_diagonal_batch_device": ([_P, _P, _I, _P, _U32, _P, _P], _I),
     "ech_sparse_trace_batch_device": ([_P, _P, _I, _P, _U32, _P, _U32, _U64, _P, _P], _I),
     "ech_gemm_bf16": ([_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P], _I),

@@ -9,7 +9,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <map>
+#include <cmath>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -1096,6 +1098,285 @@ ECH_API ech_status ech_diagonal_kth_order_stochastic_f64(ech_ctx* ctx, const ech
                                                          size_t n_indices, ech_estimator_result* out) {
   return do_diag_kth<double>(ctx, t, x, n, k, sampled_indices, n_indices, out);
 }
+
+// ── estimators built on order-3 jets along host-built directions ──
+// (src/stde/laplacian.rs:252-344, src/stde/pde.rs:11-330).  The jets run on the
+// GPU; the direction algebra (mat-vecs, projections, Gram-Schmidt) and the
+// statistics follow the reference's host code, in the sample type and order.
+
+// Welford's update as WelfordAccumulator (src/stde/types.rs:44-113), host side.
+template <class T>
+struct HostWelford {
+  T mean = T(0), m2 = T(0);
+  uint64_t count = 0;
+  void update(T s) {
+    if (!std::isfinite(s)) return;
+    count += 1;
+    const T k = (T)count;
+    const T d = s - mean;
+    mean = mean + d / k;
+    const T d2 = s - mean;
+    m2 = m2 + d * d2;
+  }
+  void finalize(T* est, T* var, T* se) const {
+    if (count == 0) { *est = std::numeric_limits<T>::quiet_NaN(); *var = T(0); *se = T(0); return; }
+    if (count == 1) { *est = mean; *var = T(0); *se = T(0); return; }
+    const T v = std::max(m2 / ((T)count - T(1)), T(0));
+    *est = mean;
+    *var = v;
+    *se = std::sqrt(v / (T)count);
+  }
+};
+
+// c0 and c2 of order-3 jets of the scalar-output tape along S host directions
+// [S][n] at one point x.
+template <class T>
+static ech_status jets_along(ech_ctx* ctx, ech_tape* t, const T* x, size_t n, const T* dirs, uint32_t S,
+                             std::vector<T>& c0, std::vector<T>& c2) {
+  c0.assign(S, T(0));
+  c2.assign(S, T(0));
+  if (S == 0) return ECH_OK;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  CU(ctx->io_in.ensure(n * sizeof(T)));
+  CU(ctx->io_in2.ensure((size_t)S * n * sizeof(T)));
+  CU(ctx->io_out.ensure((size_t)S * sizeof(T)));
+  CU(ctx->io_out2.ensure((size_t)S * sizeof(T)));
+  CU(cudaMemcpyAsync(ctx->io_in.p, x, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(ctx->io_in2.p, dirs, (size_t)S * n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  CHECK(stde_run<T>(ctx, t, (const T*)ctx->io_in.p, true, 1, S, (const T*)ctx->io_in2.p, 1, 0, false, nullptr, 0.0,
+                    0, nullptr, (T*)ctx->io_out.p, (T*)ctx->io_out2.p));
+  CU(cudaMemcpyAsync(c0.data(), ctx->io_out.p, (size_t)S * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaMemcpyAsync(c2.data(), ctx->io_out2.p, (size_t)S * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return check_err_word(ctx);
+}
+
+template <class T>
+static T fold_dot(const T* a, const T* b, size_t n) {
+  T acc = T(0);
+  for (size_t i = 0; i < n; ++i) acc = acc + a[i] * b[i];
+  return acc;
+}
+
+static void put_result(ech_estimator_result* out, double value, double est, double var, double se, uint64_t n) {
+  out->value = value;
+  out->estimate = est;
+  out->sample_variance = var;
+  out->standard_error = se;
+  out->num_samples = n;
+}
+
+// laplacian_hutchpp (src/stde/laplacian.rs:252-344)
+template <class T>
+static ech_status do_hutchpp(ech_ctx* ctx, const ech_tape* tc, const T* x, size_t n, const T* sketch, uint32_t k,
+                             const T* stoch, uint32_t m, ech_estimator_result* out) {
+  CHECK(common_checks(ctx, tc, sizeof(T) == 8));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(stde_checks(t, n, "laplacian_hutchpp", "Laplacian"));
+  if (k == 0) return fail(ECH_ERR_OTHER, "sketch_directions must not be empty");
+  if (m == 0) return fail(ECH_ERR_OTHER, "stochastic_directions must not be empty");
+  if (!x || !sketch || !stoch || !out) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  // 1. sketch: H s for every sketch direction (one HVP batch at one x)
+  std::vector<T> grads((size_t)k * n), hs((size_t)k * n);
+  CHECK(do_hvp<T>(ctx, t, x, n, false, sketch, (size_t)k * n, k, grads.data(), grads.size(), hs.data(), hs.size()));
+  // 2. modified Gram-Schmidt with the reference's drop rule (norm < sqrt(eps))
+  const T eps = std::sqrt(std::numeric_limits<T>::epsilon());
+  std::vector<std::vector<T>> cols(k);
+  for (uint32_t j = 0; j < k; ++j) cols[j].assign(hs.begin() + (size_t)j * n, hs.begin() + (size_t)(j + 1) * n);
+  size_t rank = 0, i = 0;
+  while (i < cols.size()) {
+    for (size_t j = 0; j < rank; ++j) {
+      const T dot = fold_dot(cols[j].data(), cols[i].data(), n);
+      for (size_t e = 0; e < n; ++e) cols[i][e] = cols[i][e] - dot * cols[j][e];
+    }
+    T nsq = T(0);
+    for (size_t e = 0; e < n; ++e) nsq = nsq + cols[i][e] * cols[i][e];
+    const T norm = std::sqrt(nsq);
+    if (norm < eps) {
+      std::swap(cols[i], cols.back());
+      cols.pop_back();
+    } else {
+      const T inv = T(1) / norm;
+      for (size_t e = 0; e < n; ++e) cols[i][e] = cols[i][e] * inv;
+      if (i != rank) std::swap(cols[i], cols[rank]);
+      ++rank;
+      ++i;
+    }
+  }
+  // 3. exact trace on span(Q)
+  std::vector<T> qd(rank * n), c0, c2;
+  for (size_t j = 0; j < rank; ++j) std::copy(cols[j].begin(), cols[j].end(), qd.begin() + j * n);
+  CHECK(jets_along<T>(ctx, t, x, n, qd.data(), (uint32_t)rank, c0, c2));
+  T value = T(0), exact = T(0);
+  for (size_t j = 0; j < rank; ++j) {
+    value = c0[j];
+    exact = exact + T(2) * c2[j];
+  }
+  // 4. Hutchinson on the residual: g' = g - Q (Q^T g), dots with the original g
+  std::vector<T> proj((size_t)m * n);
+  for (uint32_t g = 0; g < m; ++g) {
+    const T* gv = stoch + (size_t)g * n;
+    T* pv = proj.data() + (size_t)g * n;
+    std::copy(gv, gv + n, pv);
+    for (size_t j = 0; j < rank; ++j) {
+      const T dot = fold_dot(cols[j].data(), gv, n);
+      for (size_t e = 0; e < n; ++e) pv[e] = pv[e] - dot * cols[j][e];
+    }
+  }
+  CHECK(jets_along<T>(ctx, t, x, n, proj.data(), m, c0, c2));
+  HostWelford<T> acc;
+  for (uint32_t g = 0; g < m; ++g) {
+    value = c0[g];
+    acc.update(T(2) * c2[g]);
+  }
+  T mean, var, se;
+  acc.finalize(&mean, &var, &se);
+  put_result(out, (double)value, (double)(exact + mean), (double)var, (double)se, acc.count);
+  return ECH_OK;
+}
+
+// parabolic_diffusion (src/stde/pde.rs:128-162): (value, 1/2 sum_i 2 c2 along sigma columns)
+template <class T>
+static ech_status do_parabolic(ech_ctx* ctx, const ech_tape* tc, const T* x, size_t n, const T* sigma, uint32_t d,
+                               T* value, T* estimate) {
+  CHECK(common_checks(ctx, tc, sizeof(T) == 8));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(stde_checks(t, n, "parabolic_diffusion", "diffusion term"));
+  if (d == 0) return fail(ECH_ERR_OTHER, "sigma_columns must not be empty");
+  if (!x || !sigma || !value || !estimate) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  std::vector<T> c0, c2;
+  CHECK(jets_along<T>(ctx, t, x, n, sigma, d, c0, c2));
+  T v = T(0), sum = T(0);
+  for (uint32_t i = 0; i < d; ++i) {
+    v = c0[i];
+    sum = sum + T(2) * c2[i];
+  }
+  *value = v;
+  *estimate = T(0.5) * sum;
+  return ECH_OK;
+}
+
+// parabolic_diffusion_stochastic (src/stde/pde.rs:164-240)
+template <class T>
+static ech_status do_parabolic_stoch(ech_ctx* ctx, const ech_tape* tc, const T* x, size_t n, const T* sigma,
+                                     uint32_t d, const uint32_t* idx, uint32_t m, ech_estimator_result* out) {
+  CHECK(common_checks(ctx, tc, sizeof(T) == 8));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(stde_checks(t, n, "parabolic_diffusion_stochastic", "diffusion term"));
+  if (m == 0) return fail(ECH_ERR_OTHER, "sampled_indices must not be empty");
+  if (!x || !sigma || !idx || !out) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  std::vector<T> dirs((size_t)m * n);
+  for (uint32_t s = 0; s < m; ++s) {
+    if (idx[s] >= d) {
+      char buf[96];
+      snprintf(buf, sizeof buf, "sampled index %u out of bounds (d=%u)", idx[s], d);
+      return fail(ECH_ERR_OTHER, buf);
+    }
+    std::copy(sigma + (size_t)idx[s] * n, sigma + (size_t)(idx[s] + 1) * n, dirs.begin() + (size_t)s * n);
+  }
+  std::vector<T> c0, c2;
+  CHECK(jets_along<T>(ctx, t, x, n, dirs.data(), m, c0, c2));
+  HostWelford<T> acc;
+  T value = T(0);
+  for (uint32_t s = 0; s < m; ++s) {
+    value = c0[s];
+    acc.update(T(2) * c2[s]);
+  }
+  T mean, var, se;
+  acc.finalize(&mean, &var, &se);
+  const T scale = (T)d * T(0.5);
+  put_result(out, (double)value, (double)(mean * scale), (double)(var * scale * scale), (double)(se * scale),
+             acc.count);
+  return ECH_OK;
+}
+
+// dense_stde_2nd (src/stde/pde.rs:242-296): samples 2 c2 along v = L z, L lower
+// triangular (row-major n x n, entries above the diagonal ignored).
+template <class T>
+static ech_status do_dense_stde(ech_ctx* ctx, const ech_tape* tc, const T* x, size_t n, const T* L, const T* z,
+                                uint32_t m, ech_estimator_result* out) {
+  CHECK(common_checks(ctx, tc, sizeof(T) == 8));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(stde_checks(t, n, "dense_stde_2nd", "operator"));
+  if (m == 0) return fail(ECH_ERR_OTHER, "z_vectors must not be empty");
+  if (!x || !L || !z || !out) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  std::vector<T> dirs((size_t)m * n);
+  for (uint32_t s = 0; s < m; ++s) {
+    const T* zs = z + (size_t)s * n;
+    for (size_t i = 0; i < n; ++i) {
+      T sum = T(0);
+      for (size_t j = 0; j <= i; ++j) sum = sum + L[i * n + j] * zs[j];
+      dirs[(size_t)s * n + i] = sum;
+    }
+  }
+  std::vector<T> c0, c2;
+  CHECK(jets_along<T>(ctx, t, x, n, dirs.data(), m, c0, c2));
+  HostWelford<T> acc;
+  T value = T(0);
+  for (uint32_t s = 0; s < m; ++s) {
+    value = c0[s];
+    acc.update(T(2) * c2[s]);
+  }
+  T mean, var, se;
+  acc.finalize(&mean, &var, &se);
+  put_result(out, (double)value, (double)mean, (double)var, (double)se, acc.count);
+  return ECH_OK;
+}
+
+// divergence (src/stde/pde.rs:52-106): samples v^T J v from JVPs of a square tape.
+template <class T>
+static ech_status do_divergence(ech_ctx* ctx, const ech_tape* tc, const T* x, size_t n, const T* dirs, uint32_t m,
+                                T* values, ech_estimator_result* out) {
+  CHECK(common_checks(ctx, tc, sizeof(T) == 8));
+  const ech_tape* t = tc;
+  const size_t no = t->host.outs.size();
+  if (no != t->host.ni) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "divergence requires num_outputs (%zu) == num_inputs (%u)", no, t->host.ni);
+    return fail(ECH_ERR_OTHER, buf);
+  }
+  if (m == 0) return fail(ECH_ERR_OTHER, "directions must not be empty");
+  if (n != t->host.ni) return fail(ECH_ERR_INVALID_ARG, "x length must match the tape's num_inputs");
+  if (!x || !dirs || !out) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  std::vector<T> xs((size_t)m * n), vals((size_t)m * no), tans((size_t)m * no);
+  for (uint32_t s = 0; s < m; ++s) std::copy(x, x + n, xs.begin() + (size_t)s * n);
+  CHECK(do_tangent<T>(ctx, tc, xs.data(), xs.size(), dirs, (size_t)m * n, m, vals.data(), tans.data(), vals.size()));
+  HostWelford<T> acc;
+  for (uint32_t s = 0; s < m; ++s) acc.update(fold_dot(dirs + (size_t)s * n, tans.data() + (size_t)s * no, n));
+  if (values) std::copy(vals.begin(), vals.begin() + no, values);
+  T mean, var, se;
+  acc.finalize(&mean, &var, &se);
+  put_result(out, 0.0, (double)mean, (double)var, (double)se, acc.count);
+  return ECH_OK;
+}
+
+#define ECH_STDE_OPS(SUF, T)                                                                                       \
+  ECH_API ech_status ech_laplacian_hutchpp_##SUF(ech_ctx* c, const ech_tape* t, const T* x, size_t n,             \
+                                                 const T* sketch, uint32_t k, const T* stoch, uint32_t m,          \
+                                                 ech_estimator_result* out) {                                      \
+    return do_hutchpp<T>(c, t, x, n, sketch, k, stoch, m, out);                                                    \
+  }                                                                                                                \
+  ECH_API ech_status ech_parabolic_diffusion_##SUF(ech_ctx* c, const ech_tape* t, const T* x, size_t n,           \
+                                                   const T* sigma, uint32_t d, T* value, T* estimate) {            \
+    return do_parabolic<T>(c, t, x, n, sigma, d, value, estimate);                                                 \
+  }                                                                                                                \
+  ECH_API ech_status ech_parabolic_diffusion_stochastic_##SUF(ech_ctx* c, const ech_tape* t, const T* x, size_t n, \
+                                                              const T* sigma, uint32_t d, const uint32_t* idx,     \
+                                                              uint32_t m, ech_estimator_result* out) {             \
+    return do_parabolic_stoch<T>(c, t, x, n, sigma, d, idx, m, out);                                               \
+  }                                                                                                                \
+  ECH_API ech_status ech_dense_stde_2nd_##SUF(ech_ctx* c, const ech_tape* t, const T* x, size_t n, const T* L,    \
+                                              const T* z, uint32_t m, ech_estimator_result* out) {                 \
+    return do_dense_stde<T>(c, t, x, n, L, z, m, out);                                                             \
+  }                                                                                                                \
+  ECH_API ech_status ech_divergence_##SUF(ech_ctx* c, const ech_tape* t, const T* x, size_t n, const T* dirs,      \
+                                          uint32_t m, T* values, ech_estimator_result* out) {                      \
+    return do_divergence<T>(c, t, x, n, dirs, m, values, out);                                                     \
+  }
+ECH_STDE_OPS(f32, float)
+ECH_STDE_OPS(f64, double)
+#undef ECH_STDE_OPS
 
 extern "C" {
 

@@ -99,3 +99,65 @@ def diagonal_kth_order_stochastic_gpu(backend: CudaContext, tape, x, k: int, sam
     fn = lib.ech_diagonal_kth_order_stochastic_f64 if f64 else lib.ech_diagonal_kth_order_stochastic_f32
     _check(fn(backend._h, tape._h, _lib.ptr(xx), xx.size, int(k), _lib.ptr(idx), idx.size, ctypes.byref(r)))
     return _result(r, float)
+
+
+# ── operator estimators (src/stde/laplacian.rs:252-344, src/stde/pde.rs) ──
+
+def _fn(tape, name):
+    lib = _lib.load()
+    return getattr(lib, f"ech_{name}_{'f64' if tape.f64 else 'f32'}"), (np.float64 if tape.f64 else np.float32)
+
+
+def laplacian_hutchpp_gpu(backend: CudaContext, tape, x, sketch_directions, stochastic_directions) -> EstimatorResult:
+    """``stde::laplacian_hutchpp``: exact trace on the span of H*S, Hutchinson on the rest."""
+    fn, dt = _fn(tape, "laplacian_hutchpp")
+    xx = np.ascontiguousarray(x, dtype=dt).ravel()
+    S = np.ascontiguousarray(sketch_directions, dtype=dt).reshape(-1, xx.size)
+    G = np.ascontiguousarray(stochastic_directions, dtype=dt).reshape(-1, xx.size)
+    r = _lib.EstimatorResultC()
+    _check(fn(backend._h, tape._h, _lib.ptr(xx), xx.size, _lib.ptr(S), S.shape[0], _lib.ptr(G), G.shape[0],
+              ctypes.byref(r)))
+    return _result(r)
+
+
+def parabolic_diffusion_gpu(backend: CudaContext, tape, x, sigma_columns):
+    """``stde::parabolic_diffusion``: (value, 1/2 sum_i (sigma e_i)^T H (sigma e_i))."""
+    fn, dt = _fn(tape, "parabolic_diffusion")
+    xx = np.ascontiguousarray(x, dtype=dt).ravel()
+    sig = np.ascontiguousarray(sigma_columns, dtype=dt).reshape(-1, xx.size)
+    v, e = np.zeros(1, dt), np.zeros(1, dt)
+    _check(fn(backend._h, tape._h, _lib.ptr(xx), xx.size, _lib.ptr(sig), sig.shape[0], _lib.ptr(v), _lib.ptr(e)))
+    return float(v[0]), float(e[0])
+
+
+def parabolic_diffusion_stochastic_gpu(backend: CudaContext, tape, x, sigma_columns, sampled_indices):
+    fn, dt = _fn(tape, "parabolic_diffusion_stochastic")
+    xx = np.ascontiguousarray(x, dtype=dt).ravel()
+    sig = np.ascontiguousarray(sigma_columns, dtype=dt).reshape(-1, xx.size)
+    idx = np.ascontiguousarray(sampled_indices, dtype=np.uint32).ravel()
+    r = _lib.EstimatorResultC()
+    _check(fn(backend._h, tape._h, _lib.ptr(xx), xx.size, _lib.ptr(sig), sig.shape[0], _lib.ptr(idx), idx.size,
+              ctypes.byref(r)))
+    return _result(r)
+
+
+def dense_stde_2nd_gpu(backend: CudaContext, tape, x, cholesky, z_vectors) -> EstimatorResult:
+    """``stde::dense_stde_2nd``: samples (L z)^T H (L z), L lower triangular [n, n]."""
+    fn, dt = _fn(tape, "dense_stde_2nd")
+    xx = np.ascontiguousarray(x, dtype=dt).ravel()
+    L = np.ascontiguousarray(cholesky, dtype=dt).reshape(xx.size, xx.size)
+    Z = np.ascontiguousarray(z_vectors, dtype=dt).reshape(-1, xx.size)
+    r = _lib.EstimatorResultC()
+    _check(fn(backend._h, tape._h, _lib.ptr(xx), xx.size, _lib.ptr(L), _lib.ptr(Z), Z.shape[0], ctypes.byref(r)))
+    return _result(r)
+
+
+def divergence_gpu(backend: CudaContext, tape, x, directions):
+    """``stde::divergence``: (values, estimate of tr J from v^T J v samples)."""
+    fn, dt = _fn(tape, "divergence")
+    xx = np.ascontiguousarray(x, dtype=dt).ravel()
+    V = np.ascontiguousarray(directions, dtype=dt).reshape(-1, xx.size)
+    vals = np.zeros(xx.size, dt)
+    r = _lib.EstimatorResultC()
+    _check(fn(backend._h, tape._h, _lib.ptr(xx), xx.size, _lib.ptr(V), V.shape[0], _lib.ptr(vals), ctypes.byref(r)))
+    return vals, _result(r)

@@ -280,6 +280,46 @@ ECH_API ech_status ech_sparse_trace_batch_device(ech_ctx* ctx, const ech_tape* t
                                                  uint32_t batch_size, const float* probs, uint32_t num_samples,
                                                  uint64_t seed, ech_estimator_result* results, void* stream);
 
+/* ── operator estimators on jets (host buffers; the jets run on the GPU) ──────
+ * laplacian_hutchpp (src/stde/laplacian.rs:252-344): sketch [k][n] HVPs, modified
+ * Gram-Schmidt (columns with norm < sqrt(eps) dropped), exact trace on the span,
+ * Hutchinson on the projected stochastic directions [m][n]. */
+ECH_API ech_status ech_laplacian_hutchpp_f32(ech_ctx* ctx, const ech_tape* tape, const float* x, size_t n,
+                                             const float* sketch, uint32_t k, const float* stochastic, uint32_t m,
+                                             ech_estimator_result* out);
+ECH_API ech_status ech_laplacian_hutchpp_f64(ech_ctx* ctx, const ech_tape* tape, const double* x, size_t n,
+                                             const double* sketch, uint32_t k, const double* stochastic, uint32_t m,
+                                             ech_estimator_result* out);
+/* parabolic_diffusion (src/stde/pde.rs:128-162): value and 1/2 sum_i (sigma e_i)^T H (sigma e_i)
+ * over the columns sigma [d][n]. */
+ECH_API ech_status ech_parabolic_diffusion_f32(ech_ctx* ctx, const ech_tape* tape, const float* x, size_t n,
+                                               const float* sigma_columns, uint32_t d, float* value, float* estimate);
+ECH_API ech_status ech_parabolic_diffusion_f64(ech_ctx* ctx, const ech_tape* tape, const double* x, size_t n,
+                                               const double* sigma_columns, uint32_t d, double* value, double* estimate);
+/* parabolic_diffusion_stochastic (src/stde/pde.rs:164-240): sampled columns, estimate d/2 * mean. */
+ECH_API ech_status ech_parabolic_diffusion_stochastic_f32(ech_ctx* ctx, const ech_tape* tape, const float* x,
+                                                          size_t n, const float* sigma_columns, uint32_t d,
+                                                          const uint32_t* sampled_indices, uint32_t m,
+                                                          ech_estimator_result* out);
+ECH_API ech_status ech_parabolic_diffusion_stochastic_f64(ech_ctx* ctx, const ech_tape* tape, const double* x,
+                                                          size_t n, const double* sigma_columns, uint32_t d,
+                                                          const uint32_t* sampled_indices, uint32_t m,
+                                                          ech_estimator_result* out);
+/* dense_stde_2nd (src/stde/pde.rs:242-296): samples 2 c2 along L z (L row-major n x n,
+ * lower triangle used), z_vectors [m][n]. */
+ECH_API ech_status ech_dense_stde_2nd_f32(ech_ctx* ctx, const ech_tape* tape, const float* x, size_t n,
+                                          const float* cholesky, const float* z_vectors, uint32_t m,
+                                          ech_estimator_result* out);
+ECH_API ech_status ech_dense_stde_2nd_f64(ech_ctx* ctx, const ech_tape* tape, const double* x, size_t n,
+                                          const double* cholesky, const double* z_vectors, uint32_t m,
+                                          ech_estimator_result* out);
+/* divergence (src/stde/pde.rs:52-106): v^T J v over directions [m][n] of a tape with
+ * num_outputs == num_inputs; values[n] receives the outputs (may be NULL). */
+ECH_API ech_status ech_divergence_f32(ech_ctx* ctx, const ech_tape* tape, const float* x, size_t n,
+                                      const float* directions, uint32_t m, float* values, ech_estimator_result* out);
+ECH_API ech_status ech_divergence_f64(ech_ctx* ctx, const ech_tape* tape, const double* x, size_t n,
+                                      const double* directions, uint32_t m, double* values, ech_estimator_result* out);
+
 /* ── learned sampling proposal for sparse STDE (extension, no reference counterpart) ──
  * A softmax MLP n_in -> hidden -> hidden -> n_out (ReLU), trained on the GPU with
  * BF16 tensor-core GEMMs (tcgen05, FP32 accumulation) and Adam on FP32 master
