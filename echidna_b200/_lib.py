@@ -77,6 +77,7 @@ _SIGS = {
     "ech_hvp_batch_device": ([_P, _P, _I, _P, _I, _P, _U32, _P, _P, _P], _I),
     "ech_taylor_batch_device": ([_P, _P, _I, _P, _P, _U32, _U32, _P, _P], _I),
     "ech_noalloc_region_bytes": ([], _SZ),
+    "ech_grad_checkpointed_device": ([_P, _P, _P, _I, _P, _U32, _U32, _U32, _P], _I),
     "ech_laplacian_hutchpp_f32": ([_P, _P, _P, _SZ, _P, _U32, _P, _U32, _P], _I),
     "ech_parabolic_diffusion_f32": ([_P, _P, _P, _SZ, _P, _U32, _P, _P], _I),
     "ech_parabolic_diffusion_stochastic_f32": ([_P, _P, _P, _SZ, _P, _U32, _P, _U32, _P], _I),

@@ -110,6 +110,8 @@ struct ech_tape {
   std::map<std::tuple<int, int, uint32_t, uint32_t, uint32_t>, std::unique_ptr<HostProgram>> host_programs;
   // autotuned launch shapes, keyed (kind, K, log2 of the unit count)
   std::map<std::tuple<int, int, int>, Shape> shapes;
+  // for a step map x -> step(x): the tape of sum_j w_j step(x)_j over inputs (x, w)
+  std::unique_ptr<ech_tape> vjp;
 };
 
 // ───────────────────────────── context ──────────────────────────────────────
@@ -1377,6 +1379,187 @@ static ech_status do_divergence(ech_ctx* ctx, const ech_tape* tc, const T* x, si
 ECH_STDE_OPS(f32, float)
 ECH_STDE_OPS(f64, double)
 #undef ECH_STDE_OPS
+
+// ── checkpointed gradients of iterated maps (src/checkpoint.rs:67-126, 548-722) ──
+// x_{t+1} = step(x_t) for t < T, objective loss(x_T); gradient w.r.t. x_0 for a
+// batch of starting points.  Only the states at the checkpoint positions are
+// kept; every reverse segment recomputes its states from its checkpoint, then
+// pulls the adjoint back through each step with a vector-Jacobian product.
+// The VJP of a step is the gradient of s = sum_j w_j step(x)_j over the inputs
+// (x, w): the step tape with n extra inputs w and the weighted sum appended.
+
+static HostTape vjp_tape_of(const HostTape& h) {
+  const uint32_t n = h.ni, shift = n;
+  HostTape v;
+  v.ni = 2 * n;
+  auto map = [&](uint32_t s) { return s < n ? s : s + shift; };
+  for (uint32_t i = 0; i < n; ++i) {
+    v.op.push_back(OP_INPUT); v.a0.push_back(kUnused); v.a1.push_back(kUnused); v.vals.push_back(h.vals[i]);
+  }
+  for (uint32_t i = 0; i < n; ++i) {
+    v.op.push_back(OP_INPUT); v.a0.push_back(kUnused); v.a1.push_back(kUnused); v.vals.push_back(0.0);
+  }
+  for (uint32_t i = n; i < h.nv; ++i) {
+    const uint32_t o = h.op[i];
+    v.op.push_back(o);
+    v.vals.push_back(h.vals[i]);
+    if (o == OP_CONST) { v.a0.push_back(kUnused); v.a1.push_back(kUnused); continue; }
+    v.a0.push_back(map(h.a0[i]));
+    v.a1.push_back((o == OP_POWI || h.a1[i] == kUnused) ? h.a1[i] : map(h.a1[i]));
+  }
+  uint32_t s = kUnused;
+  for (uint32_t j = 0; j < (uint32_t)h.outs.size(); ++j) {
+    const uint32_t m = (uint32_t)v.op.size();
+    v.op.push_back(OP_MUL); v.a0.push_back(n + j); v.a1.push_back(map(h.outs[j])); v.vals.push_back(0.0);
+    if (s == kUnused) {
+      s = m;
+    } else {
+      v.op.push_back(OP_ADD); v.a0.push_back(s); v.a1.push_back(m); v.vals.push_back(0.0);
+      s = (uint32_t)v.op.size() - 1;
+    }
+  }
+  v.nv = (uint32_t)v.op.size();
+  v.out_index = s;
+  v.outs.assign(1, s);
+  return v;
+}
+
+// Stored positions, spread evenly: j * N / (C + 1) for j = 1..C; every step
+// when C >= N (spread_positions / revolve_schedule, src/checkpoint.rs:673-722).
+static std::vector<uint32_t> spread_positions(uint32_t steps, uint32_t ckpts) {
+  std::vector<uint32_t> p;
+  if (ckpts >= steps) {
+    for (uint32_t s = 1; s < steps; ++s) p.push_back(s);
+    return p;
+  }
+  for (uint32_t j = 1; j <= ckpts; ++j) p.push_back((uint32_t)((uint64_t)j * steps / (ckpts + 1)));
+  std::sort(p.begin(), p.end());
+  p.erase(std::unique(p.begin(), p.end()), p.end());
+  return p;
+}
+
+template <class T>
+static ech_status do_grad_ckpt(ech_ctx* ctx, const ech_tape* sc, const ech_tape* lc, const T* x0, uint32_t B,
+                               uint32_t steps, uint32_t ckpts, T* grads) {
+  const bool f64 = sizeof(T) == 8;
+  CHECK(common_checks(ctx, sc, f64));
+  CHECK(common_checks(ctx, lc, f64));
+  ech_tape* st = const_cast<ech_tape*>(sc);
+  ech_tape* lt = const_cast<ech_tape*>(lc);
+  const uint32_t n = st->host.ni;
+  if (st->host.outs.size() != n) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "step must preserve dimension: expected %u, got %zu", n, st->host.outs.size());
+    return fail(ECH_ERR_OTHER, buf);
+  }
+  if (lt->host.ni != n || lt->host.outs.size() != 1)
+    return fail(ECH_ERR_OTHER, "loss must map the state dimension to one output");
+  CHECK(batch_args(st, B));
+  if (!x0 || !grads) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  {
+    std::lock_guard<std::mutex> lk(st->mu);
+    if (!st->vjp) {
+      st->vjp.reset(new ech_tape());
+      st->vjp->ctx = ctx;
+      st->vjp->f64 = st->f64;
+      st->vjp->host = vjp_tape_of(st->host);
+    }
+  }
+  ech_tape* vt = st->vjp.get();
+  const size_t row = (size_t)B * n * sizeof(T);
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  if (steps == 0) {  // gradient of loss(x0)
+    SweepIO io;
+    io.x = x0;
+    CU(ctx->io_out.ensure((size_t)B * sizeof(T)));
+    io.out = ctx->io_out.p;
+    io.out2 = grads;
+    CHECK(enqueue(ctx, lt, 1, 0, B, io, s));
+    CU(cudaStreamSynchronize(s));
+    return check_err_word(ctx);
+  }
+  const uint32_t c = std::min(std::max(ckpts, 1u), steps);
+  std::vector<uint32_t> pos = spread_positions(steps, c);
+  std::vector<uint32_t> seg_start(1, 0);
+  seg_start.insert(seg_start.end(), pos.begin(), pos.end());
+  uint32_t max_seg = 0;
+  for (size_t k = 0; k < seg_start.size(); ++k) {
+    const uint32_t e = k + 1 < seg_start.size() ? seg_start[k + 1] : steps;
+    max_seg = std::max(max_seg, e - seg_start[k]);
+  }
+  // buffers: checkpoints, one segment of states, (x | w) rows and their gradient, adjoint
+  DevBuf ck, states, xw, gw, adj, lossv;
+  CU(ck.ensure(row * seg_start.size()));
+  CU(states.ensure(row * (size_t)(max_seg + 1)));
+  CU(xw.ensure(2 * row));
+  CU(gw.ensure(2 * row));
+  CU(adj.ensure(row));
+  CU(lossv.ensure((size_t)B * sizeof(T)));
+  auto ckp = [&](size_t k) { return (unsigned char*)ck.p + k * row; };
+  auto stp = [&](size_t k) { return (unsigned char*)states.p + k * row; };
+  auto fwd = [&](const void* in, void* out) -> ech_status {
+    SweepIO io;
+    io.x = in;
+    io.out = out;
+    return enqueue(ctx, st, 0, 0, B, io, s);
+  };
+  // forward pass: keep the state at every checkpoint position
+  CU(cudaMemcpyAsync(ckp(0), x0, row, cudaMemcpyDeviceToDevice, s));
+  size_t next_ck = 1;
+  const void* cur = x0;
+  for (uint32_t t = 0; t < steps; ++t) {
+    void* out = stp(t & 1);
+    CHECK(fwd(cur, out));
+    if (next_ck < seg_start.size() && seg_start[next_ck] == t + 1) {
+      CU(cudaMemcpyAsync(ckp(next_ck), out, row, cudaMemcpyDeviceToDevice, s));
+      ++next_ck;
+    }
+    cur = out;
+  }
+  // the objective's gradient at the final state seeds the adjoint
+  {
+    SweepIO io;
+    io.x = cur;
+    io.out = lossv.p;
+    io.out2 = adj.p;
+    CHECK(enqueue(ctx, lt, 1, 0, B, io, s));
+  }
+  for (size_t seg = seg_start.size(); seg-- > 0;) {
+    const uint32_t a = seg_start[seg];
+    const uint32_t e = seg + 1 < seg_start.size() ? seg_start[seg + 1] : steps;
+    const uint32_t len = e - a;
+    CU(cudaMemcpyAsync(stp(0), ckp(seg), row, cudaMemcpyDeviceToDevice, s));
+    for (uint32_t i = 0; i < len; ++i) CHECK(fwd(stp(i), stp(i + 1)));
+    for (uint32_t i = len; i-- > 0;) {
+      // (x | w) rows = [states[i] | adjoint]
+      CU(cudaMemcpy2DAsync(xw.p, 2 * n * sizeof(T), stp(i), n * sizeof(T), n * sizeof(T), B,
+                           cudaMemcpyDeviceToDevice, s));
+      CU(cudaMemcpy2DAsync((unsigned char*)xw.p + n * sizeof(T), 2 * n * sizeof(T), adj.p, n * sizeof(T),
+                           n * sizeof(T), B, cudaMemcpyDeviceToDevice, s));
+      SweepIO io;
+      io.x = xw.p;
+      io.out = lossv.p;
+      io.out2 = gw.p;
+      CHECK(enqueue(ctx, vt, 1, 0, B, io, s));
+      CU(cudaMemcpy2DAsync(adj.p, n * sizeof(T), gw.p, 2 * n * sizeof(T), n * sizeof(T), B,
+                           cudaMemcpyDeviceToDevice, s));
+    }
+  }
+  CU(cudaMemcpyAsync(grads, adj.p, row, cudaMemcpyDeviceToDevice, s));
+  CU(cudaStreamSynchronize(s));
+  return check_err_word(ctx);
+}
+
+ECH_API ech_status ech_grad_checkpointed_device(ech_ctx* ctx, const ech_tape* step, const ech_tape* loss, int f64,
+                                                const void* x0, uint32_t B, uint32_t num_steps,
+                                                uint32_t num_checkpoints, void* grads) {
+  if (!ctx || !step || !loss) return fail(ECH_ERR_INVALID_ARG, "null argument");
+  return f64 ? do_grad_ckpt<double>(ctx, step, loss, (const double*)x0, B, num_steps, num_checkpoints,
+                                    (double*)grads)
+             : do_grad_ckpt<float>(ctx, step, loss, (const float*)x0, B, num_steps, num_checkpoints, (float*)grads);
+}
 
 extern "C" {
 

@@ -320,6 +320,18 @@ ECH_API ech_status ech_divergence_f32(ech_ctx* ctx, const ech_tape* tape, const 
 ECH_API ech_status ech_divergence_f64(ech_ctx* ctx, const ech_tape* tape, const double* x, size_t n,
                                       const double* directions, uint32_t m, double* values, ech_estimator_result* out);
 
+/* grad_checkpointed (src/checkpoint.rs:67-126) for a batch of starting points:
+ * x_{t+1} = step(x_t) (a tape with num_outputs == num_inputs = n), objective
+ * loss(x_T) (n inputs, one output); grads [B][n] = d loss / d x_0.  Only the
+ * states at min(max(num_checkpoints, 1), num_steps) evenly spread positions are
+ * kept; each reverse segment recomputes its states from its checkpoint and pulls
+ * the adjoint back one step at a time (vector-Jacobian products as gradients of
+ * sum_j w_j step(x)_j).  Device arrays; synchronous.  num_steps = 0 gives the
+ * gradient of loss(x_0). */
+ECH_API ech_status ech_grad_checkpointed_device(ech_ctx* ctx, const ech_tape* step, const ech_tape* loss, int f64,
+                                                const void* x0, uint32_t batch_size, uint32_t num_steps,
+                                                uint32_t num_checkpoints, void* grads);
+
 /* ── learned sampling proposal for sparse STDE (extension, no reference counterpart) ──
  * A softmax MLP n_in -> hidden -> hidden -> n_out (ReLU), trained on the GPU with
  * BF16 tensor-core GEMMs (tcgen05, FP32 accumulation) and Adam on FP32 master
