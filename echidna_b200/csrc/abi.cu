@@ -65,13 +65,10 @@ struct DevPlan {
   Plan host;
   DIns* d_fwd = nullptr;
   DRIns* d_rev = nullptr;
-  DFTerm* d_fterms = nullptr;  // fused-chain terms (forward form)
-  DRTerm* d_rterms = nullptr;  // fused-chain terms (reverse form)
+  uint32_t n_fwd = 0, n_rev = 0;  // records of the device programs (chain terms inline)
   ~DevPlan() {
     if (d_fwd) cudaFree(d_fwd);
     if (d_rev) cudaFree(d_rev);
-    if (d_fterms) cudaFree(d_fterms);
-    if (d_rterms) cudaFree(d_rterms);
   }
 };
 
@@ -326,10 +323,8 @@ static ech_status get_plan(ech_tape* t, int kind, int K, uint32_t cap, uint32_t 
   CU(cudaMalloc(&dp->d_rev, std::max<size_t>(prog.rev.size(), 1) * sizeof(DRIns)));
   if (!prog.rev.empty())
     CU(cudaMemcpy(dp->d_rev, prog.rev.data(), prog.rev.size() * sizeof(DRIns), cudaMemcpyHostToDevice));
-  CU(cudaMalloc(&dp->d_fterms, prog.fterms.size() * sizeof(DFTerm)));
-  CU(cudaMemcpy(dp->d_fterms, prog.fterms.data(), prog.fterms.size() * sizeof(DFTerm), cudaMemcpyHostToDevice));
-  CU(cudaMalloc(&dp->d_rterms, prog.rterms.size() * sizeof(DRTerm)));
-  CU(cudaMemcpy(dp->d_rterms, prog.rterms.data(), prog.rterms.size() * sizeof(DRTerm), cudaMemcpyHostToDevice));
+  dp->n_fwd = (uint32_t)prog.fwd.size();
+  dp->n_rev = (uint32_t)prog.rev.size();
   *out = dp.get();
   t->plans[key] = std::move(dp);
   return ECH_OK;
@@ -358,11 +353,9 @@ static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_
   c.smem = kRingBytes + (size_t)regs * c.tile * c.vbytes;
   KParams kp{};
   kp.fwd = dp->d_fwd;
-  kp.n_fwd = (uint32_t)p.fwd.size();
+  kp.n_fwd = dp->n_fwd;
   kp.rev = dp->d_rev;
-  kp.n_rev = c.req.rev ? (uint32_t)p.rev.size() : 0u;
-  kp.fterms = dp->d_fterms;
-  kp.rterms = dp->d_rterms;
+  kp.n_rev = c.req.rev ? dp->n_rev : 0u;
   kp.far_slots = p.far_slots;
   kp.smem_regs = regs;
   kp.tile = c.tile;
@@ -1704,11 +1697,9 @@ static ech_status multi_prepare(ech_multi* m, Shape sh) {
     J j{};
     KParams& kp = j.job.kp;
     kp.fwd = dp->d_fwd;
-    kp.n_fwd = (uint32_t)p.fwd.size();
+    kp.n_fwd = dp->n_fwd;
     kp.rev = dp->d_rev;
-    kp.n_rev = (uint32_t)p.rev.size();
-    kp.fterms = dp->d_fterms;
-    kp.rterms = dp->d_rterms;
+    kp.n_rev = dp->n_rev;
     kp.far_slots = p.far_slots;
     kp.tile = c.tile;
     kp.n_units = it.n_points;
@@ -1721,7 +1712,7 @@ static ech_status multi_prepare(ech_multi* m, Shape sh) {
     kp.out3 = it.hvps;
     kp.err = ctx->d_err;
     j.tiles = (it.n_points + c.tile - 1) / c.tile;
-    j.cost = (uint64_t)p.fwd.size() + p.rev.size();
+    j.cost = (uint64_t)dp->n_fwd + dp->n_rev;
     js.push_back(j);
   }
   if (js.empty()) return fail(ECH_ERR_OTHER, "batch_size must be non-zero");

@@ -126,8 +126,15 @@ struct alignas(16) DRIns {
 };
 static_assert(sizeof(DRIns) == 48, "DRIns must be 48 bytes");
 
-// Chain terms as executed.  Forward: operand locations; reverse: adjoint
-// locations and trajectory offsets of the values an x*y term reads.
+// Chain terms as executed.  They travel inline in the program stream, right
+// after their chain instruction, in the order the executor consumes them, so
+// the TMA program ring stages them with the instructions:
+//   D_CHAIN    forward: n DFTerm records, term order
+//   D_CHAIN    reverse: n DRTerm records, last term first
+//   D_CHAIN_LC forward: ceil(n/2) DFPair records, terms (2k, 2k+1)
+//   D_CHAIN_LC reverse: ceil(n/2) DRPair records, terms (n-1-2k, n-2-2k)
+// Forward: operand locations; reverse: adjoint locations and trajectory
+// offsets of the values an x*y term reads.
 struct alignas(16) DFTerm {
   uint8_t kind, op, xm, ym;   // xm / ym: M_SMEM or M_GLOB
   uint32_t x, y;              // byte offsets
@@ -135,7 +142,7 @@ struct alignas(16) DFTerm {
   double c;
   uint64_t pad2;
 };
-static_assert(sizeof(DFTerm) == 32, "DFTerm must be 32 bytes");
+static_assert(sizeof(DFTerm) == sizeof(DIns), "forward term records are instruction-sized");
 struct alignas(16) DRTerm {
   uint8_t kind, op;
   uint16_t flags;             // ChainFlag bits
@@ -143,8 +150,26 @@ struct alignas(16) DRTerm {
   uint32_t vx, vy;            // trajectory byte offsets (x*y terms)
   uint32_t pad;
   double c;
+  uint64_t pad2[2];
 };
-static_assert(sizeof(DRTerm) == 32, "DRTerm must be 32 bytes");
+static_assert(sizeof(DRTerm) == sizeof(DRIns), "reverse term records are instruction-sized");
+// Two terms of a linear-combination chain (Mul(c, x) or Mul(x, c), added).
+struct alignas(16) DFPair {
+  double c[2];
+  uint32_t x[2];              // operand byte offsets
+  uint8_t m[2];               // M_SMEM / M_GLOB
+  uint8_t cx[2];              // 1: Mul(c, x), 0: Mul(x, c)
+  uint32_t pad;
+};
+static_assert(sizeof(DFPair) == sizeof(DIns), "forward term records are instruction-sized");
+struct alignas(16) DRPair {
+  double c[2];
+  uint32_t ax[2];             // adjoint byte offsets
+  uint16_t flags[2];          // ChainFlag bits (CF_X_INIT, CF_X_GLOB)
+  uint32_t pad;
+  uint64_t pad2[2];
+};
+static_assert(sizeof(DRPair) == sizeof(DRIns), "reverse term records are instruction-sized");
 
 // Interpreter geometry shared by every kernel.
 constexpr int kChunk = 128;   // instructions per staged chunk

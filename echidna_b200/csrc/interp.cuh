@@ -28,12 +28,10 @@ namespace ech {
 
 // ───────────────────────────── launch parameters ────────────────────────────
 struct KParams {
-  const DIns* fwd;       // forward program (device encoding)
-  uint32_t n_fwd;
+  const DIns* fwd;       // forward program (device encoding; chain terms inline)
+  uint32_t n_fwd;        // records
   const DRIns* rev;      // reverse program (gradient / HVP kinds)
   uint32_t n_rev;
-  const DFTerm* fterms;  // fused-chain terms, forward form (D_CHAIN)
-  const DRTerm* rterms;  // fused-chain terms, reverse form
   void* scratch;         // per-CTA global slot regions
   uint64_t scratch_stride_bytes;  // bytes per CTA region
   uint32_t far_slots;    // global slots before the trajectory region
@@ -141,40 +139,96 @@ __device__ __forceinline__ void ring_drain(Ring& rg) {
   rg.inflight = 0;
 }
 
-// Runs one program through the ring, calling exec(record) for each
-// instruction.  Returns false if a wait gave up (all threads agree).
+// Makes chunk `c` of a program current: waits (bounded) for its copy, and
+// once every thread has passed the barrier (so all are done with chunk c-1)
+// refills chunk c-1's stage with chunk c-1+kStages.  Returns the chunk's
+// record count, 0 when a wait gave up or the program ended early (every thread
+// sees the same value).  Out of line: it runs once per chunk.
+struct Chunk {
+  const unsigned char* base;
+  uint32_t count;
+};
+template <int REC>
+__device__ __noinline__ Chunk ring_chunk(Ring* rg, const unsigned char* prog, uint32_t nins, uint32_t c,
+                                         uint32_t* err) {
+  const uint32_t nchunks = (nins + kChunk - 1) / kChunk;
+  if (c >= nchunks) {  // a chain ran past the end of its program
+    if (threadIdx.x == 0) atomicOr(err, (uint32_t)KERR_BADINS);
+    ring_drain(*rg);
+    return {nullptr, 0u};
+  }
+  const uint32_t stage = rg->seq % kStages;
+  const bool ok = mbar_wait_bounded(rg->full + stage, (rg->seq / kStages) & 1u);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicOr(err, (uint32_t)KERR_TIMEOUT);
+    ring_drain(*rg);
+    return {nullptr, 0u};
+  }
+  if (threadIdx.x == 0) {
+    rg->inflight &= ~(1u << stage);
+    if (c > 0 && c - 1 + kStages < nchunks) {
+      fence_proxy_async();
+      ring_issue<REC>(*rg, prog, nins, c - 1 + kStages, (rg->seq + kStages - 1) % kStages);
+    }
+  }
+  rg->seq += 1;
+  return {rg->buf + (size_t)stage * kChunk * 48, min((uint32_t)kChunk, nins - c * kChunk)};
+}
+
+// The records of one program in order, read from the ring.  Executors pull
+// the records that follow an instruction (a chain's terms) with next(); every
+// thread pulls the same records.  A record's fields must be read before the
+// next pull, which may recycle its stage.
+template <int REC>
+struct Stream {
+  Ring* rg;
+  const unsigned char* prog;
+  uint32_t nins;
+  uint32_t* err;
+  const unsigned char* rec;  // next record in the current chunk
+  uint32_t left;             // records left in the current chunk
+  uint32_t chunk;            // chunks made current so far
+  bool failed;
+
+  __device__ __forceinline__ const unsigned char* next() {
+    if (left == 0) {
+      const Chunk ch = ring_chunk<REC>(rg, prog, nins, chunk, err);
+      if (ch.count == 0) {
+        failed = true;
+        return nullptr;
+      }
+      chunk += 1;
+      rec = ch.base;
+      left = ch.count;
+    }
+    const unsigned char* r = rec;
+    rec += REC;
+    left -= 1;
+    return r;
+  }
+};
+
+// Runs one program through the ring: exec(record, stream) per instruction
+// (chain instructions pull their terms from the stream).  Returns false if a
+// wait gave up or the program is malformed (all threads agree).
 template <int REC, class Exec>
 __device__ __forceinline__ bool run_program(Ring& rg, const unsigned char* prog, uint32_t nins, uint32_t* err,
                                             Exec& exec) {
-  const uint32_t nchunks = (nins + kChunk - 1) / kChunk;
-  if (nchunks == 0) return true;
+  if (nins == 0) return true;
   if (threadIdx.x == 0) {
     fence_proxy_async();
-    const uint32_t pre = min((uint32_t)kStages, nchunks);
+    const uint32_t pre = min((uint32_t)kStages, (nins + kChunk - 1) / kChunk);
     for (uint32_t c = 0; c < pre; ++c) ring_issue<REC>(rg, prog, nins, c, (rg.seq + c) % kStages);
   }
-  for (uint32_t c = 0; c < nchunks; ++c) {
-    const uint32_t stage = rg.seq % kStages;
-    const uint32_t parity = (rg.seq / kStages) & 1u;
-    const bool ok = mbar_wait_bounded(rg.full + stage, parity);
-    if (ok) {
-      if (threadIdx.x == 0) rg.inflight &= ~(1u << stage);
-      const uint32_t cnt = min((uint32_t)kChunk, nins - c * kChunk);
-      const unsigned char* base = rg.buf + (size_t)stage * kChunk * 48;
+  Stream<REC> st{&rg, prog, nins, err, nullptr, 0u, 0u, false};
+  const uint32_t total_chunks = (nins + kChunk - 1) / kChunk;
 #pragma unroll 1
-      for (uint32_t k = 0; k < cnt; ++k) exec(base + k * (uint32_t)REC);
-    }
-    if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) atomicOr(err, (uint32_t)KERR_TIMEOUT);
-      ring_drain(rg);
-      return false;
-    }
-    rg.seq += 1;
-    if (threadIdx.x == 0 && c + kStages < nchunks) {
-      fence_proxy_async();
-      ring_issue<REC>(rg, prog, nins, c + kStages, stage);
-    }
+  while (st.chunk < total_chunks || st.left > 0) {
+    const unsigned char* r = st.next();
+    if (r == nullptr || !exec(r, st)) return false;
   }
+  // every thread is done with the last chunk before the ring is refilled
+  __syncthreads();
   return true;
 }
 
@@ -346,15 +400,17 @@ template <class V, int P> struct FwdExec {
 
   // Fused chain s_t = s_{t-1} (+|-) term_t, t = 1..n, s_0 = acc0: the same
   // Mul / Add / Sub evaluations, in the same operand order, as the tape ops it
-  // replaces.  DFTerm layout: kind|op|xm|ym, x, y, pad | c, pad.
-  __device__ __forceinline__ void chain(uint32_t ma, uint32_t ao, double imm, uint32_t first, uint32_t n,
+  // replaces.  The n DFTerm records follow in the stream
+  // (kind|op|xm|ym, x, y, pad | c, pad).
+  __device__ __forceinline__ bool chain(Stream<32>& st, uint32_t ma, uint32_t ao, double imm, uint32_t n,
                                         V (&acc)[P]) const {
     ld(ma, ao, imm, acc);
-    const uint4* tp = reinterpret_cast<const uint4*>(kp.fterms + first);
 #pragma unroll 1
     for (uint32_t q = 0; q < n; ++q) {
-      const uint4 w0 = __ldg(tp + 2 * q);
-      const uint2 w1 = __ldg(reinterpret_cast<const uint2*>(tp + 2 * q + 1));
+      const unsigned char* rec = st.next();
+      if (rec == nullptr) return false;
+      const uint4 w0 = *reinterpret_cast<const uint4*>(rec);
+      const uint2 w1 = *reinterpret_cast<const uint2*>(rec + 16);
       const uint32_t kind = w0.x & 0xFFu, op = (w0.x >> 8) & 0xFFu;
       V t[P], x[P];
       if (kind == CK_C) {
@@ -397,48 +453,46 @@ template <class V, int P> struct FwdExec {
           break;
       }
     }
+    return true;
   }
 
   // Linear-combination chain: every term is Mul(c, x) or Mul(x, c) added to the
-  // running value, in tape order; two terms per iteration so their operand
-  // loads overlap.
-  __device__ __forceinline__ void chain_lc(uint32_t ma, uint32_t ao, double imm, uint32_t first, uint32_t n,
+  // running value, in tape order.  DFPair records carry two terms each
+  // (c0, c1 | x0, x1, m0|m1|cx0|cx1, pad), so both operand loads are issued
+  // before the arithmetic.
+  __device__ __forceinline__ bool chain_lc(Stream<32>& st, uint32_t ma, uint32_t ao, double imm, uint32_t n,
                                            V (&acc)[P]) const {
     ld(ma, ao, imm, acc);
-    const uint4* tp = reinterpret_cast<const uint4*>(kp.fterms + first);
-    uint32_t q = 0;
 #pragma unroll 1
-    for (; q + 2 <= n; q += 2) {
-      const uint4 a0 = __ldg(tp + 2 * q);
-      const uint2 a1 = __ldg(reinterpret_cast<const uint2*>(tp + 2 * q + 1));
-      const uint4 b0 = __ldg(tp + 2 * q + 2);
-      const uint2 b1 = __ldg(reinterpret_cast<const uint2*>(tp + 2 * q + 3));
-      V xa[P], xb[P];
-      ldv((a0.x >> 16) & 0xFFu, a0.y, xa);
-      ldv((b0.x >> 16) & 0xFFu, b0.y, xb);
-      const V ca = dm::VT<V>::cst(__hiloint2double((int)a1.y, (int)a1.x));
-      const V cb = dm::VT<V>::cst(__hiloint2double((int)b1.y, (int)b1.x));
-      const bool a_cx = (a0.x & 0xFFu) == CK_CX, b_cx = (b0.x & 0xFFu) == CK_CX;
+    for (uint32_t q = 0; q < n; q += 2) {
+      const unsigned char* rec = st.next();
+      if (rec == nullptr) return false;
+      const uint4 cw = *reinterpret_cast<const uint4*>(rec);
+      const uint4 xw = *reinterpret_cast<const uint4*>(rec + 16);
+      const V ca = dm::VT<V>::cst(__hiloint2double((int)cw.y, (int)cw.x));
+      const bool a_cx = ((xw.z >> 16) & 0xFFu) != 0;
+      V xa[P];
+      ldv(xw.z & 0xFFu, xw.x, xa);
+      if (q + 1 < n) {
+        V xb[P];
+        ldv((xw.z >> 8) & 0xFFu, xw.y, xb);
+        const V cb = dm::VT<V>::cst(__hiloint2double((int)cw.w, (int)cw.z));
+        const bool b_cx = (xw.z >> 24) != 0;
 #pragma unroll
-      for (int p = 0; p < P; ++p) {
-        const V ta = a_cx ? Kd::mul(ca, xa[p]) : Kd::mul(xa[p], ca);
-        const V tb = b_cx ? Kd::mul(cb, xb[p]) : Kd::mul(xb[p], cb);
-        acc[p] = Kd::add(Kd::add(acc[p], ta), tb);
+        for (int p = 0; p < P; ++p) {
+          const V ta = a_cx ? Kd::mul(ca, xa[p]) : Kd::mul(xa[p], ca);
+          const V tb = b_cx ? Kd::mul(cb, xb[p]) : Kd::mul(xb[p], cb);
+          acc[p] = Kd::add(Kd::add(acc[p], ta), tb);
+        }
+      } else {
+#pragma unroll
+        for (int p = 0; p < P; ++p) acc[p] = Kd::add(acc[p], a_cx ? Kd::mul(ca, xa[p]) : Kd::mul(xa[p], ca));
       }
     }
-    if (q < n) {
-      const uint4 a0 = __ldg(tp + 2 * q);
-      const uint2 a1 = __ldg(reinterpret_cast<const uint2*>(tp + 2 * q + 1));
-      V xa[P];
-      ldv((a0.x >> 16) & 0xFFu, a0.y, xa);
-      const V ca = dm::VT<V>::cst(__hiloint2double((int)a1.y, (int)a1.x));
-      const bool a_cx = (a0.x & 0xFFu) == CK_CX;
-#pragma unroll
-      for (int p = 0; p < P; ++p) acc[p] = Kd::add(acc[p], a_cx ? Kd::mul(ca, xa[p]) : Kd::mul(xa[p], ca));
-    }
+    return true;
   }
 
-  __device__ __forceinline__ void operator()(const unsigned char* raw) const {
+  __device__ __forceinline__ bool operator()(const unsigned char* raw, Stream<32>& st) const {
     const uint4 w0 = *reinterpret_cast<const uint4*>(raw);
     const uint4 w1 = *reinterpret_cast<const uint4*>(raw + 16);
     const uint32_t opc = w0.x & 0xFFu;
@@ -451,44 +505,44 @@ template <class V, int P> struct FwdExec {
 #pragma unroll
         for (int p = 0; p < P; ++p) r[p] = Lane<V>::make_input(kp, unit0 + p, (uint32_t)aux, valid[p]);
         put(w0.x >> 24, dof, save, r);
-        return;
+        return true;
       case D_STOUT:
         ld((w0.x >> 8) & 0xFFu, ao, imm, a);
 #pragma unroll
         for (int p = 0; p < P; ++p) Lane<V>::store_output(kp, unit0 + p, (uint32_t)aux, a[p], valid[p]);
-        return;
+        return true;
       case D_MOV:
         ld((w0.x >> 8) & 0xFFu, ao, imm, a);
         put(w0.x >> 24, dof, save, a);
-        return;
+        return true;
       case D_CHAIN:
-        chain((w0.x >> 8) & 0xFFu, ao, imm, bo, (uint32_t)aux, r);
+        if (!chain(st, (w0.x >> 8) & 0xFFu, ao, imm, (uint32_t)aux, r)) return false;
         put(w0.x >> 24, dof, save, r);
-        return;
+        return true;
       case D_CHAIN_LC:
-        chain_lc((w0.x >> 8) & 0xFFu, ao, imm, bo, (uint32_t)aux, r);
+        if (!chain_lc(st, (w0.x >> 8) & 0xFFu, ao, imm, (uint32_t)aux, r)) return false;
         put(w0.x >> 24, dof, save, r);
-        return;
+        return true;
 #define ECH_FB(NAME, FN)                                                     \
   case D_##NAME##_RR:                                                        \
     C::ld(sm + ao, a);                                                       \
     C::ld(sm + bo, b);                                                       \
     _Pragma("unroll") for (int p = 0; p < P; ++p) r[p] = Kd::FN(a[p], b[p]); \
     put_sm(dof, save, r);                                                    \
-    return;                                                                  \
+    return true;                                                                  \
   case D_##NAME##_IR: {                                                      \
     const V c = dm::VT<V>::cst(imm);                                         \
     C::ld(sm + bo, b);                                                       \
     _Pragma("unroll") for (int p = 0; p < P; ++p) r[p] = Kd::FN(c, b[p]);    \
     put_sm(dof, save, r);                                                    \
-    return;                                                                  \
+    return true;                                                                  \
   }                                                                          \
   case D_##NAME##_RI: {                                                      \
     const V c = dm::VT<V>::cst(imm);                                         \
     C::ld(sm + ao, a);                                                       \
     _Pragma("unroll") for (int p = 0; p < P; ++p) r[p] = Kd::FN(a[p], c);    \
     put_sm(dof, save, r);                                                    \
-    return;                                                                  \
+    return true;                                                                  \
   }
       ECH_FB(ADD, add)
       ECH_FB(SUB, sub)
@@ -500,7 +554,7 @@ template <class V, int P> struct FwdExec {
     C::ld(sm + ao, a);                                                                           \
     _Pragma("unroll") for (int p = 0; p < P; ++p) r[p] = dm::eval_forward<V>(OP, a[p], a[p], aux); \
     put_sm(dof, save, r);                                                                        \
-    return;
+    return true;
       ECH_FU(OP_NEG) ECH_FU(OP_RECIP) ECH_FU(OP_SQRT) ECH_FU(OP_CBRT) ECH_FU(OP_POWI) ECH_FU(OP_EXP)
       ECH_FU(OP_EXP2) ECH_FU(OP_EXPM1) ECH_FU(OP_LN) ECH_FU(OP_LOG2) ECH_FU(OP_LOG10) ECH_FU(OP_LN1P)
       ECH_FU(OP_SIN) ECH_FU(OP_COS) ECH_FU(OP_TAN) ECH_FU(OP_ASIN) ECH_FU(OP_ACOS) ECH_FU(OP_ATAN)
@@ -523,6 +577,7 @@ template <class V, int P> struct FwdExec {
 #pragma unroll
     for (int p = 0; p < P; ++p) r[p] = dm::eval_forward<V>(opc, a[p], b[p], aux);
     put(w0.x >> 24, dof, save, r);
+    return true;
   }
 };
 
@@ -580,12 +635,12 @@ template <class V, int P> struct RevExec {
 
   // Reverse of a fused chain: for t = n..1 the Add/Sub (its two operands in
   // operand order), then the absorbed Mul, exactly as the per-op sweep visits
-  // them.  Adjoints of the chain's intermediates stay in registers.
-  // DRTerm layout: kind|op|flags, ax, ay, vx | vy, pad, c.
-  __device__ __forceinline__ void chain(uint32_t flags, uint32_t ro, uint32_t ao, uint32_t first, uint32_t n) const {
+  // them.  Adjoints of the chain's intermediates stay in registers.  The n
+  // DRTerm records follow in the stream, last term first
+  // (kind|op|flags, ax, ay, vx | vy, pad, c | pad).
+  __device__ __forceinline__ bool chain(Stream<48>& st, uint32_t flags, uint32_t ro, uint32_t ao, uint32_t n) const {
     V adj[P];
     C::ld(loc(flags & RF_R_GLOB, ro), adj);
-    const uint4* tp = reinterpret_cast<const uint4*>(kp.rterms + first);
     V one[P], mone[P];
     {
       V d0, d1;
@@ -595,8 +650,10 @@ template <class V, int P> struct RevExec {
     }
 #pragma unroll 1
     for (uint32_t q = n; q-- > 0;) {
-      const uint4 w0 = __ldg(tp + 2 * q);
-      const uint4 w1 = __ldg(tp + 2 * q + 1);
+      const unsigned char* rec = st.next();
+      if (rec == nullptr) return false;
+      const uint4 w0 = *reinterpret_cast<const uint4*>(rec);
+      const uint4 w1 = *reinterpret_cast<const uint4*>(rec + 16);
       const uint32_t kind = w0.x & 0xFFu, op = (w0.x >> 8) & 0xFFu, tf = w0.x >> 16;
       const bool chain_a = (op & 1u) == 0;
       // partials of the Add / Sub: acc side and term side
@@ -633,89 +690,87 @@ template <class V, int P> struct RevExec {
         for (int p = 0; p < P; ++p) adj[p] = nadj[p];
       }
     }
+    return true;
+  }
+
+  // One term t of a linear-combination chain in reverse, after its Add: the
+  // term's adjoint (the running adjoint, through the Add's multiplier 1) and
+  // its Mul's contribution c * adj(term) to adj(x).
+  __device__ __forceinline__ void lc_term(V (&adj)[P], const V (&one)[P], unsigned char* px, bool init,
+                                          const V& cv) const {
+    V t[P], c[P];
+    internal(adj, one, t);
+#pragma unroll
+    for (int p = 0; p < P; ++p) c[p] = cv;
+    accumulate<false>(px, init, t, c);
+#pragma unroll
+    for (int p = 0; p < P; ++p) adj[p] = t[p];
   }
 
   // Reverse of a linear-combination chain (every term Mul(c, x) or Mul(x, c),
   // op acc + term): for t = n..1 the Add (acc side, then the term side), then
   // the Mul's contribution c * adj(term) to adj(x).  Both Add sides see the
   // multiplier 1, so the running adjoint and the term's adjoint are the same
-  // value.
-  __device__ __forceinline__ void chain_lc(uint32_t flags, uint32_t ro, uint32_t ao, uint32_t first,
+  // value.  DRPair records carry terms (n-1-2k, n-2-2k)
+  // (c0, c1 | ax0, ax1, flags0|flags1, pad | pad).
+  __device__ __forceinline__ bool chain_lc(Stream<48>& st, uint32_t flags, uint32_t ro, uint32_t ao,
                                            uint32_t n) const {
     V adj[P], one[P];
 #pragma unroll
     for (int p = 0; p < P; ++p) one[p] = Kd::c(1);
     C::ld(loc(flags & RF_R_GLOB, ro), adj);
-    const uint4* tp = reinterpret_cast<const uint4*>(kp.rterms + first);
-    uint32_t q = n;
 #pragma unroll 1
-    while (q >= 3) {
-      // terms q-1 and q-2 (neither is the first term): when their adjoint
-      // targets differ the two read-modify-writes are independent, so both
-      // loads are issued before either store
-      const uint4 a0 = __ldg(tp + 2 * (q - 1));
-      const uint4 a1 = __ldg(tp + 2 * (q - 1) + 1);
-      const uint4 b0 = __ldg(tp + 2 * (q - 2));
-      const uint4 b1 = __ldg(tp + 2 * (q - 2) + 1);
-      const uint32_t fa = a0.x >> 16, fb = b0.x >> 16;
-      unsigned char* pa = loc(fa & CF_X_GLOB, a0.y);
-      unsigned char* pb = loc(fb & CF_X_GLOB, b0.y);
-      V ta[P], tb[P];
-      internal(adj, one, ta);
-      if (pa == pb) {
-        const V ca = dm::VT<V>::cst(__hiloint2double((int)a1.w, (int)a1.z));
-        V c[P];
+    for (uint32_t q = n; q > 0; q = q >= 2 ? q - 2 : 0) {
+      // this record: terms q-1 and (when q >= 2) q-2
+      const unsigned char* rec = st.next();
+      if (rec == nullptr) return false;
+      const uint4 cw = *reinterpret_cast<const uint4*>(rec);
+      const uint4 aw = *reinterpret_cast<const uint4*>(rec + 16);
+      const uint32_t fa = aw.z & 0xFFFFu, fb = aw.z >> 16;
+      unsigned char* pa = loc(fa & CF_X_GLOB, aw.x);
+      unsigned char* pb = loc(fb & CF_X_GLOB, aw.y);
+      const V ca = dm::VT<V>::cst(__hiloint2double((int)cw.y, (int)cw.x));
+      const V cb = dm::VT<V>::cst(__hiloint2double((int)cw.w, (int)cw.z));
+      if (q >= 3 && pa != pb) {
+        // neither term is the first and their adjoint targets differ: the two
+        // read-modify-writes are independent, so both loads issue first
+        V ta[P], tb[P], cura[P], curb[P];
+        internal(adj, one, ta);
+        internal(ta, one, tb);
+        if (fa & CF_X_INIT) {
 #pragma unroll
-        for (int p = 0; p < P; ++p) c[p] = ca;
-        accumulate<false>(pa, (fa & CF_X_INIT) != 0, ta, c);
+          for (int p = 0; p < P; ++p) cura[p] = Kd::c(0);
+        } else {
+          C::ld(pa, cura);
+        }
+        if (fb & CF_X_INIT) {
 #pragma unroll
-        for (int p = 0; p < P; ++p) adj[p] = ta[p];
-        q -= 1;
+          for (int p = 0; p < P; ++p) curb[p] = Kd::c(0);
+        } else {
+          C::ld(pb, curb);
+        }
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          if (!Kd::all_zero(ta[p]) && !Kd::all_zero(ca)) cura[p] = Kd::add(cura[p], Kd::mul(ca, ta[p]));
+          if (!Kd::all_zero(tb[p]) && !Kd::all_zero(cb)) curb[p] = Kd::add(curb[p], Kd::mul(cb, tb[p]));
+        }
+        C::st(pa, cura);
+        C::st(pb, curb);
+#pragma unroll
+        for (int p = 0; p < P; ++p) adj[p] = tb[p];
         continue;
       }
-      internal(ta, one, tb);
-      V cura[P], curb[P];
-      if (fa & CF_X_INIT) {
-#pragma unroll
-        for (int p = 0; p < P; ++p) cura[p] = Kd::c(0);
-      } else {
-        C::ld(pa, cura);
-      }
-      if (fb & CF_X_INIT) {
-#pragma unroll
-        for (int p = 0; p < P; ++p) curb[p] = Kd::c(0);
-      } else {
-        C::ld(pb, curb);
-      }
-      const V ca = dm::VT<V>::cst(__hiloint2double((int)a1.w, (int)a1.z));
-      const V cb = dm::VT<V>::cst(__hiloint2double((int)b1.w, (int)b1.z));
-#pragma unroll
-      for (int p = 0; p < P; ++p) {
-        if (!Kd::all_zero(ta[p]) && !Kd::all_zero(ca)) cura[p] = Kd::add(cura[p], Kd::mul(ca, ta[p]));
-        if (!Kd::all_zero(tb[p]) && !Kd::all_zero(cb)) curb[p] = Kd::add(curb[p], Kd::mul(cb, tb[p]));
-      }
-      C::st(pa, cura);
-      C::st(pb, curb);
-#pragma unroll
-      for (int p = 0; p < P; ++p) adj[p] = tb[p];
-      q -= 2;
-    }
-#pragma unroll 1
-    while (q-- > 0) {
-      const uint4 w0 = __ldg(tp + 2 * q);
-      const uint4 w1 = __ldg(tp + 2 * q + 1);
-      const uint32_t tf = w0.x >> 16;
-      if (q == 0 && (flags & RF_HAS_A))
+      // one term at a time; the first term's Add also pays adj(acc0)
+      if (q == 1 && (flags & RF_HAS_A))
         accumulate<false>(loc(flags & RF_A_GLOB, ao), (flags & RF_A_INIT) != 0, adj, one);
-      V t[P], c[P];
-      internal(adj, one, t);
-      const V cv = dm::VT<V>::cst(__hiloint2double((int)w1.w, (int)w1.z));
-#pragma unroll
-      for (int p = 0; p < P; ++p) c[p] = cv;
-      accumulate<false>(loc(tf & CF_X_GLOB, w0.y), (tf & CF_X_INIT) != 0, t, c);
-#pragma unroll
-      for (int p = 0; p < P; ++p) adj[p] = t[p];
+      lc_term(adj, one, pa, (fa & CF_X_INIT) != 0, ca);
+      if (q >= 2) {
+        if (q == 2 && (flags & RF_HAS_A))
+          accumulate<false>(loc(flags & RF_A_GLOB, ao), (flags & RF_A_INIT) != 0, adj, one);
+        lc_term(adj, one, pb, (fb & CF_X_INIT) != 0, cb);
+      }
     }
+    return true;
   }
 
   // One reverse op: adj(a) += da * adj(r), adj(b) += db * adj(r) with the
@@ -737,7 +792,7 @@ template <class V, int P> struct RevExec {
       accumulate<FAST>(FAST ? sm + bo : loc(flags & RF_B_GLOB, bo), (flags & RF_B_INIT) != 0, adj, db);
   }
 
-  __device__ __forceinline__ void operator()(const unsigned char* raw) const {
+  __device__ __forceinline__ bool operator()(const unsigned char* raw, Stream<48>& st) const {
     const uint4 w0 = *reinterpret_cast<const uint4*>(raw);
     const uint4 w1 = *reinterpret_cast<const uint4*>(raw + 16);
     const uint2 w2 = *reinterpret_cast<const uint2*>(raw + 32);
@@ -752,14 +807,12 @@ template <class V, int P> struct RevExec {
 #pragma unroll
         for (int p = 0; p < P; ++p) one[p] = Kd::c(1);
         C::st(loc(flags & RF_R_GLOB, ro), one);
-        return;
+        return true;
       }
       case D_CHAIN:
-        chain(flags, ro, ao, w1.x, (uint32_t)aux);
-        return;
+        return chain(st, flags, ro, ao, (uint32_t)aux);
       case D_CHAIN_LC:
-        chain_lc(flags, ro, ao, w1.x, (uint32_t)aux);
-        return;
+        return chain_lc(st, flags, ro, ao, (uint32_t)aux);
       case D_STGRAD: {
         V g[P];
         if (ro == kNone) {
@@ -770,10 +823,10 @@ template <class V, int P> struct RevExec {
         }
 #pragma unroll
         for (int p = 0; p < P; ++p) GradOut<V>::store(kp, unit0 + p, (uint32_t)aux, g[p], valid[p]);
-        return;
+        return true;
       }
 #define ECH_RF(OP) \
-  case D_RF_BASE + OP: body<true>(OP, flags, ro, ao, bo, w1.x, w1.y, w1.z, aux, imm); return;
+  case D_RF_BASE + OP: body<true>(OP, flags, ro, ao, bo, w1.x, w1.y, w1.z, aux, imm); return true;
       ECH_RF(OP_ADD) ECH_RF(OP_SUB) ECH_RF(OP_MUL) ECH_RF(OP_DIV) ECH_RF(OP_REM) ECH_RF(OP_POWF)
       ECH_RF(OP_ATAN2) ECH_RF(OP_HYPOT) ECH_RF(OP_MAX) ECH_RF(OP_MIN) ECH_RF(OP_NEG) ECH_RF(OP_RECIP)
       ECH_RF(OP_SQRT) ECH_RF(OP_CBRT) ECH_RF(OP_POWI) ECH_RF(OP_EXP) ECH_RF(OP_EXP2) ECH_RF(OP_EXPM1)
@@ -784,7 +837,7 @@ template <class V, int P> struct RevExec {
 #undef ECH_RF
       default:
         body<false>(opc, flags, ro, ao, bo, w1.x, w1.y, w1.z, aux, imm);
-        return;
+        return true;
     }
   }
 };

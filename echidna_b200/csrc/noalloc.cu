@@ -75,9 +75,7 @@ extern "C" ECH_API ech_status ech_gradient_batch_device_noalloc(ech_ctx* ctx, co
   const Plan& p = *hs.plan;
   const size_t b_fwd = round256(std::max<size_t>(pg.fwd.size(), 1) * sizeof(DIns));
   const size_t b_rev = round256(std::max<size_t>(pg.rev.size(), 1) * sizeof(DRIns));
-  const size_t b_ft = round256(pg.fterms.size() * sizeof(DFTerm));
-  const size_t b_rt = round256(pg.rterms.size() * sizeof(DRTerm));
-  const size_t b_prog = b_fwd + b_rev + b_ft + b_rt;
+  const size_t b_prog = b_fwd + b_rev;
   const uint64_t slots = (uint64_t)p.far_slots + p.traj_slots;
   const uint64_t stride = round256(slots * hs.tile * hs.vbytes);
   if (b_prog + std::max<uint64_t>(stride, 256) > kNoAllocBytes) {
@@ -91,9 +89,7 @@ extern "C" ECH_API ech_status ech_gradient_batch_device_noalloc(ech_ctx* ctx, co
   cudaStream_t st = stream ? (cudaStream_t)stream : hs.stream;
   unsigned char* d_fwd = region;
   unsigned char* d_rev = d_fwd + b_fwd;
-  unsigned char* d_ft = d_rev + b_rev;
-  unsigned char* d_rt = d_ft + b_ft;
-  unsigned char* d_scratch = d_rt + b_rt;
+  unsigned char* d_scratch = d_rev + b_rev;
   const size_t scratch_bytes = kNoAllocBytes - b_prog;
 
   KParams kp{};
@@ -101,8 +97,6 @@ extern "C" ECH_API ech_status ech_gradient_batch_device_noalloc(ech_ctx* ctx, co
   kp.n_fwd = (uint32_t)pg.fwd.size();
   kp.rev = reinterpret_cast<const DRIns*>(d_rev);
   kp.n_rev = (uint32_t)pg.rev.size();
-  kp.fterms = reinterpret_cast<const DFTerm*>(d_ft);
-  kp.rterms = reinterpret_cast<const DRTerm*>(d_rt);
   kp.far_slots = p.far_slots;
   kp.smem_regs = std::max<uint32_t>(p.smem_regs, 1);
   kp.tile = hs.tile;
@@ -128,10 +122,6 @@ extern "C" ECH_API ech_status ech_gradient_batch_device_noalloc(ech_ctx* ctx, co
   if (!pg.fwd.empty()) e = cudaMemcpyAsync(d_fwd, pg.fwd.data(), pg.fwd.size() * sizeof(DIns), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && !pg.rev.empty())
     e = cudaMemcpyAsync(d_rev, pg.rev.data(), pg.rev.size() * sizeof(DRIns), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(d_ft, pg.fterms.data(), pg.fterms.size() * sizeof(DFTerm), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(d_rt, pg.rterms.data(), pg.rterms.size() * sizeof(DRTerm), cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return set_error(ECH_ERR_OTHER, std::string("program copy: ") + cudaGetErrorString(e));
   e = launch_sweep(hs.req, kp, (int)grid, hs.threads, hs.smem, st, &bps);
   if (e != cudaSuccess) return set_error(ECH_ERR_OTHER, std::string("kernel launch: ") + cudaGetErrorString(e));

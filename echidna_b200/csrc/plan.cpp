@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
 #include <set>
 #include <sstream>
 #include <stdexcept>
@@ -832,6 +833,15 @@ static bool linear_combination(const Plan& p, uint32_t first, uint32_t n) {
   return true;
 }
 
+// A term record reinterpreted as an instruction-sized record of the stream.
+template <class R, class T>
+static R as_record(const T& t) {
+  static_assert(sizeof(R) == sizeof(T), "records of one stream have one size");
+  R r;
+  std::memcpy(&r, &t, sizeof r);
+  return r;
+}
+
 bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out, std::string& err) {
   const uint64_t row = (uint64_t)tile * vbytes;
   bool ok = true;
@@ -843,6 +853,32 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out,
       return 0;
     }
     return (uint32_t)o;
+  };
+  auto fterm = [&](const PTerm& pt) {
+    DFTerm f{};
+    f.kind = pt.kind;
+    f.op = pt.op;
+    f.xm = pt.fxm;
+    f.ym = pt.fym;
+    f.x = (pt.fxm == M_SMEM || pt.fxm == M_GLOB) ? off(pt.fxi) : kNone;
+    f.y = (pt.fym == M_SMEM || pt.fym == M_GLOB) ? off(pt.fyi) : kNone;
+    f.c = pt.c;
+    return f;
+  };
+  auto rterm = [&](const PTerm& pt) {
+    DRTerm r{};
+    r.kind = pt.kind;
+    r.op = pt.op;
+    uint16_t fl = pt.flags & (CF_X_INIT | CF_Y_INIT | CF_X_ADJ | CF_Y_ADJ);
+    if (pt.rxm == M_GLOB) fl |= CF_X_GLOB;
+    if (pt.rym == M_GLOB) fl |= CF_Y_GLOB;
+    r.flags = fl;
+    r.ax = (pt.flags & CF_X_ADJ) ? off(pt.rxi) : kNone;
+    r.ay = (pt.flags & CF_Y_ADJ) ? off(pt.ryi) : kNone;
+    r.vx = off(pt.vx);
+    r.vy = off(pt.vy);
+    r.c = pt.c;
+    return r;
   };
   out.fwd.clear();
   out.rev.clear();
@@ -861,10 +897,28 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out,
     uint8_t opc = in.opc;
     const bool dsm = in.md == M_SMEM;
     if (opc == XI_CHAIN) {
-      d.b = in.b;  // first term (index into the term tables)
+      // the terms follow the instruction in the stream
+      const uint32_t first = in.b, n = (uint32_t)in.aux;
+      const bool lc = linear_combination(p, first, n);
+      d.b = 0;
       d.mb = M_NONE;
-      d.opc = linear_combination(p, in.b, (uint32_t)in.aux) ? D_CHAIN_LC : D_CHAIN;
+      d.opc = lc ? D_CHAIN_LC : D_CHAIN;
       out.fwd.push_back(d);
+      if (lc) {
+        for (uint32_t k = 0; k < n; k += 2) {
+          DFPair pr{};
+          for (uint32_t j = 0; j < 2 && k + j < n; ++j) {
+            const PTerm& pt = p.terms[first + k + j];
+            pr.c[j] = pt.c;
+            pr.x[j] = off(pt.fxi);
+            pr.m[j] = pt.fxm;
+            pr.cx[j] = pt.kind == CK_CX ? 1 : 0;
+          }
+          out.fwd.push_back(as_record<DIns>(pr));
+        }
+      } else {
+        for (uint32_t q = first; q < first + n; ++q) out.fwd.push_back(as_record<DIns>(fterm(p.terms[q])));
+      }
       continue;
     }
     if (dsm && (opc == OP_ADD || opc == OP_SUB || opc == OP_MUL || opc == OP_DIV)) {
@@ -884,14 +938,32 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out,
     d.flags = in.flags;
     d.aux = in.aux;
     if (in.opc == XI_CHAIN) {
-      d.opc = linear_combination(p, in.va, (uint32_t)in.aux) ? D_CHAIN_LC : D_CHAIN;
+      // the terms follow the instruction, last term first
+      const uint32_t first = in.va, n = (uint32_t)in.aux;
+      const bool lc = linear_combination(p, first, n);
+      d.opc = lc ? D_CHAIN_LC : D_CHAIN;
       d.r = off(in.r);
       d.a = off(in.a);
       d.b = kNone;
-      d.va = in.va;  // first term
+      d.va = kNone;
       d.vb = kNone;
       d.vr = kNone;
       out.rev.push_back(d);
+      if (lc) {
+        for (uint32_t k = 0; k < n; k += 2) {
+          DRPair pr{};
+          for (uint32_t j = 0; j < 2 && k + j < n; ++j) {
+            const PTerm& pt = p.terms[first + n - 1 - k - j];
+            const DRTerm r = rterm(pt);
+            pr.c[j] = pt.c;
+            pr.ax[j] = r.ax;
+            pr.flags[j] = r.flags;
+          }
+          out.rev.push_back(as_record<DRIns>(pr));
+        }
+      } else {
+        for (uint32_t k = 0; k < n; ++k) out.rev.push_back(as_record<DRIns>(rterm(p.terms[first + n - 1 - k])));
+      }
       continue;
     }
     d.r = off(in.r);
@@ -920,36 +992,6 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out,
       opc = (uint8_t)(D_RF_BASE + opc);
     d.opc = opc;
     out.rev.push_back(d);
-  }
-  out.fterms.clear();
-  out.rterms.clear();
-  for (const PTerm& pt : p.terms) {
-    DFTerm f{};
-    f.kind = pt.kind;
-    f.op = pt.op;
-    f.xm = pt.fxm;
-    f.ym = pt.fym;
-    f.x = (pt.fxm == M_SMEM || pt.fxm == M_GLOB) ? off(pt.fxi) : kNone;
-    f.y = (pt.fym == M_SMEM || pt.fym == M_GLOB) ? off(pt.fyi) : kNone;
-    f.c = pt.c;
-    out.fterms.push_back(f);
-    DRTerm r{};
-    r.kind = pt.kind;
-    r.op = pt.op;
-    uint16_t fl = pt.flags & (CF_X_INIT | CF_Y_INIT | CF_X_ADJ | CF_Y_ADJ);
-    if (pt.rxm == M_GLOB) fl |= CF_X_GLOB;
-    if (pt.rym == M_GLOB) fl |= CF_Y_GLOB;
-    r.flags = fl;
-    r.ax = (pt.flags & CF_X_ADJ) ? off(pt.rxi) : kNone;
-    r.ay = (pt.flags & CF_Y_ADJ) ? off(pt.ryi) : kNone;
-    r.vx = off(pt.vx);
-    r.vy = off(pt.vy);
-    r.c = pt.c;
-    out.rterms.push_back(r);
-  }
-  if (out.fterms.empty()) {
-    out.fterms.push_back(DFTerm{});
-    out.rterms.push_back(DRTerm{});
   }
   if (!ok) err = "slot region exceeds the 32-bit offset encoding; use a smaller tile";
   return ok;

@@ -65,11 +65,11 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap);
 // Device encoding of a plan for a launch geometry (`tile` points per CTA,
 // `vbytes` bytes per slot value).  Returns false (with `err`) if an offset does
 // not fit the 32-bit encoding.
+// Chain terms are records of the streams (after their chain instruction), so
+// the record counts exceed the plan's instruction counts.
 struct DevProgram {
   std::vector<DIns> fwd;
   std::vector<DRIns> rev;
-  std::vector<DFTerm> fterms;
-  std::vector<DRTerm> rterms;
 };
 bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out, std::string& err);
 
