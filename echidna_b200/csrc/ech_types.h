@@ -74,6 +74,7 @@ enum RFlag : uint16_t {
   RF_VB_IMM = 1 << 6,
   RF_HAS_A = 1 << 7,    // contribute to adj(a)
   RF_HAS_B = 1 << 8,
+  RF_LC_DISTINCT = 1 << 9,  // D_CHAIN_LC: the terms' adjoint targets are pairwise distinct
 };
 struct alignas(16) RIns {
   uint8_t opc;

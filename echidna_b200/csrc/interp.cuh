@@ -458,13 +458,45 @@ template <class V, int P> struct FwdExec {
 
   // Linear-combination chain: every term is Mul(c, x) or Mul(x, c) added to the
   // running value, in tape order.  DFPair records carry two terms each
-  // (c0, c1 | x0, x1, m0|m1|cx0|cx1, pad), so both operand loads are issued
-  // before the arithmetic.
+  // (c0, c1 | x0, x1, m0|m1|cx0|cx1, pad).  kLcGroup records at a time: all
+  // their operand loads are issued before the arithmetic, so a warp keeps
+  // several L2 round trips (global slots) in flight; the additions stay in
+  // term order.
+  static constexpr int kWords = (int)(sizeof(V) * P / 4);
+  static constexpr int kLcGroup = kWords <= 4 ? 4 : (kWords <= 8 ? 2 : 1);
   __device__ __forceinline__ bool chain_lc(Stream<32>& st, uint32_t ma, uint32_t ao, double imm, uint32_t n,
                                            V (&acc)[P]) const {
     ld(ma, ao, imm, acc);
+    uint32_t q = 0;
+    if constexpr (kLcGroup > 1) {
 #pragma unroll 1
-    for (uint32_t q = 0; q < n; q += 2) {
+      for (; q + 2 * kLcGroup <= n; q += 2 * kLcGroup) {
+        V xs[2 * kLcGroup][P];
+        V cs[2 * kLcGroup];
+        bool cx[2 * kLcGroup];
+#pragma unroll
+        for (int k = 0; k < kLcGroup; ++k) {
+          const unsigned char* rec = st.next();
+          if (rec == nullptr) return false;
+          const uint4 cw = *reinterpret_cast<const uint4*>(rec);
+          const uint4 xw = *reinterpret_cast<const uint4*>(rec + 16);
+          ldv(xw.z & 0xFFu, xw.x, xs[2 * k]);
+          ldv((xw.z >> 8) & 0xFFu, xw.y, xs[2 * k + 1]);
+          cs[2 * k] = dm::VT<V>::cst(__hiloint2double((int)cw.y, (int)cw.x));
+          cs[2 * k + 1] = dm::VT<V>::cst(__hiloint2double((int)cw.w, (int)cw.z));
+          cx[2 * k] = ((xw.z >> 16) & 0xFFu) != 0;
+          cx[2 * k + 1] = (xw.z >> 24) != 0;
+        }
+#pragma unroll
+        for (int j = 0; j < 2 * kLcGroup; ++j) {
+#pragma unroll
+          for (int p = 0; p < P; ++p)
+            acc[p] = Kd::add(acc[p], cx[j] ? Kd::mul(cs[j], xs[j][p]) : Kd::mul(xs[j][p], cs[j]));
+        }
+      }
+    }
+#pragma unroll 1
+    for (; q < n; q += 2) {
       const unsigned char* rec = st.next();
       if (rec == nullptr) return false;
       const uint4 cw = *reinterpret_cast<const uint4*>(rec);
@@ -713,14 +745,67 @@ template <class V, int P> struct RevExec {
   // multiplier 1, so the running adjoint and the term's adjoint are the same
   // value.  DRPair records carry terms (n-1-2k, n-2-2k)
   // (c0, c1 | ax0, ax1, flags0|flags1, pad | pad).
+  static constexpr int kWords = (int)(sizeof(V) * P / 4);
+  static constexpr int kLcGroup = kWords <= 4 ? 2 : 1;  // records per batch of independent updates
   __device__ __forceinline__ bool chain_lc(Stream<48>& st, uint32_t flags, uint32_t ro, uint32_t ao,
                                            uint32_t n) const {
     V adj[P], one[P];
 #pragma unroll
     for (int p = 0; p < P; ++p) one[p] = Kd::c(1);
     C::ld(loc(flags & RF_R_GLOB, ro), adj);
+    uint32_t q = n;
+    if constexpr (kLcGroup > 1) {
+      // The chain's adjoint targets are pairwise distinct (RF_LC_DISTINCT): the
+      // updates of 2*kLcGroup terms that are not the first are independent, so
+      // all their loads issue before the first store; the running adjoint is
+      // still passed through each term's Add in order.
+      if (flags & RF_LC_DISTINCT) {
 #pragma unroll 1
-    for (uint32_t q = n; q > 0; q = q >= 2 ? q - 2 : 0) {
+        while (q >= 2 * kLcGroup + 1) {
+          unsigned char* pt[2 * kLcGroup];
+          V cs[2 * kLcGroup];
+          V cur[2 * kLcGroup][P];
+#pragma unroll
+          for (int k = 0; k < kLcGroup; ++k) {
+            const unsigned char* rec = st.next();
+            if (rec == nullptr) return false;
+            const uint4 cw = *reinterpret_cast<const uint4*>(rec);
+            const uint4 aw = *reinterpret_cast<const uint4*>(rec + 16);
+            const uint32_t f0 = aw.z & 0xFFFFu, f1 = aw.z >> 16;
+            pt[2 * k] = loc(f0 & CF_X_GLOB, aw.x);
+            pt[2 * k + 1] = loc(f1 & CF_X_GLOB, aw.y);
+            cs[2 * k] = dm::VT<V>::cst(__hiloint2double((int)cw.y, (int)cw.x));
+            cs[2 * k + 1] = dm::VT<V>::cst(__hiloint2double((int)cw.w, (int)cw.z));
+            if (f0 & CF_X_INIT) {
+#pragma unroll
+              for (int p = 0; p < P; ++p) cur[2 * k][p] = Kd::c(0);
+            } else {
+              C::ld(pt[2 * k], cur[2 * k]);
+            }
+            if (f1 & CF_X_INIT) {
+#pragma unroll
+              for (int p = 0; p < P; ++p) cur[2 * k + 1][p] = Kd::c(0);
+            } else {
+              C::ld(pt[2 * k + 1], cur[2 * k + 1]);
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < 2 * kLcGroup; ++j) {
+            V t[P];
+            internal(adj, one, t);
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+              if (!Kd::all_zero(t[p]) && !Kd::all_zero(cs[j])) cur[j][p] = Kd::add(cur[j][p], Kd::mul(cs[j], t[p]));
+              adj[p] = t[p];
+            }
+            C::st(pt[j], cur[j]);
+          }
+          q -= 2 * kLcGroup;
+        }
+      }
+    }
+#pragma unroll 1
+    for (; q > 0; q = q >= 2 ? q - 2 : 0) {
       // this record: terms q-1 and (when q >= 2) q-2
       const unsigned char* rec = st.next();
       if (rec == nullptr) return false;

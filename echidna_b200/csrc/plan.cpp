@@ -942,6 +942,12 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out,
       const uint32_t first = in.va, n = (uint32_t)in.aux;
       const bool lc = linear_combination(p, first, n);
       d.opc = lc ? D_CHAIN_LC : D_CHAIN;
+      if (lc) {
+        // pairwise distinct adjoint targets let the kernel batch the terms' updates
+        std::set<std::pair<uint8_t, uint32_t>> targets;
+        for (uint32_t q = first; q < first + n; ++q) targets.insert({p.terms[q].rxm, p.terms[q].rxi});
+        if (targets.size() == n) d.flags |= RF_LC_DISTINCT;
+      }
       d.r = off(in.r);
       d.a = off(in.a);
       d.b = kNone;
