@@ -316,7 +316,7 @@ static ech_status get_plan(ech_tape* t, int kind, int K, uint32_t cap, uint32_t 
   dp->host = build_plan(t->host, kind_of(kind), cap);
   DevProgram prog;
   std::string err;
-  if (!encode_plan(dp->host, tile, vbytes, prog, err)) return fail(ECH_ERR_OTHER, err);
+  if (!encode_plan(dp->host, tile, vbytes, !t->f64, prog, err)) return fail(ECH_ERR_OTHER, err);
   CU(cudaMalloc(&dp->d_fwd, std::max<size_t>(prog.fwd.size(), 1) * sizeof(DIns)));
   if (!prog.fwd.empty())
     CU(cudaMemcpy(dp->d_fwd, prog.fwd.data(), prog.fwd.size() * sizeof(DIns), cudaMemcpyHostToDevice));
@@ -1877,7 +1877,7 @@ ech_status prepare_gradient_host(ech_ctx* ctx, const ech_tape* tc, int f64, uint
       std::unique_ptr<ech_tape::HostProgram> np(new ech_tape::HostProgram());
       np->plan = build_plan(t->host, Kind::Gradient, c.cap);
       std::string err;
-      if (!encode_plan(np->plan, c.tile, (uint32_t)c.vbytes, np->prog, err)) return fail(ECH_ERR_OTHER, err);
+      if (!encode_plan(np->plan, c.tile, (uint32_t)c.vbytes, !t->f64, np->prog, err)) return fail(ECH_ERR_OTHER, err);
       it = t->host_programs.emplace(key, std::move(np)).first;
     }
     hp = it->second.get();

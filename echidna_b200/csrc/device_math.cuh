@@ -141,20 +141,30 @@ template <> struct VT<double> {
   using S = double;
   static __device__ __forceinline__ double prim(double x) { return x; }
   static __device__ __forceinline__ double cst(double v) { return v; }
+  static __device__ __forceinline__ double cst_s(double v) { return v; }
 };
 template <> struct VT<float> {
   using S = float;
   static __device__ __forceinline__ float prim(float x) { return x; }
   static __device__ __forceinline__ float cst(double v) { return (float)v; }
+  static __device__ __forceinline__ float cst_s(float v) { return v; }
 };
 template <class T> struct VT<Dual<T>> {
   using S = T;
   static __device__ __forceinline__ T prim(const Dual<T>& x) { return x.re; }
   static __device__ __forceinline__ Dual<T> cst(double v) { return {(T)v, T(0)}; }
+  static __device__ __forceinline__ Dual<T> cst_s(T v) { return {v, T(0)}; }
 };
 template <class T, int K> struct VT<Jet<T, K>> {
   using S = T;
   static __device__ __forceinline__ T prim(const Jet<T, K>& x) { return x.c[0]; }
+  static __device__ __forceinline__ Jet<T, K> cst_s(T v) {
+    Jet<T, K> j;
+    j.c[0] = v;
+#pragma unroll
+    for (int k = 1; k < K; ++k) j.c[k] = T(0);
+    return j;
+  }
   static __device__ __forceinline__ Jet<T, K> cst(double v) {
     Jet<T, K> j;
     j.c[0] = (T)v;

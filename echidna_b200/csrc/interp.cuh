@@ -285,6 +285,15 @@ template <class V, int P> struct Col {
   }
 };
 
+// Constant of a linear-combination term record: programs for f32 values carry
+// it already rounded to f32 (the low word of the 8-byte field), f64 programs
+// the double.
+template <class V>
+__device__ __forceinline__ V lc_const(uint32_t lo, uint32_t hi) {
+  if constexpr (sizeof(typename dm::VT<V>::S) == 4) return dm::VT<V>::cst_s(__uint_as_float(lo));
+  else return dm::VT<V>::cst(__hiloint2double((int)hi, (int)lo));
+}
+
 // Per-kind input construction and output handling; the primary template is
 // the plain-value kind (forward, gradient).
 template <class T> struct Lane {
@@ -482,8 +491,8 @@ template <class V, int P> struct FwdExec {
           const uint4 xw = *reinterpret_cast<const uint4*>(rec + 16);
           ldv(xw.z & 0xFFu, xw.x, xs[2 * k]);
           ldv((xw.z >> 8) & 0xFFu, xw.y, xs[2 * k + 1]);
-          cs[2 * k] = dm::VT<V>::cst(__hiloint2double((int)cw.y, (int)cw.x));
-          cs[2 * k + 1] = dm::VT<V>::cst(__hiloint2double((int)cw.w, (int)cw.z));
+          cs[2 * k] = lc_const<V>(cw.x, cw.y);
+          cs[2 * k + 1] = lc_const<V>(cw.z, cw.w);
           cx[2 * k] = ((xw.z >> 16) & 0xFFu) != 0;
           cx[2 * k + 1] = (xw.z >> 24) != 0;
         }
@@ -501,14 +510,14 @@ template <class V, int P> struct FwdExec {
       if (rec == nullptr) return false;
       const uint4 cw = *reinterpret_cast<const uint4*>(rec);
       const uint4 xw = *reinterpret_cast<const uint4*>(rec + 16);
-      const V ca = dm::VT<V>::cst(__hiloint2double((int)cw.y, (int)cw.x));
+      const V ca = lc_const<V>(cw.x, cw.y);
       const bool a_cx = ((xw.z >> 16) & 0xFFu) != 0;
       V xa[P];
       ldv(xw.z & 0xFFu, xw.x, xa);
       if (q + 1 < n) {
         V xb[P];
         ldv((xw.z >> 8) & 0xFFu, xw.y, xb);
-        const V cb = dm::VT<V>::cst(__hiloint2double((int)cw.w, (int)cw.z));
+        const V cb = lc_const<V>(cw.z, cw.w);
         const bool b_cx = (xw.z >> 24) != 0;
 #pragma unroll
         for (int p = 0; p < P; ++p) {
@@ -725,40 +734,42 @@ template <class V, int P> struct RevExec {
     return true;
   }
 
-  // One term t of a linear-combination chain in reverse, after its Add: the
-  // term's adjoint (the running adjoint, through the Add's multiplier 1) and
-  // its Mul's contribution c * adj(term) to adj(x).
-  __device__ __forceinline__ void lc_term(V (&adj)[P], const V (&one)[P], unsigned char* px, bool init,
-                                          const V& cv) const {
-    V t[P], c[P];
-    internal(adj, one, t);
-#pragma unroll
-    for (int p = 0; p < P; ++p) c[p] = cv;
-    accumulate<false>(px, init, t, c);
-#pragma unroll
-    for (int p = 0; p < P; ++p) adj[p] = t[p];
-  }
-
   // Reverse of a linear-combination chain (every term Mul(c, x) or Mul(x, c),
   // op acc + term): for t = n..1 the Add (acc side, then the term side), then
   // the Mul's contribution c * adj(term) to adj(x).  Both Add sides see the
   // multiplier 1, so the running adjoint and the term's adjoint are the same
-  // value.  DRPair records carry terms (n-1-2k, n-2-2k)
-  // (c0, c1 | ax0, ax1, flags0|flags1, pad | pad).
+  // value, internal(running).  internal() is idempotent (a value it returns
+  // comes back unchanged, NaN stays NaN), so every term sees
+  // t = internal(adj(r)), and the first term's acc side sees adj(r) itself when
+  // the chain has one term, t otherwise.  DRPair records carry terms
+  // (n-1-2k, n-2-2k) (c0, c1 | ax0, ax1, flags0|flags1, pad | pad).
   static constexpr int kWords = (int)(sizeof(V) * P / 4);
   static constexpr int kLcGroup = kWords <= 4 ? 2 : 1;  // records per batch of independent updates
+  __device__ __forceinline__ void lc_update(V (&cur)[P], const V (&t)[P], const V& c) const {
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+      if (!Kd::all_zero(t[p]) && !Kd::all_zero(c)) cur[p] = Kd::add(cur[p], Kd::mul(c, t[p]));
+  }
+  __device__ __forceinline__ void lc_load(unsigned char* ptr, bool init, V (&cur)[P]) const {
+    if (init) {
+#pragma unroll
+      for (int p = 0; p < P; ++p) cur[p] = Kd::c(0);
+    } else {
+      C::ld(ptr, cur);
+    }
+  }
   __device__ __forceinline__ bool chain_lc(Stream<48>& st, uint32_t flags, uint32_t ro, uint32_t ao,
                                            uint32_t n) const {
-    V adj[P], one[P];
+    V adj[P], one[P], t[P];
 #pragma unroll
     for (int p = 0; p < P; ++p) one[p] = Kd::c(1);
     C::ld(loc(flags & RF_R_GLOB, ro), adj);
+    internal(adj, one, t);
     uint32_t q = n;
     if constexpr (kLcGroup > 1) {
       // The chain's adjoint targets are pairwise distinct (RF_LC_DISTINCT): the
       // updates of 2*kLcGroup terms that are not the first are independent, so
-      // all their loads issue before the first store; the running adjoint is
-      // still passed through each term's Add in order.
+      // all their loads issue before the first store.
       if (flags & RF_LC_DISTINCT) {
 #pragma unroll 1
         while (q >= 2 * kLcGroup + 1) {
@@ -774,30 +785,14 @@ template <class V, int P> struct RevExec {
             const uint32_t f0 = aw.z & 0xFFFFu, f1 = aw.z >> 16;
             pt[2 * k] = loc(f0 & CF_X_GLOB, aw.x);
             pt[2 * k + 1] = loc(f1 & CF_X_GLOB, aw.y);
-            cs[2 * k] = dm::VT<V>::cst(__hiloint2double((int)cw.y, (int)cw.x));
-            cs[2 * k + 1] = dm::VT<V>::cst(__hiloint2double((int)cw.w, (int)cw.z));
-            if (f0 & CF_X_INIT) {
-#pragma unroll
-              for (int p = 0; p < P; ++p) cur[2 * k][p] = Kd::c(0);
-            } else {
-              C::ld(pt[2 * k], cur[2 * k]);
-            }
-            if (f1 & CF_X_INIT) {
-#pragma unroll
-              for (int p = 0; p < P; ++p) cur[2 * k + 1][p] = Kd::c(0);
-            } else {
-              C::ld(pt[2 * k + 1], cur[2 * k + 1]);
-            }
+            cs[2 * k] = lc_const<V>(cw.x, cw.y);
+            cs[2 * k + 1] = lc_const<V>(cw.z, cw.w);
+            lc_load(pt[2 * k], (f0 & CF_X_INIT) != 0, cur[2 * k]);
+            lc_load(pt[2 * k + 1], (f1 & CF_X_INIT) != 0, cur[2 * k + 1]);
           }
 #pragma unroll
           for (int j = 0; j < 2 * kLcGroup; ++j) {
-            V t[P];
-            internal(adj, one, t);
-#pragma unroll
-            for (int p = 0; p < P; ++p) {
-              if (!Kd::all_zero(t[p]) && !Kd::all_zero(cs[j])) cur[j][p] = Kd::add(cur[j][p], Kd::mul(cs[j], t[p]));
-              adj[p] = t[p];
-            }
+            lc_update(cur[j], t, cs[j]);
             C::st(pt[j], cur[j]);
           }
           q -= 2 * kLcGroup;
@@ -814,45 +809,32 @@ template <class V, int P> struct RevExec {
       const uint32_t fa = aw.z & 0xFFFFu, fb = aw.z >> 16;
       unsigned char* pa = loc(fa & CF_X_GLOB, aw.x);
       unsigned char* pb = loc(fb & CF_X_GLOB, aw.y);
-      const V ca = dm::VT<V>::cst(__hiloint2double((int)cw.y, (int)cw.x));
-      const V cb = dm::VT<V>::cst(__hiloint2double((int)cw.w, (int)cw.z));
+      const V ca = lc_const<V>(cw.x, cw.y);
+      const V cb = lc_const<V>(cw.z, cw.w);
+      V cura[P], curb[P];
       if (q >= 3 && pa != pb) {
         // neither term is the first and their adjoint targets differ: the two
         // read-modify-writes are independent, so both loads issue first
-        V ta[P], tb[P], cura[P], curb[P];
-        internal(adj, one, ta);
-        internal(ta, one, tb);
-        if (fa & CF_X_INIT) {
-#pragma unroll
-          for (int p = 0; p < P; ++p) cura[p] = Kd::c(0);
-        } else {
-          C::ld(pa, cura);
-        }
-        if (fb & CF_X_INIT) {
-#pragma unroll
-          for (int p = 0; p < P; ++p) curb[p] = Kd::c(0);
-        } else {
-          C::ld(pb, curb);
-        }
-#pragma unroll
-        for (int p = 0; p < P; ++p) {
-          if (!Kd::all_zero(ta[p]) && !Kd::all_zero(ca)) cura[p] = Kd::add(cura[p], Kd::mul(ca, ta[p]));
-          if (!Kd::all_zero(tb[p]) && !Kd::all_zero(cb)) curb[p] = Kd::add(curb[p], Kd::mul(cb, tb[p]));
-        }
+        lc_load(pa, (fa & CF_X_INIT) != 0, cura);
+        lc_load(pb, (fb & CF_X_INIT) != 0, curb);
+        lc_update(cura, t, ca);
+        lc_update(curb, t, cb);
         C::st(pa, cura);
         C::st(pb, curb);
-#pragma unroll
-        for (int p = 0; p < P; ++p) adj[p] = tb[p];
         continue;
       }
       // one term at a time; the first term's Add also pays adj(acc0)
       if (q == 1 && (flags & RF_HAS_A))
-        accumulate<false>(loc(flags & RF_A_GLOB, ao), (flags & RF_A_INIT) != 0, adj, one);
-      lc_term(adj, one, pa, (fa & CF_X_INIT) != 0, ca);
+        accumulate<false>(loc(flags & RF_A_GLOB, ao), (flags & RF_A_INIT) != 0, n == 1 ? adj : t, one);
+      lc_load(pa, (fa & CF_X_INIT) != 0, cura);
+      lc_update(cura, t, ca);
+      C::st(pa, cura);
       if (q >= 2) {
         if (q == 2 && (flags & RF_HAS_A))
-          accumulate<false>(loc(flags & RF_A_GLOB, ao), (flags & RF_A_INIT) != 0, adj, one);
-        lc_term(adj, one, pb, (fb & CF_X_INIT) != 0, cb);
+          accumulate<false>(loc(flags & RF_A_GLOB, ao), (flags & RF_A_INIT) != 0, t, one);
+        lc_load(pb, (fb & CF_X_INIT) != 0, curb);
+        lc_update(curb, t, cb);
+        C::st(pb, curb);
       }
     }
     return true;

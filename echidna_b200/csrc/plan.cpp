@@ -842,7 +842,7 @@ static R as_record(const T& t) {
   return r;
 }
 
-bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out, std::string& err) {
+bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, bool f32, DevProgram& out, std::string& err) {
   const uint64_t row = (uint64_t)tile * vbytes;
   bool ok = true;
   auto off = [&](uint32_t idx) -> uint32_t {
@@ -853,6 +853,18 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out,
       return 0;
     }
     return (uint32_t)o;
+  };
+  // linear-combination term constants: f32 programs carry the f32 rounding
+  // (round to nearest, as the device's conversion) in the field's low word
+  auto lc_c = [&](double c) {
+    if (!f32) return c;
+    const float f = (float)c;
+    uint32_t u;
+    std::memcpy(&u, &f, sizeof u);
+    const uint64_t w = u;
+    double r;
+    std::memcpy(&r, &w, sizeof r);
+    return r;
   };
   auto fterm = [&](const PTerm& pt) {
     DFTerm f{};
@@ -909,7 +921,7 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out,
           DFPair pr{};
           for (uint32_t j = 0; j < 2 && k + j < n; ++j) {
             const PTerm& pt = p.terms[first + k + j];
-            pr.c[j] = pt.c;
+            pr.c[j] = lc_c(pt.c);
             pr.x[j] = off(pt.fxi);
             pr.m[j] = pt.fxm;
             pr.cx[j] = pt.kind == CK_CX ? 1 : 0;
@@ -961,7 +973,7 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out,
           for (uint32_t j = 0; j < 2 && k + j < n; ++j) {
             const PTerm& pt = p.terms[first + n - 1 - k - j];
             const DRTerm r = rterm(pt);
-            pr.c[j] = pt.c;
+            pr.c[j] = lc_c(pt.c);
             pr.ax[j] = r.ax;
             pr.flags[j] = r.flags;
           }

@@ -71,7 +71,8 @@ struct DevProgram {
   std::vector<DIns> fwd;
   std::vector<DRIns> rev;
 };
-bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, DevProgram& out, std::string& err);
+// `f32`: the program runs on f32 values (their linear-combination constants are stored rounded).
+bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, bool f32, DevProgram& out, std::string& err);
 
 // Validation with the reference's messages.  Empty string = valid.
 //   BytecodeTape::validate   (src/bytecode_tape/mod.rs:575-705)
