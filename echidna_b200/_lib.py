@@ -103,6 +103,10 @@ _SIGS = {
     "ech_laplacian_batch_device": ([_P, _P, _I, _P, _U32, _P, _U32, _I, _U64, _P, _P], _I),
     "ech_diagonal_kth_order_stochastic_f32": ([_P, _P, _P, _SZ, _U32, _P, _SZ, _P], _I),
     "ech_diagonal_kth_order_stochastic_f64": ([_P, _P, _P, _SZ, _U32, _P, _SZ, _P], _I),
+    "ech_stde_sparse_batch_f32": ([_P, _P, _P, _SZ, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, ctypes.c_float, _P, _U32,
+                                   _P], _I),
+    "ech_stde_sparse_batch_f64": ([_P, _P, _P, _SZ, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, ctypes.c_double, _P, _U32,
+                                   _P], _I),
     "ech_detect_hessian_sparsity": ([_P, _P, _P, _U32, _U32, _P, _P, _SZ, ctypes.POINTER(_SZ)], _I),
     "ech_detect_jacobian_sparsity": ([_P, _P, _P, _U32, _U32, _P, _U32, _P, _P, _SZ, ctypes.POINTER(_SZ)], _I),
     "ech_greedy_coloring": ([_U32, _P, _P, _SZ, _P, ctypes.POINTER(_U32)], _I),

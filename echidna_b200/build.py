@@ -27,7 +27,8 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC
            "--expt-relaxed-constexpr", "-I", CSRC, "-I", os.path.join(ROOT, "include")]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-ffp-contract=off", "-I", CSRC]
 
-CU_SOURCES = ["abi.cu", "k_plain.cu", "k_dual.cu", "k_jet.cu", "k_jet1.cu", "k_jet2.cu", "k_jet3.cu", "k_jet4.cu", "k_jet5.cu",
+CU_SOURCES = ["abi.cu", "k_plain.cu", "k_dual.cu", "k_jet.cu", "k_jet1.cu", "k_jet2.cu", "k_jet3.cu", "k_jet4.cu", "k_jet5.cu", "k_jet6.cu",
+              "k_jet7.cu", "k_jet8.cu", "k_jet9.cu",
               "stde.cu", "noalloc.cu", "k_multi.cu", "mlp.cu"]
 CXX_SOURCES = ["plan.cpp", "sparsity.cpp"]
 

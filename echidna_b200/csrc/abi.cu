@@ -341,6 +341,8 @@ struct SweepIO {
   uint32_t S = 0;
   int dir_mode = 0;
   uint64_t seed = 0;
+  const uint32_t* seed_off = nullptr;  // dir_mode 5
+  const void* seed_items = nullptr;
 };
 
 static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n_units, const SweepIO& io,
@@ -372,6 +374,8 @@ static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_
   kp.S = io.S;
   kp.dir_mode = io.dir_mode;
   kp.seed = io.seed;
+  kp.seed_off = io.seed_off;
+  kp.seed_items = io.seed_items;
   int bps = 0;
   cudaError_t e = launch_sweep(c.req, kp, 0, c.threads, c.smem, st, &bps);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
@@ -1092,6 +1096,119 @@ ECH_API ech_status ech_diagonal_kth_order_stochastic_f64(ech_ctx* ctx, const ech
                                                          uint32_t k, const uint32_t* sampled_indices,
                                                          size_t n_indices, ech_estimator_result* out) {
   return do_diag_kth<double>(ctx, t, x, n, k, sampled_indices, n_indices, out);
+}
+
+// stde_sparse (src/stde/sparse.rs:37-78) over the sampling distribution of a
+// homogeneous differential operator (SparseSamplingDistribution,
+// src/diffop.rs:896-1045), for many points: unit (b, s) runs one jet of order
+// jet_order + 1 seeded per entry (input var gets coefficient `slot` =
+// input_coeff, every input c0 = x), and sample = sign * Z * prefactor *
+// c_{output_coeff_index} enters the point's Welford accumulator in order.
+// The entry tables are the distribution's, flattened: entry e's seeds are
+// [entry_offsets[e], entry_offsets[e+1]) of vars / slots / input_coeffs.
+template <class T>
+static ech_status do_stde_sparse(ech_ctx* ctx, const ech_tape* tc, const T* xs, size_t n_xs, uint32_t B,
+                                 uint32_t n_entries, const uint32_t* off, const uint32_t* vars, const uint32_t* slots,
+                                 const T* coeffs, const uint32_t* kout, const T* pref, const T* sign, T z,
+                                 const uint64_t* idx, uint32_t S, ech_estimator_result* results) {
+  CHECK(common_checks(ctx, tc, sizeof(T) == 8));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  const uint32_t n = t->host.ni;
+  CHECK(stde_checks(t, n, "stde_sparse", "derivatives"));
+  CHECK(batch_args(t, B));
+  if (S == 0) return fail(ECH_ERR_OTHER, "sampled_indices must not be empty");
+  if (n_entries == 0) return fail(ECH_ERR_OTHER, "the distribution has no entries");
+  if (!xs || !off || !kout || !pref || !sign || !idx || !results) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  if (n_xs != (size_t)B * n) return fail(ECH_ERR_INVALID_ARG, "xs length must be batch_size * num_inputs");
+  const uint32_t n_items = off[n_entries];
+  if (n_items && (!vars || !slots || !coeffs)) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  uint32_t kmax = 0;
+  for (uint32_t e = 0; e < n_entries; ++e) {
+    if (off[e] > off[e + 1]) return fail(ECH_ERR_INVALID_ARG, "entry_offsets must be nondecreasing");
+    kmax = std::max(kmax, kout[e]);
+  }
+  const uint32_t K = kmax + 1;  // jet order = dist.jet_order() + 1
+  if (K > 9) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "jet order %u exceeds the GPU jets (at most 9: output coefficient index <= 8)", K);
+    return fail(ECH_ERR_OTHER, buf);
+  }
+  std::vector<SlotSeed> items(std::max<uint32_t>(n_items, 1));
+  for (uint32_t q = 0; q < n_items; ++q) {
+    if (vars[q] >= n) return fail(ECH_ERR_INVALID_ARG, "seed variable out of range");
+    items[q] = SlotSeed{vars[q], slots[q], (double)coeffs[q]};
+  }
+  const uint64_t units = (uint64_t)B * S;
+  std::vector<uint32_t> ent(units);
+  for (uint64_t u = 0; u < units; ++u) {
+    if (idx[u] >= n_entries) {
+      char buf[128];
+      snprintf(buf, sizeof buf, "sampled index %llu out of bounds (%u entries)", (unsigned long long)idx[u], n_entries);
+      return fail(ECH_ERR_OTHER, buf);
+    }
+    ent[u] = (uint32_t)idx[u];
+  }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  // io_in: xs | io_in2: unit entries, entry offsets, seeds, kout, prefactor, sign
+  auto r256 = [](uint64_t b) { return (b + 255) & ~(uint64_t)255; };
+  const uint64_t b_ent = r256(units * 4), b_off = r256((n_entries + 1) * 4ull), b_it = r256(items.size() * 16ull),
+                 b_k = r256(n_entries * 4ull), b_t = r256(n_entries * (uint64_t)sizeof(T));
+  CU(ctx->io_in.ensure((size_t)n_xs * sizeof(T)));
+  CU(ctx->io_in2.ensure(b_ent + b_off + b_it + b_k + 2 * b_t));
+  CU(ctx->io_out3.ensure(B * sizeof(ech_estimator_result)));
+  unsigned char* base = (unsigned char*)ctx->io_in2.p;
+  uint32_t* d_ent = (uint32_t*)base;
+  uint32_t* d_off = (uint32_t*)(base + b_ent);
+  SlotSeed* d_it = (SlotSeed*)(base + b_ent + b_off);
+  uint32_t* d_k = (uint32_t*)(base + b_ent + b_off + b_it);
+  T* d_pref = (T*)(base + b_ent + b_off + b_it + b_k);
+  T* d_sign = (T*)(base + b_ent + b_off + b_it + b_k + b_t);
+  cudaStream_t st = ctx->stream;
+  CU(cudaMemcpyAsync(ctx->io_in.p, xs, n_xs * sizeof(T), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(d_ent, ent.data(), units * 4, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(d_off, off, (n_entries + 1) * 4ull, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(d_it, items.data(), items.size() * 16ull, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(d_k, kout, n_entries * 4ull, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(d_pref, pref, n_entries * sizeof(T), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(d_sign, sign, n_entries * sizeof(T), cudaMemcpyHostToDevice, st));
+  CU(ctx->stde_tmp.ensure(units * (uint64_t)K * sizeof(T)));
+  SweepIO io;
+  io.x = ctx->io_in.p;
+  io.v = d_ent;
+  io.out = ctx->stde_tmp.p;
+  io.S = S;
+  io.dir_mode = 5;
+  io.seed_off = d_off;
+  io.seed_items = d_it;
+  CHECK(enqueue(ctx, t, 4, (int)K, units, io, st));
+  CU(launch_stde_sparse_reduce(sizeof(T) == 8, ctx->stde_tmp.p, units, d_ent, d_k, d_pref, d_sign, (double)z, B, S,
+                               ctx->io_out3.p, st));
+  CU(cudaMemcpyAsync(results, ctx->io_out3.p, B * sizeof(ech_estimator_result), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  return check_err_word(ctx);
+}
+
+ECH_API ech_status ech_stde_sparse_batch_f32(ech_ctx* ctx, const ech_tape* t, const float* xs, size_t n_xs, uint32_t B,
+                                             uint32_t n_entries, const uint32_t* entry_offsets, const uint32_t* vars,
+                                             const uint32_t* slots, const float* input_coeffs,
+                                             const uint32_t* output_coeff_index, const float* extraction_prefactor,
+                                             const float* sign, float normalization, const uint64_t* sampled_indices,
+                                             uint32_t n_samples, ech_estimator_result* results) {
+  return do_stde_sparse<float>(ctx, t, xs, n_xs, B, n_entries, entry_offsets, vars, slots, input_coeffs,
+                               output_coeff_index, extraction_prefactor, sign, normalization, sampled_indices,
+                               n_samples, results);
+}
+ECH_API ech_status ech_stde_sparse_batch_f64(ech_ctx* ctx, const ech_tape* t, const double* xs, size_t n_xs,
+                                             uint32_t B, uint32_t n_entries, const uint32_t* entry_offsets,
+                                             const uint32_t* vars, const uint32_t* slots, const double* input_coeffs,
+                                             const uint32_t* output_coeff_index, const double* extraction_prefactor,
+                                             const double* sign, double normalization,
+                                             const uint64_t* sampled_indices, uint32_t n_samples,
+                                             ech_estimator_result* results) {
+  return do_stde_sparse<double>(ctx, t, xs, n_xs, B, n_entries, entry_offsets, vars, slots, input_coeffs,
+                                output_coeff_index, extraction_prefactor, sign, normalization, sampled_indices,
+                                n_samples, results);
 }
 
 // ── estimators built on order-3 jets along host-built directions ──

@@ -172,6 +172,15 @@ struct alignas(16) DRPair {
 };
 static_assert(sizeof(DRPair) == sizeof(DRIns), "reverse term records are instruction-sized");
 
+// One seeded input coefficient of a slot-seeded jet (sparse STDE over a
+// differential operator): input `var` gets coefficient `slot` = `coef`.
+struct SlotSeed {
+  uint32_t var;
+  uint32_t slot;
+  double coef;
+};
+static_assert(sizeof(SlotSeed) == 16, "SlotSeed must be 16 bytes");
+
 // Interpreter geometry shared by every kernel.
 constexpr int kChunk = 128;   // instructions per staged chunk
 constexpr int kStages = 3;    // staged chunks in flight

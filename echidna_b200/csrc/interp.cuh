@@ -51,8 +51,11 @@ struct KParams {
   // STDE: units = points * S; directions from host or device RNG
   uint32_t S;            // directions per point (0 = not STDE)
   int dir_mode;          // 0: v per unit, 1: v shared [S][ni], 2: device Rademacher, 3: basis e_s,
-                         // 4: basis e_{v[u]} (v: one uint32 coordinate per unit)
+                         // 4: basis e_{v[u]} (v: one uint32 coordinate per unit),
+                         // 5: slot-seeded jets (v: one uint32 entry per unit into seed_off / seed_items)
   uint64_t seed;
+  const uint32_t* seed_off;  // dir_mode 5: entry e's seeds are seed_items[seed_off[e] .. seed_off[e+1])
+  const void* seed_items;    // SlotSeed records
 };
 
 // ───────────────────────────── bounded mbarrier waits ───────────────────────
@@ -342,6 +345,20 @@ template <class T, int K> struct Lane<dm::Jet<T, K>> {
     const T* x = (const T*)kp.x;
     const uint64_t xrow = kp.x_bcast ? 0 : (kp.S ? u / kp.S : u);
     j.c[0] = x[xrow * kp.ni + i];
+    if (kp.dir_mode == 5) {
+      // the unit's entry seeds coefficient `slot` of each of its active inputs
+      // (seed_taylor_dyn_jets, src/taylor_dyn.rs); every other coefficient is 0
+      const uint32_t e = reinterpret_cast<const uint32_t*>(kp.v)[u];
+      const SlotSeed* it = reinterpret_cast<const SlotSeed*>(kp.seed_items);
+      for (uint32_t q = kp.seed_off[e]; q < kp.seed_off[e + 1]; ++q) {
+        if (it[q].var != i) continue;
+        const T c = (T)it[q].coef;
+#pragma unroll
+        for (int k = 1; k < K; ++k)
+          if ((uint32_t)k == it[q].slot) j.c[k] = c;
+      }
+      return j;
+    }
     if (K > 1) j.c[1] = dir_component(kp, u, i);
     return j;
   }

@@ -36,4 +36,12 @@ cudaError_t launch_by_p(const LaunchReq& r, const KParams& kp, int grid, int blo
   }
 }
 
+// One point per thread only (wide jets used by the sparse STDE path).
+template <class V>
+cudaError_t launch_p1(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
+                      int* bps) {
+  if (r.rev || r.P != 1) return cudaErrorInvalidValue;
+  return launch_one<V, 1, false>(kp, grid, block, smem, st, bps);
+}
+
 }  // namespace ech

@@ -1,0 +1,11 @@
+// Sweep kernels on Taylor jets of order 7 (forward only, one point per thread):
+// the wide jets of sparse STDE over differential operators.
+#include "k_common.cuh"
+
+namespace ech {
+cudaError_t launch_jet7(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
+                        int* bps) {
+  return r.f64 ? launch_p1<dm::Jet<double, 7>>(r, kp, grid, block, smem, st, bps)
+               : launch_p1<dm::Jet<float, 7>>(r, kp, grid, block, smem, st, bps);
+}
+}  // namespace ech

@@ -53,6 +53,11 @@ cudaError_t launch_stde_reduce_t(bool f64, bool acc64, const void* c0, const voi
 cudaError_t launch_sample_coords(bool f64, const float* probs, uint32_t n, uint64_t npoints, uint32_t S,
                                  uint64_t seed, uint32_t* idx, void* wmul, cudaStream_t st);
 cudaError_t launch_scale(bool f64, void* y, double a, size_t n, cudaStream_t st);
+// Sparse STDE over a differential operator: per point, samples sign_e * Z *
+// prefactor_e * c_{kout[e]} of the sampled entries (Welford in the sample type).
+cudaError_t launch_stde_sparse_reduce(bool f64, const void* coeffs, uint64_t units, const uint32_t* ent,
+                                      const uint32_t* kout, const void* pref, const void* sign, double z,
+                                      uint64_t npoints, uint32_t S, void* results, cudaStream_t st);
 cudaError_t launch_control_term(bool f64, const void* dirs, const void* diag, uint32_t S, uint32_t n, void* cv,
                                 cudaStream_t st);
 

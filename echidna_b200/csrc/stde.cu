@@ -83,6 +83,54 @@ __global__ void stde_reduce_kernel(const T* c0, const T* ck, T scale, uint64_t n
   out[p] = r;
 }
 
+// stde_sparse (src/stde/sparse.rs:37-78), per point: for each sampled entry e
+// in order, raw = c_{k_e} * prefactor_e and sample = sign_e * Z * raw, Welford in
+// the sample type; the value is c0 of the point's last sample.  Coefficients
+// are coefficient-major, coeffs[k * units + u] (one scalar output).
+template <class T>
+__global__ void stde_sparse_reduce_kernel(const T* coeffs, uint64_t units, const uint32_t* ent, const uint32_t* kout,
+                                          const T* pref, const T* sign, T z, uint64_t npoints, uint32_t S,
+                                          ech_estimator_result* out) {
+  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npoints) return;
+  Welford<T> acc;
+  T value = T(0);
+  for (uint32_t s = 0; s < S; ++s) {
+    const uint64_t u = p * S + s;
+    const uint32_t e = ent[u];
+    value = coeffs[u];
+    const T raw = coeffs[(uint64_t)kout[e] * units + u] * pref[e];
+    const T sample = sign[e] * z * raw;
+    acc.update(sample);
+  }
+  T est, var, se;
+  acc.finalize(&est, &var, &se);
+  ech_estimator_result r;
+  r.value = (double)value;
+  r.estimate = (double)est;
+  r.sample_variance = (double)var;
+  r.standard_error = (double)se;
+  r.num_samples = acc.count;
+  out[p] = r;
+}
+
+cudaError_t launch_stde_sparse_reduce(bool f64, const void* coeffs, uint64_t units, const uint32_t* ent,
+                                      const uint32_t* kout, const void* pref, const void* sign, double z,
+                                      uint64_t npoints, uint32_t S, void* results, cudaStream_t st) {
+  const int threads = 128;
+  const unsigned blocks = (unsigned)((npoints + threads - 1) / threads);
+  if (blocks == 0) return cudaSuccess;
+  if (f64)
+    stde_sparse_reduce_kernel<double><<<blocks, threads, 0, st>>>((const double*)coeffs, units, ent, kout,
+                                                                  (const double*)pref, (const double*)sign, z,
+                                                                  npoints, S, (ech_estimator_result*)results);
+  else
+    stde_sparse_reduce_kernel<float><<<blocks, threads, 0, st>>>((const float*)coeffs, units, ent, kout,
+                                                                 (const float*)pref, (const float*)sign, (float)z,
+                                                                 npoints, S, (ech_estimator_result*)results);
+  return cudaGetLastError();
+}
+
 // v^T diag(H) v per direction, summed in index order in T (src/gpu/stde_gpu.rs:178-184).
 template <class T>
 __global__ void control_term_kernel(const T* dirs, const T* diag, uint32_t S, uint32_t n, T* cv) {

@@ -234,6 +234,31 @@ ECH_API ech_status ech_diagonal_kth_order_stochastic_f64(ech_ctx* ctx, const ech
                                                          size_t n, uint32_t k, const uint32_t* sampled_indices,
                                                          size_t n_indices, ech_estimator_result* out);
 
+/* stde::stde_sparse (src/stde/sparse.rs:37-78) over a SparseSamplingDistribution
+ * (src/diffop.rs:896-1045), for `batch` points xs [batch][n] with their own
+ * sampled entry indices sampled_indices [batch][n_samples]; batch = 1 is the
+ * reference call.  The distribution is passed flattened: entry e seeds inputs
+ * vars[q] at coefficient slots[q] with input_coeffs[q] (1/slot!) for q in
+ * [entry_offsets[e], entry_offsets[e+1]); output_coeff_index[e],
+ * extraction_prefactor[e] and sign[e] extract its sample sign * Z * prefactor *
+ * c_k with Z = normalization.  Jets run on the GPU up to order 9 (output
+ * coefficient index <= 8); Welford in the sample type, value = c0.  Errors:
+ * "sampled_indices must not be empty", out-of-range indices, scalar-output
+ * tapes only. */
+ECH_API ech_status ech_stde_sparse_batch_f32(ech_ctx* ctx, const ech_tape* tape, const float* xs, size_t n_xs,
+                                             uint32_t batch, uint32_t n_entries, const uint32_t* entry_offsets,
+                                             const uint32_t* vars, const uint32_t* slots, const float* input_coeffs,
+                                             const uint32_t* output_coeff_index, const float* extraction_prefactor,
+                                             const float* sign, float normalization, const uint64_t* sampled_indices,
+                                             uint32_t n_samples, ech_estimator_result* results);
+ECH_API ech_status ech_stde_sparse_batch_f64(ech_ctx* ctx, const ech_tape* tape, const double* xs, size_t n_xs,
+                                             uint32_t batch, uint32_t n_entries, const uint32_t* entry_offsets,
+                                             const uint32_t* vars, const uint32_t* slots, const double* input_coeffs,
+                                             const uint32_t* output_coeff_index, const double* extraction_prefactor,
+                                             const double* sign, double normalization,
+                                             const uint64_t* sampled_indices, uint32_t n_samples,
+                                             ech_estimator_result* results);
+
 /* ── many tapes in one launch (extension, no reference counterpart) ─────────
  * Gradient + per-point HVP for a batch of different tapes with uneven input
  * sizes and point counts, as one persistent launch.  Every pointer in an item is

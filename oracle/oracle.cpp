@@ -1030,6 +1030,51 @@ template <class F> void laplacian_stats_point(const Tape<F>& t, const F* x, cons
   out[0] = value; out[1] = est; out[2] = var; out[3] = se; out[4] = (F)acc.count;
 }
 
+// stde_sparse (src/stde/sparse.rs:37-78): per sampled entry e in order, input
+// jets c0 = x_i with coefficient slots[q] of input vars[q] set to coefs[q]
+// (seed_taylor_dyn_jets), one forward jet sweep, raw = c_{kout[e]} * pref[e],
+// sample = sign[e] * Z * raw into a Welford accumulator; value = c0 of the
+// primary output.  out = {value, estimate, variance, se, num_samples}.
+template <class F, int K>
+void stde_sparse_k(const Tape<F>& t, const F* x, const uint32_t* off, const uint32_t* vars, const uint32_t* slots,
+                   const F* coefs, const uint32_t* kout, const F* pref, const F* sign, F z, const uint64_t* idx,
+                   uint64_t nidx, F* out) {
+  std::vector<Tay<F, K>> in(t.ni), buf;
+  Welford<F> acc;
+  F value = F(0);
+  for (uint64_t s = 0; s < nidx; ++s) {
+    const uint64_t e = idx[s];
+    for (uint32_t i = 0; i < t.ni; ++i) {
+      for (int k = 0; k < K; ++k) in[i].c[k] = F(0);
+      in[i].c[0] = x[i];
+    }
+    for (uint32_t q = off[e]; q < off[e + 1]; ++q)
+      if (slots[q] < (uint32_t)K) in[vars[q]].c[slots[q]] = coefs[q];
+    forward_tangent<F, Tay<F, K>>(t, in.data(), buf);
+    const Tay<F, K>& o = buf[t.out_idx];
+    value = o.c[0];
+    const F raw = o.c[kout[e]] * pref[e];
+    const F sample = sign[e] * z * raw;
+    acc.update(sample);
+  }
+  F est, var, se;
+  acc.finalize(&est, &var, &se);
+  out[0] = value; out[1] = est; out[2] = var; out[3] = se; out[4] = (F)acc.count;
+}
+
+template <class F>
+int stde_sparse(const Tape<F>& t, int K, const F* x, const uint32_t* off, const uint32_t* vars, const uint32_t* slots,
+                const F* coefs, const uint32_t* kout, const F* pref, const F* sign, F z, const uint64_t* idx,
+                uint64_t nidx, F* out) {
+  switch (K) {
+#define ORC_SS(KK) \
+  case KK: stde_sparse_k<F, KK>(t, x, off, vars, slots, coefs, kout, pref, sign, z, idx, nidx, out); return 0;
+    ORC_SS(1) ORC_SS(2) ORC_SS(3) ORC_SS(4) ORC_SS(5) ORC_SS(6) ORC_SS(7) ORC_SS(8) ORC_SS(9) ORC_SS(10) ORC_SS(11)
+#undef ORC_SS
+    default: return -1;
+  }
+}
+
 }  // namespace orc
 
 // ───────────────────────── extern "C" surface ───────────────────────────────
@@ -1268,6 +1313,13 @@ template <class F, int ORDER> void dks(const orc::Tape<F>& t, const F* x, const 
                                   int nth) {                                                                        \
     auto t = mk<F>(d);                                                                                              \
     return orc::taylor_batch<F>(t, K, P, S, B, coeffs, nth);                                                        \
+  }                                                                                                                 \
+  ORC_EXPORT int orc_stde_sparse_##SUF(const orc_tape_desc* d, int K, const F* x, const uint32_t* off,             \
+                                       const uint32_t* vars, const uint32_t* slots, const F* coefs,                \
+                                       const uint32_t* kout, const F* pref, const F* sign, F z,                    \
+                                       const uint64_t* idx, uint64_t nidx, F* out) {                               \
+    auto t = mk<F>(d);                                                                                              \
+    return orc::stde_sparse<F>(t, K, x, off, vars, slots, coefs, kout, pref, sign, z, idx, nidx, out);              \
   }                                                                                                                 \
   ORC_EXPORT void orc_hessian_##SUF(const orc_tape_desc* d, const F* x, F* value, F* grad, F* hess) {              \
     hessian_full<F>(d, x, value, grad, hess);                                                                       \

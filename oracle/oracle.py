@@ -125,6 +125,23 @@ class OracleTape:
             raise ValueError(f"oracle: unsupported order {order}")
         return c
 
+    def stde_sparse(self, x, dist, sampled_indices):
+        """``stde::stde_sparse`` (``src/stde/sparse.rs:37-78``) at one point over a
+        ``SparseSamplingDistribution`` (``echidna_b200.diffop``); returns
+        (value, estimate, sample_variance, standard_error, num_samples)."""
+        off, vars_, slots, coefs, kout, pref, sign = dist.flatten()
+        coefs, pref, sign = (np.ascontiguousarray(a, dtype=self.dtype) for a in (coefs, pref, sign))
+        x = self._arr(x).ravel()
+        idx = np.ascontiguousarray(sampled_indices, dtype=np.uint64).ravel()
+        K = int(kout.max()) + 1
+        out = np.empty(5, dtype=self.dtype)
+        z = (ctypes.c_double if self.dtype == np.float64 else ctypes.c_float)(float(dist.normalization()))
+        rc = self._f("stde_sparse")(ctypes.byref(self.desc), K, _p(x), _p(off), _p(vars_), _p(slots), _p(coefs),
+                                     _p(kout), _p(pref), _p(sign), z, _p(idx), ctypes.c_uint64(idx.size), _p(out))
+        if rc != 0:
+            raise ValueError(f"oracle: unsupported jet order {K}")
+        return float(out[0]), float(out[1]), float(out[2]), float(out[3]), int(out[4])
+
     def hessian(self, x):
         x = self._arr(x)
         n = self.ni
