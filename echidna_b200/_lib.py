@@ -117,7 +117,7 @@ _SIGS = {
     "ech_gradient_batch_device_noalloc": ([_P, _P, _I, _P, _U32, _P, _P, _P], _I),
     "ech_tape_plan_stats": ([_P, _P, _I, _U32, _I, ctypes.POINTER(_U64)], _I),
     "ech_plan_dump": ([_P, _P, _P, _P, _U32, _U32, _U32, _P, _U32, _I, _U32, _P, _SZ, _P, _SZ, _P, _SZ, _P, _SZ,
-                       ctypes.POINTER(_U64)], _I),
+                       _P, _SZ, ctypes.POINTER(_U64)], _I),
 }
 
 

@@ -1690,7 +1690,7 @@ ECH_API ech_status ech_plan_dump(const uint32_t* op, const uint32_t* a0, const u
                                  uint32_t nv, uint32_t ni, uint32_t output_index, const uint32_t* outs,
                                  uint32_t nouts, int kind, uint32_t cap, void* fwd, size_t fwd_cap, void* rev,
                                  size_t rev_cap, double* pool, size_t pool_cap, void* terms, size_t terms_cap,
-                                 uint64_t* counts) {
+                                 void* gathers, size_t gathers_cap, uint64_t* counts) {
   if (!op || !a0 || !a1 || !values || !counts) return fail(ECH_ERR_INVALID_ARG, "null argument");
   std::string m = validate_bytecode_tape(op, a0, a1, nv, ni, output_index, outs, nouts, false);
   if (!m.empty()) return fail(ECH_ERR_OTHER, "invalid bytecode tape: " + m);
@@ -1713,6 +1713,8 @@ ECH_API ech_status ech_plan_dump(const uint32_t* op, const uint32_t* a0, const u
   counts[4] = p.far_slots;
   counts[5] = p.traj_slots;
   counts[6] = p.terms.size();
+  counts[7] = p.gathers.size();
+  if (gathers) memcpy(gathers, p.gathers.data(), std::min(gathers_cap, p.gathers.size()) * sizeof(GRec));
   if (terms) memcpy(terms, p.terms.data(), std::min(terms_cap, p.terms.size()) * sizeof(PTerm));
   if (fwd) memcpy(fwd, p.fwd.data(), std::min(fwd_cap, p.fwd.size()) * sizeof(Ins));
   if (rev) memcpy(rev, p.rev.data(), std::min(rev_cap, p.rev.size()) * sizeof(RIns));

@@ -20,6 +20,8 @@ enum OpCode : uint8_t {
   XI_SEED = 67,   // reverse: adj(r) <- 1
   XI_STGRAD = 68, // reverse: grad[aux] <- adj(r)   (r mode NONE -> 0)
   XI_CHAIN = 69,  // fused linear chain: dst <- acc0 (+|-) term_1 (+|-) ... ; terms in the chain table
+  XI_NORM = 84,   // reverse: adj(r) <- adj(r) passed through a unit Add (the chain's term adjoint)
+  XI_GATHER = 85, // reverse: each target adjoint accumulated over its chain contributions, stored once
 };
 
 // One term of a fused chain s_t = s_{t-1} (+|-) term_t.  `kind` says how the
@@ -99,6 +101,9 @@ enum DOp : uint8_t {
   D_MUL_RR, D_MUL_IR, D_MUL_RI, D_DIV_RR, D_DIV_IR, D_DIV_RI,  // .. 83
   D_CHAIN = 69,     // fused linear chain (forward and reverse)
   D_CHAIN_LC = 70,  // fused chain whose terms are all c*x or x*c added to the running value
+  D_NORM = 84,      // reverse: XI_NORM
+  D_GATHER = 85,    // reverse: XI_GATHER; per target a DRTerm header (ax, flags, ay = contributions)
+                    // followed by DRPair records (ax = the chain adjoint's offset, c)
   D_FU_BASE = 96,   // forward unary fast form: 96 + (op - OP_NEG), a and dst smem
   D_RF_BASE = 128,  // reverse fast form: 128 + op, every adjoint location in smem
 };

@@ -857,6 +857,63 @@ template <class V, int P> struct RevExec {
     return true;
   }
 
+  // Reverse gather (D_GATHER): for each target, its adjoint (+0 when this is
+  // its first contribution) plus c * t for each contribution in order, with
+  // the zero-adjoint skip and the zero-multiplier guard, then one store.  t is
+  // a chain's adjoint after D_NORM.  Contribution loads are grouped so several
+  // are in flight; the updates stay in order.
+  static constexpr int kGather = kWords <= 4 ? 4 : (kWords <= 8 ? 2 : 1);
+  __device__ __forceinline__ bool gather(Stream<48>& st, uint32_t ntargets) const {
+#pragma unroll 1
+    for (uint32_t g = 0; g < ntargets; ++g) {
+      const unsigned char* rec = st.next();
+      if (rec == nullptr) return false;
+      const uint4 h = *reinterpret_cast<const uint4*>(rec);
+      const uint32_t hf = h.x >> 16, nc = h.z;
+      unsigned char* px = loc(hf & CF_X_GLOB, h.y);
+      V cur[P];
+      lc_load(px, (hf & CF_X_INIT) != 0, cur);
+      uint32_t q = 0;
+      if constexpr (kGather > 1) {
+#pragma unroll 1
+        for (; q + 2 * kGather <= nc; q += 2 * kGather) {
+          V ts[2 * kGather][P];
+          V cs[2 * kGather];
+#pragma unroll
+          for (int k = 0; k < kGather; ++k) {
+            const unsigned char* r2 = st.next();
+            if (r2 == nullptr) return false;
+            const uint4 cw = *reinterpret_cast<const uint4*>(r2);
+            const uint4 aw = *reinterpret_cast<const uint4*>(r2 + 16);
+            C::ld(loc(aw.z & CF_X_GLOB, aw.x), ts[2 * k]);
+            C::ld(loc((aw.z >> 16) & CF_X_GLOB, aw.y), ts[2 * k + 1]);
+            cs[2 * k] = lc_const<V>(cw.x, cw.y);
+            cs[2 * k + 1] = lc_const<V>(cw.z, cw.w);
+          }
+#pragma unroll
+          for (int j = 0; j < 2 * kGather; ++j) lc_update(cur, ts[j], cs[j]);
+        }
+      }
+#pragma unroll 1
+      for (; q < nc; q += 2) {
+        const unsigned char* r2 = st.next();
+        if (r2 == nullptr) return false;
+        const uint4 cw = *reinterpret_cast<const uint4*>(r2);
+        const uint4 aw = *reinterpret_cast<const uint4*>(r2 + 16);
+        V t0[P];
+        C::ld(loc(aw.z & CF_X_GLOB, aw.x), t0);
+        lc_update(cur, t0, lc_const<V>(cw.x, cw.y));
+        if (q + 1 < nc) {
+          V t1[P];
+          C::ld(loc((aw.z >> 16) & CF_X_GLOB, aw.y), t1);
+          lc_update(cur, t1, lc_const<V>(cw.z, cw.w));
+        }
+      }
+      C::st(px, cur);
+    }
+    return true;
+  }
+
   // One reverse op: adj(a) += da * adj(r), adj(b) += db * adj(r) with the
   // zero-adjoint skip and the zero-multiplier guard.  FAST: every adjoint
   // location is in shared memory.
@@ -897,6 +954,18 @@ template <class V, int P> struct RevExec {
         return chain(st, flags, ro, ao, (uint32_t)aux);
       case D_CHAIN_LC:
         return chain_lc(st, flags, ro, ao, (uint32_t)aux);
+      case D_NORM: {
+        V a[P], one[P], t[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) one[p] = Kd::c(1);
+        unsigned char* pr = loc(flags & RF_R_GLOB, ro);
+        C::ld(pr, a);
+        internal(a, one, t);
+        C::st(pr, t);
+        return true;
+      }
+      case D_GATHER:
+        return gather(st, (uint32_t)aux);
       case D_STGRAD: {
         V g[P];
         if (ro == kNone) {

@@ -760,6 +760,159 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
       pl.stats.rev_ops++;
       emit_grads(i, i);
     }
+    // ── reverse gather of linear-combination chains ──
+    // A run of linear-combination chain reverses (constant acc0, every term
+    // c*x or x*c added) is rewritten when the reverse ops between them touch
+    // none of the run's adjoint targets and no chain's result is a target of
+    // the run: each chain becomes XI_NORM at its own position (its adjoint
+    // passed through the unit Add once, in place: the value every term of the
+    // chain multiplies), and one XI_GATHER after the run's last chain
+    // accumulates each target over the run's contributions, in the original
+    // order, and stores it once.  Every adjoint receives the same additions in
+    // the same order, so results are unchanged; the per-term read-modify-write
+    // of a target becomes a read of a chain adjoint.
+    bool grouped = false;
+    {
+      auto lc_chain = [&](const RSym& r) -> bool {
+        if (r.opc != XI_CHAIN || (r.flags & RF_HAS_A) || r.chain < 0) return false;
+        const Chain& ch = chains[r.chain];
+        if (ch.tn == 0) return false;
+        for (uint32_t q = ch.tb; q < ch.tb + ch.tn; ++q) {
+          const PTerm& pt = pl.terms[q];
+          if ((pt.kind != CK_CX && pt.kind != CK_XC) || pt.op != 0) return false;
+        }
+        return true;
+      };
+      // adjoint slots an entry reads or writes
+      auto touched = [&](const RSym& r, std::vector<int64_t>& out) {
+        out.clear();
+        if (r.r >= 0) out.push_back(r.r);
+        if (r.a >= 0) out.push_back(r.a);
+        if (r.b >= 0) out.push_back(r.b);
+        if (r.opc == XI_CHAIN && r.chain >= 0) {
+          const Chain& ch = chains[r.chain];
+          for (uint32_t q = ch.tb; q < ch.tb + ch.tn; ++q) {
+            const PTerm& pt = pl.terms[q];
+            if (pt.flags & CF_X_ADJ) out.push_back(pt.xs);
+            if (pt.flags & CF_Y_ADJ) out.push_back(pt.ys);
+          }
+        }
+      };
+      std::vector<RSym> out;
+      out.reserve(rs.size());
+      std::vector<int64_t> tv;
+      size_t k = 0;
+      while (k < rs.size()) {
+        if (!lc_chain(rs[k])) {
+          out.push_back(rs[k++]);
+          continue;
+        }
+        std::vector<size_t> members;
+        std::set<int64_t> targets, results;
+        size_t last = k;
+        for (size_t j = k; j < rs.size(); ++j) {
+          const RSym& e = rs[j];
+          if (lc_chain(e) && !targets.count(e.r)) {
+            const Chain& ch = chains[e.chain];
+            bool ok = true;
+            for (uint32_t q = ch.tb; q < ch.tb + ch.tn && ok; ++q) ok = !results.count(pl.terms[q].xs);
+            if (ok) {
+              members.push_back(j);
+              for (uint32_t q = ch.tb; q < ch.tb + ch.tn; ++q) targets.insert(pl.terms[q].xs);
+              results.insert(e.r);
+              last = j;
+              continue;
+            }
+          }
+          // runs before the gather: it must not touch the members' targets or results
+          touched(e, tv);
+          bool conflict = false;
+          for (int64_t x : tv) conflict = conflict || targets.count(x) || results.count(x);
+          if (conflict) break;
+        }
+        if (members.size() < 2) {
+          out.push_back(rs[k++]);
+          continue;
+        }
+        // targets in order of first contribution
+        std::vector<int64_t> order;
+        std::set<int64_t> seen;
+        for (size_t m : members) {
+          const Chain& ch = chains[rs[m].chain];
+          for (uint32_t q = ch.tn; q-- > 0;) {
+            const int64_t x = pl.terms[ch.tb + q].xs;
+            if (seen.insert(x).second) order.push_back(x);
+          }
+        }
+        RSym g = mk(XI_GATHER);
+        g.va = (uint32_t)pl.gathers.size();
+        g.aux = (int32_t)order.size();
+        for (int64_t x : order) {
+          GRec h{};
+          h.s = (uint32_t)x;
+          const size_t hpos = pl.gathers.size();
+          pl.gathers.push_back(h);
+          uint32_t nc = 0;
+          uint16_t hf = 0;
+          for (size_t m : members) {
+            const Chain& ch = chains[rs[m].chain];
+            for (uint32_t q = ch.tn; q-- > 0;) {
+              const PTerm& pt = pl.terms[ch.tb + q];
+              if (pt.xs != (uint32_t)x) continue;
+              if (pt.flags & CF_X_INIT) hf |= CF_X_INIT;
+              GRec c{};
+              c.s = (uint32_t)rs[m].r;
+              c.c = pt.c;
+              pl.gathers.push_back(c);
+              ++nc;
+            }
+          }
+          pl.gathers[hpos].n = nc;
+          pl.gathers[hpos].flags = hf;
+        }
+        size_t mi = 0;
+        for (size_t j = k; j <= last; ++j) {
+          if (mi < members.size() && members[mi] == j) {
+            RSym nr = mk(XI_NORM);
+            nr.r = rs[j].r;
+            out.push_back(nr);
+            ++mi;
+          } else {
+            out.push_back(rs[j]);
+          }
+        }
+        out.push_back(g);
+        grouped = true;
+        k = last + 1;
+      }
+      if (grouped) {
+        rs.swap(out);
+        // live ranges from the rewritten order: first to last access
+        std::fill(birth.begin(), birth.end(), -1);
+        std::fill(death.begin(), death.end(), -1);
+        auto at = [&](int64_t s2, int64_t pos) {
+          if (s2 < 0) return;
+          if (birth[s2] < 0) birth[s2] = pos;
+          death[s2] = pos;
+        };
+        for (size_t pos = 0; pos < rs.size(); ++pos) {
+          const RSym& e = rs[pos];
+          if (e.opc == XI_GATHER) {
+            // the gather reads its sources while it writes targets, so a target
+            // must not take a source's register: sources stay live one past it
+            for (uint32_t q = e.va, h = 0; h < (uint32_t)e.aux; ++h) {
+              const GRec& hd = pl.gathers[q];
+              for (uint32_t c = 1; c <= hd.n; ++c) at(pl.gathers[q + c].s, (int64_t)pos + 1);
+              at(hd.s, (int64_t)pos);
+              q += 1 + hd.n;
+            }
+            continue;
+          }
+          touched(e, tv);
+          for (int64_t x : tv) at(x, (int64_t)pos);
+        }
+      }
+    }
     // Every reachable op other than the seed has a reachable consumer, so its
     // adjoint is born (first contribution, RF_*_INIT) before it is read.
     LinearScan lsr;
@@ -799,6 +952,10 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
       in.vr = r.vr;
       in.flags = fl;
       pl.rev.push_back(in);
+    }
+    for (GRec& gr : pl.gathers) {
+      gr.mode = lsr.loc[gr.s].mode;
+      gr.idx = lsr.loc[gr.s].idx;
     }
     for (const Chain& ch : chains) {
       for (uint32_t q = 0; q < ch.tn; ++q) {
@@ -949,6 +1106,40 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, bool f32, DevPro
     DRIns d{};
     d.flags = in.flags;
     d.aux = in.aux;
+    if (in.opc == XI_NORM) {
+      d.opc = D_NORM;
+      d.r = off(in.r);
+      d.a = d.b = d.va = d.vb = d.vr = kNone;
+      out.rev.push_back(d);
+      continue;
+    }
+    if (in.opc == XI_GATHER) {
+      // per target: a header (target offset, flags, contribution count), then
+      // its contributions two per record (chain adjoint offset, constant)
+      d.opc = D_GATHER;
+      d.r = d.a = d.b = d.va = d.vb = d.vr = kNone;
+      out.rev.push_back(d);
+      for (uint32_t h = 0, q = in.va; h < (uint32_t)in.aux; ++h) {
+        const GRec& hd = p.gathers[q];
+        DRTerm head{};
+        head.flags = (uint16_t)(hd.flags | (hd.mode == M_GLOB ? CF_X_GLOB : 0));
+        head.ax = off(hd.idx);
+        head.ay = hd.n;
+        out.rev.push_back(as_record<DRIns>(head));
+        for (uint32_t c = 0; c < hd.n; c += 2) {
+          DRPair pr{};
+          for (uint32_t j = 0; j < 2 && c + j < hd.n; ++j) {
+            const GRec& g = p.gathers[q + 1 + c + j];
+            pr.c[j] = lc_c(g.c);
+            pr.ax[j] = off(g.idx);
+            pr.flags[j] = g.mode == M_GLOB ? (uint16_t)CF_X_GLOB : (uint16_t)0;
+          }
+          out.rev.push_back(as_record<DRIns>(pr));
+        }
+        q += 1 + hd.n;
+      }
+      continue;
+    }
     if (in.opc == XI_CHAIN) {
       // the terms follow the instruction, last term first
       const uint32_t first = in.va, n = (uint32_t)in.aux;

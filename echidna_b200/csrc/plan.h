@@ -48,8 +48,25 @@ struct PTerm {
 };
 static_assert(sizeof(PTerm) == 48, "PTerm must be 48 bytes");
 
+// One record of a reverse gather (XI_GATHER): a target header followed by its
+// contributions.  Header: s = the target's adjoint slot id, n = contributions
+// that follow, flags CF_X_INIT (first contribution to the target); a
+// contribution: s = a chain result whose normalised adjoint is multiplied by c.
+// mode / idx: the slot after allocation.
+struct GRec {
+  uint32_t s;
+  uint32_t n;
+  uint16_t flags;
+  uint8_t mode, pad;
+  uint32_t idx;
+  double c;
+  uint64_t pad2;
+};
+static_assert(sizeof(GRec) == 32, "GRec must be 32 bytes");
+
 struct Plan {
   std::vector<PTerm> terms;  // fused-chain terms, shared by both programs
+  std::vector<GRec> gathers; // reverse gather records (XI_GATHER: va = first header, aux = targets)
   std::vector<Ins> fwd;
   std::vector<RIns> rev;
   std::vector<double> pool;

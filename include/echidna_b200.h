@@ -414,15 +414,16 @@ ECH_API ech_status ech_tape_plan_stats(ech_ctx* ctx, const ech_tape* tape, int k
                                        uint64_t* stats);
 /* Host-only lowering dump (no device needed): the forward / reverse programs
  * (32-byte records) and constant pool for `kind` with `smem_reg_cap` shared
- * registers, plus the fused-chain terms (48-byte records).  counts[7]: n_fwd,
- * n_rev, n_pool, smem_regs, far_slots, traj_slots, n_terms.  Used to check
- * the lowering on machines without a GPU. */
+ * registers, plus the fused-chain terms (48-byte records) and the reverse
+ * gather records (32-byte).  counts[8]: n_fwd, n_rev, n_pool, smem_regs,
+ * far_slots, traj_slots, n_terms, n_gather_records.  Used to check the
+ * lowering on machines without a GPU. */
 ECH_API ech_status ech_plan_dump(const uint32_t* opcodes, const uint32_t* arg0, const uint32_t* arg1,
                                  const double* values, uint32_t num_variables, uint32_t num_inputs,
                                  uint32_t output_index, const uint32_t* output_indices, uint32_t n_output_indices,
                                  int kind, uint32_t smem_reg_cap, void* fwd, size_t fwd_cap, void* rev,
                                  size_t rev_cap, double* pool, size_t pool_cap, void* terms, size_t terms_cap,
-                                 uint64_t* counts);
+                                 void* gathers, size_t gathers_cap, uint64_t* counts);
 /* Launch configuration override for tuning (0 = automatic): threads per CTA,
  * points per thread and the shared-register cap. */
 ECH_API ech_status ech_ctx_set_launch(ech_ctx* ctx, uint32_t threads, uint32_t points_per_thread,

@@ -18,7 +18,9 @@ from echidna_b200.tape import OpCode
 INS = struct.Struct("<BBBBIIIIid")
 RINS = struct.Struct("<BBHIIIIIIi")
 TERM = struct.Struct("<BBHIIBBBBIIIIIId")   # PTerm, 48 bytes
+GREC = struct.Struct("<IIHBBIdQ")            # GRec, 32 bytes
 XI_LDIN, XI_STOUT, XI_MOV, XI_SEED, XI_STGRAD, XI_CHAIN = 64, 65, 66, 67, 68, 69
+XI_NORM, XI_GATHER = 84, 85
 CK_X, CK_CX, CK_XC, CK_XY, CK_C = range(5)
 CF = dict(X_INIT=1, Y_INIT=2, X_GLOB=4, Y_GLOB=8, X_ADJ=16, Y_ADJ=32)
 M_SMEM, M_GLOB, M_IMM, M_NONE = 0, 1, 2, 3
@@ -32,18 +34,19 @@ def plan_dump(tape, kind: str, cap: int):
     op, a0, a1, vals = tape.arrays()
     vals = np.ascontiguousarray(vals, dtype=np.float64)
     outs = np.asarray(tape.output_indices, dtype=np.uint32)
-    counts = (ctypes.c_uint64 * 7)()
+    counts = (ctypes.c_uint64 * 8)()
     args = [_lib.ptr(op), _lib.ptr(a0), _lib.ptr(a1), _lib.ptr(vals), len(op), tape.num_inputs, tape.output_index,
             _lib.ptr(outs), len(outs), KIND[kind], cap]
-    st = lib.ech_plan_dump(*args, None, 0, None, 0, None, 0, None, 0, counts)
+    st = lib.ech_plan_dump(*args, None, 0, None, 0, None, 0, None, 0, None, 0, counts)
     assert st == 0, _lib.last_error()
-    nf, nr, npool, nt = counts[0], counts[1], counts[2], counts[6]
+    nf, nr, npool, nt, ng = counts[0], counts[1], counts[2], counts[6], counts[7]
+    gb = ctypes.create_string_buffer(max(ng, 1) * 32)
     fb = ctypes.create_string_buffer(max(nf, 1) * 32)
     rb = ctypes.create_string_buffer(max(nr, 1) * 32)
     tb = ctypes.create_string_buffer(max(nt, 1) * 48)
     pool = np.zeros(max(npool, 1), dtype=np.float64)
     st = lib.ech_plan_dump(*args, ctypes.addressof(fb), nf, ctypes.addressof(rb), nr, _lib.ptr(pool), npool,
-                           ctypes.addressof(tb), nt, counts)
+                           ctypes.addressof(tb), nt, ctypes.addressof(gb), ng, counts)
     assert st == 0, _lib.last_error()
     fwd = [INS.unpack_from(fb, 32 * k) for k in range(nf)]
     rev = [RINS.unpack_from(rb, 32 * k) for k in range(nr)]
@@ -52,7 +55,12 @@ def plan_dump(tape, kind: str, cap: int):
         (kind_, op_, flags, xs, ys, fxm, fym, rxm, rym, fxi, fyi, rxi, ryi, vx, vy, c) = TERM.unpack_from(tb, 48 * k)
         terms.append(dict(kind=kind_, op=op_, flags=flags, fxm=fxm, fym=fym, fxi=fxi, fyi=fyi, rxm=rxm, rym=rym,
                           rxi=rxi, ryi=ryi, vx=vx, vy=vy, c=c))
-    return fwd, rev, pool, dict(smem_regs=counts[3], far_slots=counts[4], traj_slots=counts[5], terms=terms)
+    gathers = []
+    for k in range(ng):
+        s, n, flags, mode, _pad, idx, c, _p2 = GREC.unpack_from(gb, 32 * k)
+        gathers.append(dict(s=s, n=n, flags=flags, mode=mode, idx=idx, c=c))
+    return fwd, rev, pool, dict(smem_regs=counts[3], far_slots=counts[4], traj_slots=counts[5], terms=terms,
+                                gathers=gathers)
 
 
 def _fwd(op, a, b, aux):
@@ -170,7 +178,25 @@ def run_gradient(tape, X, cap):
         if opc == XI_STGRAD:
             grads[:, aux] = 0.0 if r == NONE else regs[mr][r]
             continue
+        if opc == XI_GATHER:
+            gathers = info["gathers"]
+            q = va
+            for _ in range(aux):
+                hd = gathers[q]
+                cur = np.zeros(B) if hd["flags"] & CF["X_INIT"] else regs[hd["mode"]][hd["idx"]]
+                for g in gathers[q + 1:q + 1 + hd["n"]]:
+                    t = regs[g["mode"]][g["idx"]]
+                    hit = (t != 0) & (g["c"] != 0)
+                    with np.errstate(all="ignore"):
+                        cur = np.where(hit, cur + g["c"] * t, cur)
+                regs[hd["mode"]][hd["idx"]] = cur
+                q += 1 + hd["n"]
+            continue
         adj = regs[mr][r]
+        if opc == XI_NORM:
+            with np.errstate(all="ignore"):
+                regs[mr][r] = np.where(adj != 0, 0.0 + 1.0 * adj, 0.0)
+            continue
         if opc == XI_CHAIN:
             adj_s = adj
 

@@ -9,8 +9,36 @@ from oracle.oracle import OracleTape
 from tests.plan_emulator import plan_dump, run_gradient
 
 
+def _lc_net(seed, n=5):
+    """Layers of dot products over earlier values (repeated operands allowed),
+    each followed by tanh or by a product with an earlier value, so reverse
+    gathers form, break on conflicts and mix with other ops."""
+    rng = np.random.default_rng(seed)
+
+    def f(v):
+        vals = list(v)
+        for _layer in range(3):
+            new = []
+            for _j in range(4):
+                s = constant(float(rng.normal()))
+                for i in rng.choice(len(vals), size=int(rng.integers(1, 6)), replace=True):
+                    s = s + constant(float(rng.normal())) * vals[int(i)]
+                s = s.tanh() if rng.random() < 0.5 else s * vals[int(rng.integers(len(vals)))]
+                new.append(s)
+            vals = vals + new
+        out = constant(0.0)
+        for x in vals[-4:]:
+            out = out + x * x
+        return out
+    return record(f, [0.1] * n)[0]
+
+
 def _tapes():
     yield "rosen10", configs.rosenbrock(10)
+    yield "mlp8", configs.mlp(8, 8)
+    yield "lcnet1", _lc_net(1)
+    yield "lcnet2", _lc_net(2)
+    yield "lcnet3", _lc_net(3, n=3)
     yield "mlp4", configs.mlp(4, 4)
     yield "dag", configs.random_dag(6, 300, seed=7)
     yield "dag2", configs.random_dag(3, 120, seed=11)
@@ -55,3 +83,17 @@ def test_mlp_trajectory_is_three_layers_of_width():
     tape = configs.mlp(64, 64)
     _, _, _, info = plan_dump(tape, "gradient", 4096)
     assert info["traj_slots"] == 3 * 64
+
+
+def test_dense_layers_reverse_as_gathers():
+    # the MLP's two dense layers: every chain reverse becomes a normalisation and
+    # each layer one gather (one store per input adjoint)
+    tape = configs.mlp(8, 8)
+    _, rev, _, info = plan_dump(tape, "gradient", 4096)
+    ops = [r[0] for r in rev]
+    assert ops.count(85) >= 2 and ops.count(84) == 16 and ops.count(69) <= 1
+    headers, q = [], 0
+    while q < len(info["gathers"]):
+        headers.append(info["gathers"][q])
+        q += 1 + info["gathers"][q]["n"]
+    assert sorted(h["n"] for h in headers) == [8] * 16
