@@ -82,6 +82,11 @@ struct ech_ctx {
   bool autotune = true;        // pick launch shapes by timing (per tape, kind, batch size)
   std::mutex mu;
   DevBuf scratch, io_in, io_in2, io_out, io_out2, io_out3, stde_tmp;
+  // host-buffer sweeps of large batches run as chunks, one stream each
+  static constexpr int kPipe = 4;
+  cudaStream_t pipe[kPipe] = {};
+  cudaEvent_t pipe_ev = nullptr;
+  DevBuf pipe_scratch[kPipe];
   uint32_t* d_err = nullptr;
   // launch overrides (0 = automatic)
   uint32_t ov_threads = 0, ov_ppt = 0, ov_cap = 0;
@@ -139,6 +144,12 @@ extern "C" ECH_API void ech_ctx_destroy(ech_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (cudaStream_t s : ctx->pipe)
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  if (ctx->pipe_ev) cudaEventDestroy(ctx->pipe_ev);
   if (ctx->d_err) cudaFree(ctx->d_err);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -346,7 +357,8 @@ struct SweepIO {
 };
 
 static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n_units, const SweepIO& io,
-                             cudaStream_t st, LaunchCfg c) {
+                             cudaStream_t st, LaunchCfg c, DevBuf* scratch = nullptr) {
+  if (!scratch) scratch = &ctx->scratch;
   DevPlan* dp = nullptr;
   ech_status s = get_plan(t, kind, K, c.cap, c.tile, (uint32_t)c.vbytes, &dp);
   if (s != ECH_OK) return s;
@@ -385,8 +397,8 @@ static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_
   const uint64_t slots = (uint64_t)p.far_slots + p.traj_slots;
   uint64_t stride = slots * c.tile * c.vbytes;
   stride = (stride + 255) & ~(uint64_t)255;
-  CU(ctx->scratch.ensure(std::max<uint64_t>(stride * grid, 256)));
-  kp.scratch = ctx->scratch.p;
+  CU(scratch->ensure(std::max<uint64_t>(stride * grid, 256)));
+  kp.scratch = scratch->p;
   kp.scratch_stride_bytes = stride;
   if (grid == 0) return ECH_OK;
   e = launch_sweep(c.req, kp, (int)grid, c.threads, c.smem, st, &bps);
@@ -475,6 +487,94 @@ static ech_status enqueue(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n
   return launch_cfg(ctx, t, kind, K, n_units, io, st, choose_cfg(ctx, t, kind, K));
 }
 
+// ── host-buffer sweeps in chunks ──
+// A host-buffer call on a large batch whose launch shape is already tuned runs
+// as ech_ctx::kPipe chunks, each on its own stream: copy its inputs in, sweep,
+// copy its outputs out, so the copies of one chunk overlap the sweeps of the
+// others.  Every chunk uses the whole batch's tuned shape (the chunks' kernels
+// run side by side and together fill the GPU like one launch) and its own
+// per-CTA scratch.  Results are the same as one launch (a point's arithmetic
+// does not depend on the launch).  The first call of a (tape, kind, batch
+// octave) runs whole and tunes the shape.
+struct PipeArray {
+  void* dev;          // device base (inputs: destination; outputs: source)
+  void* host;         // host base
+  size_t unit_bytes;  // bytes per unit
+  bool in;
+};
+static constexpr uint64_t kPipeMinUnits = 16384;
+
+static ech_status run_pipelined(ech_ctx* ctx, ech_tape* t, int kind, uint64_t n_units, const SweepIO& io,
+                                const size_t io_unit_bytes[5], const std::vector<PipeArray>& arrays, bool* done) {
+  *done = false;
+  const bool overridden = ctx->ov_threads || ctx->ov_ppt || ctx->ov_cap;
+  if (overridden || !ctx->autotune || n_units < kPipeMinUnits) return ECH_OK;
+  Shape sh;
+  {
+    std::lock_guard<std::mutex> lk(t->mu);
+    auto it = t->shapes.find(std::make_tuple(kind, 0, size_bucket(n_units)));
+    if (it == t->shapes.end()) return ECH_OK;
+    sh = it->second;
+  }
+  const LaunchCfg c = cfg_for(ctx, t, kind, 0, sh);
+  if (!ctx->pipe_ev) CU(cudaEventCreateWithFlags(&ctx->pipe_ev, cudaEventDisableTiming));
+  for (cudaStream_t& s : ctx->pipe)
+    if (!s) CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  // the chunks start after the context stream's earlier work
+  CU(cudaEventRecord(ctx->pipe_ev, ctx->stream));
+  const int nc = ech_ctx::kPipe;
+  uint64_t per = (n_units + nc - 1) / nc;
+  per = (per + c.tile - 1) / c.tile * c.tile;
+  ech_status first = ECH_OK;
+  for (int k = 0; k < nc; ++k) {
+    const uint64_t off = (uint64_t)k * per;
+    if (off >= n_units) break;
+    const uint64_t n = std::min<uint64_t>(per, n_units - off);
+    cudaStream_t st = ctx->pipe[k];
+    cudaError_t e = cudaStreamWaitEvent(st, ctx->pipe_ev, 0);
+    for (const PipeArray& a : arrays) {
+      if (e != cudaSuccess || !a.in) continue;
+      e = cudaMemcpyAsync((unsigned char*)a.dev + off * a.unit_bytes, (const unsigned char*)a.host + off * a.unit_bytes,
+                          n * a.unit_bytes, cudaMemcpyHostToDevice, st);
+    }
+    if (e != cudaSuccess) {
+      first = cuda_fail(e, "chunk copy");
+      break;
+    }
+    SweepIO ck = io;
+    auto shift = [&](const void* p, size_t ub) -> const void* {
+      return (p && ub) ? (const void*)((const unsigned char*)p + off * ub) : p;
+    };
+    ck.x = shift(io.x, io_unit_bytes[0]);
+    ck.v = shift(io.v, io_unit_bytes[1]);
+    ck.out = const_cast<void*>(shift(io.out, io_unit_bytes[2]));
+    ck.out2 = const_cast<void*>(shift(io.out2, io_unit_bytes[3]));
+    ck.out3 = const_cast<void*>(shift(io.out3, io_unit_bytes[4]));
+    ech_status s = launch_cfg(ctx, t, kind, 0, n, ck, st, c, &ctx->pipe_scratch[k]);
+    if (s != ECH_OK) {
+      first = s;
+      break;
+    }
+    for (const PipeArray& a : arrays) {
+      if (e != cudaSuccess || a.in) continue;
+      e = cudaMemcpyAsync((unsigned char*)a.host + off * a.unit_bytes, (const unsigned char*)a.dev + off * a.unit_bytes,
+                          n * a.unit_bytes, cudaMemcpyDeviceToHost, st);
+    }
+    if (e != cudaSuccess) {
+      first = cuda_fail(e, "chunk copy");
+      break;
+    }
+  }
+  // every chunk's copies finish before the host buffers are handed back
+  for (cudaStream_t st : ctx->pipe) {
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess && first == ECH_OK) first = cuda_fail(e, "chunk sync");
+  }
+  if (first != ECH_OK) return first;
+  *done = true;
+  return ECH_OK;
+}
+
 static ech_status check_err_word(ech_ctx* ctx) {
   uint32_t h = 0;
   CU(cudaMemcpy(&h, ctx->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost));
@@ -560,11 +660,20 @@ static ech_status do_gradient(ech_ctx* ctx, const ech_tape* tc, const T* in, siz
   CU(ctx->io_in.ensure(n_in * sizeof(T)));
   CU(ctx->io_out.ensure(n_out * sizeof(T)));
   CU(ctx->io_out2.ensure(n_grads * sizeof(T)));
-  CU(cudaMemcpyAsync(ctx->io_in.p, in, n_in * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
   SweepIO io;
   io.x = ctx->io_in.p;
   io.out = ctx->io_out.p;
   io.out2 = ctx->io_out2.p;
+  {
+    const size_t ub[5] = {ni * sizeof(T), 0, no * sizeof(T), ni * sizeof(T), 0};
+    const std::vector<PipeArray> arr = {{ctx->io_in.p, const_cast<T*>(in), ni * sizeof(T), true},
+                                        {ctx->io_out.p, out, no * sizeof(T), false},
+                                        {ctx->io_out2.p, grads, ni * sizeof(T), false}};
+    bool done = false;
+    CHECK(run_pipelined(ctx, t, 1, B, io, ub, arr, &done));
+    if (done) return check_err_word(ctx);
+  }
+  CU(cudaMemcpyAsync(ctx->io_in.p, in, n_in * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
   CHECK(enqueue(ctx, t, 1, 0, B, io, ctx->stream));
   CU(cudaMemcpyAsync(out, ctx->io_out.p, n_out * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
   CU(cudaMemcpyAsync(grads, ctx->io_out2.p, n_grads * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
@@ -591,14 +700,24 @@ static ech_status do_hvp(ech_ctx* ctx, const ech_tape* tc, const T* x, size_t n_
   CU(ctx->io_in2.ensure(n_dirs * sizeof(T)));
   CU(ctx->io_out2.ensure(n_grads * sizeof(T)));
   CU(ctx->io_out3.ensure(n_hvps * sizeof(T)));
-  CU(cudaMemcpyAsync(ctx->io_in.p, x, n_x * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
-  CU(cudaMemcpyAsync(ctx->io_in2.p, dirs, n_dirs * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
   SweepIO io;
   io.x = ctx->io_in.p;
   io.v = ctx->io_in2.p;
   io.x_bcast = per_point ? 0 : 1;
   io.out2 = ctx->io_out2.p;
   io.out3 = ctx->io_out3.p;
+  if (per_point) {
+    const size_t ub[5] = {ni * sizeof(T), ni * sizeof(T), 0, ni * sizeof(T), ni * sizeof(T)};
+    const std::vector<PipeArray> arr = {{ctx->io_in.p, const_cast<T*>(x), ni * sizeof(T), true},
+                                        {ctx->io_in2.p, const_cast<T*>(dirs), ni * sizeof(T), true},
+                                        {ctx->io_out2.p, grads, ni * sizeof(T), false},
+                                        {ctx->io_out3.p, hvps, ni * sizeof(T), false}};
+    bool done = false;
+    CHECK(run_pipelined(ctx, t, 2, B, io, ub, arr, &done));
+    if (done) return check_err_word(ctx);
+  }
+  CU(cudaMemcpyAsync(ctx->io_in.p, x, n_x * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(ctx->io_in2.p, dirs, n_dirs * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
   CHECK(enqueue(ctx, t, 2, 0, B, io, ctx->stream));
   CU(cudaMemcpyAsync(grads, ctx->io_out2.p, n_grads * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
   CU(cudaMemcpyAsync(hvps, ctx->io_out3.p, n_hvps * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
