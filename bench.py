@@ -453,12 +453,20 @@ class UnevenWorkload:
                 "multi_shape": self.multi.info()}
 
     def e2e_step(self):
-        from echidna_b200 import _lib
-        P = _lib.ptr
-        for _, gt, n, *_, hx, hv, hg, hh in self.jobs:
-            st = self.lib.ech_hvp_batch_points_f32(self.ctx._h, gt._h, P(hx), hx.size, P(hv), hv.size, n, P(hg),
-                                                   hg.size, P(hh), hh.size)
-            assert st == 0, _lib.last_error()
+        """Through the many-tape API: every tape's points and directions copied in
+        from pinned host memory, one persistent launch, gradients and HVPs copied
+        back (all on the launch stream), then a synchronise."""
+        torch = self.torch
+        ext = torch.cuda.ExternalStream(self.sp)
+        with torch.cuda.stream(ext):
+            for _, _, _, dx, dv, _, _, hx, hv, _, _ in self.jobs:
+                dx.copy_(torch.from_numpy(hx), non_blocking=True)
+                dv.copy_(torch.from_numpy(hv), non_blocking=True)
+            self.multi.launch(self.sp)
+            for _, _, _, _, _, g, h, _, _, hg, hh in self.jobs:
+                torch.from_numpy(hg).copy_(g, non_blocking=True)
+                torch.from_numpy(hh).copy_(h, non_blocking=True)
+        ext.synchronize()
 
     def io_bytes(self):
         h2d = sum(j[7].nbytes + j[8].nbytes for j in self.jobs)
