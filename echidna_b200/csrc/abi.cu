@@ -268,6 +268,7 @@ struct LaunchCfg {
   uint32_t tile = 128;
   uint32_t cap = 0;
   size_t smem = 0;
+  size_t smem_full = 0;  // the shape's whole per-CTA share of shared memory
   size_t vbytes = 0;
 };
 
@@ -302,6 +303,7 @@ static LaunchCfg cfg_for(ech_ctx* ctx, const ech_tape* t, int kind, int K, Shape
   size_t cap = per_cta > (size_t)kRingBytes ? (per_cta - kRingBytes) / (c.tile * c.vbytes) : 0;
   if (ctx->ov_cap) cap = std::min<size_t>(cap, ctx->ov_cap);
   c.cap = (uint32_t)std::max<size_t>(cap, 1);
+  c.smem_full = per_cta;
   return c;
 }
 
@@ -365,6 +367,12 @@ static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_
   const Plan& p = dp->host;
   const uint32_t regs = std::max<uint32_t>(p.smem_regs, 1);
   c.smem = kRingBytes + (size_t)regs * c.tile * c.vbytes;
+  // the trajectory goes to shared memory when it fits the shape's share beside
+  // the registers (narrow CTAs on small batches): the reverse then reads it at
+  // shared-memory latency
+  const size_t smem_traj = c.smem + (size_t)p.traj_slots * c.tile * c.vbytes;
+  const bool traj_smem = p.traj_slots > 0 && smem_traj <= std::min(c.smem_full, ctx->smem_optin);
+  if (traj_smem) c.smem = smem_traj;
   KParams kp{};
   kp.fwd = dp->d_fwd;
   kp.n_fwd = dp->n_fwd;
@@ -372,6 +380,7 @@ static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_
   kp.n_rev = c.req.rev ? dp->n_rev : 0u;
   kp.far_slots = p.far_slots;
   kp.smem_regs = regs;
+  kp.traj_smem = traj_smem ? 1u : 0u;
   kp.tile = c.tile;
   kp.n_units = n_units;
   kp.ni = t->host.ni;
@@ -394,7 +403,7 @@ static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_
   if (bps <= 0) return fail(ECH_ERR_OTHER, "tape live set does not fit the shared-memory slot file");
   const uint64_t ntiles = (n_units + c.tile - 1) / c.tile;
   const uint64_t grid = std::min<uint64_t>(ntiles, (uint64_t)bps * ctx->sm_count);
-  const uint64_t slots = (uint64_t)p.far_slots + p.traj_slots;
+  const uint64_t slots = (uint64_t)p.far_slots + (traj_smem ? 0 : p.traj_slots);
   uint64_t stride = slots * c.tile * c.vbytes;
   stride = (stride + 255) & ~(uint64_t)255;
   CU(scratch->ensure(std::max<uint64_t>(stride * grid, 256)));
@@ -422,7 +431,7 @@ static int size_bucket(uint64_t n) {
 static const Shape kShapes[] = {
     {128, 1, 1}, {128, 1, 2}, {128, 1, 3}, {128, 1, 4}, {128, 2, 1}, {128, 2, 2},
     {128, 2, 3}, {128, 4, 1}, {128, 4, 2}, {256, 1, 1}, {256, 1, 2}, {64, 2, 4},
-    {64, 1, 2}, {64, 1, 4}, {32, 1, 2}, {32, 1, 4},
+    {64, 1, 2}, {64, 1, 4}, {32, 1, 2}, {32, 1, 4}, {64, 1, 1}, {32, 1, 1},
 };
 
 static ech_status tune(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n_units, const SweepIO& io,

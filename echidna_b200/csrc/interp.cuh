@@ -36,6 +36,7 @@ struct KParams {
   uint64_t scratch_stride_bytes;  // bytes per CTA region
   uint32_t far_slots;    // global slots before the trajectory region
   uint32_t smem_regs;    // shared-memory registers
+  uint32_t traj_smem;    // 1: the trajectory rows follow the shared registers (else in the global scratch)
   uint32_t tile;         // points per CTA tile
   uint64_t n_units;      // evaluation units (points, or point-direction pairs)
   uint32_t ni, no;       // inputs / outputs per unit
@@ -1005,7 +1006,8 @@ __device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned
   const uint32_t tile = kp.tile;
   const size_t colb = (size_t)threadIdx.x * P * sizeof(V);
   unsigned char* gs = gbase + colb;
-  unsigned char* tj = gbase + (size_t)kp.far_slots * tile * sizeof(V) + colb;
+  unsigned char* tj = kp.traj_smem ? sm + (size_t)kp.smem_regs * tile * sizeof(V)
+                                   : gbase + (size_t)kp.far_slots * tile * sizeof(V) + colb;
   const uint64_t unit0 = t * tile + (uint64_t)threadIdx.x * P;
   FwdExec<V, P> fx{kp, sm, gs, tj, unit0, {}};
 #pragma unroll
