@@ -406,8 +406,20 @@ class UnevenWorkload:
             hg, hh = _pinned(torch, np.empty_like(x)), _pinned(torch, np.empty_like(x))
             self.jobs.append((tape, gt, n, dx, dv, g, h, hx, hv, hg, hh))
         torch.cuda.synchronize()
-        self.multi = MultiTapeHvp(ctx, [(gt, dx.data_ptr(), dv.data_ptr(), n, g.data_ptr(), h.data_ptr())
-                                        for _, gt, n, dx, dv, g, h, *_ in self.jobs], f64=False, autotune=True)
+        items = [(gt, dx.data_ptr(), dv.data_ptr(), n, g.data_ptr(), h.data_ptr())
+                 for _, gt, n, dx, dv, g, h, *_ in self.jobs]
+        self.multi = MultiTapeHvp(ctx, items, f64=False, autotune=True)
+        # end to end: the tapes in four groups of about equal bytes, each its own
+        # many-tape launch on its own stream, so one group's copies overlap the
+        # others' sweeps
+        order = sorted(range(len(self.jobs)), key=lambda k: -self.jobs[k][7].nbytes)
+        groups, load = [[] for _ in range(4)], [0] * 4
+        for k in order:
+            gi = int(np.argmin(load))
+            groups[gi].append(k)
+            load[gi] += self.jobs[k][7].nbytes
+        self.e2e_groups = [(ks, MultiTapeHvp(ctx, [items[k] for k in ks], f64=False, autotune=True),
+                            torch.cuda.Stream()) for ks in groups if ks]
 
     def kernels(self):
         return [("multi-tape launch", lambda: self.multi.launch(self.sp))]
@@ -453,20 +465,23 @@ class UnevenWorkload:
                 "multi_shape": self.multi.info()}
 
     def e2e_step(self):
-        """Through the many-tape API: every tape's points and directions copied in
-        from pinned host memory, one persistent launch, gradients and HVPs copied
-        back (all on the launch stream), then a synchronise."""
+        """Through the many-tape API, pipelined: per group of tapes, on the group's
+        stream, its points and directions copied in from pinned host memory, one
+        persistent launch, its gradients and HVPs copied back; then a synchronise."""
         torch = self.torch
-        ext = torch.cuda.ExternalStream(self.sp)
-        with torch.cuda.stream(ext):
-            for _, _, _, dx, dv, _, _, hx, hv, _, _ in self.jobs:
-                dx.copy_(torch.from_numpy(hx), non_blocking=True)
-                dv.copy_(torch.from_numpy(hv), non_blocking=True)
-            self.multi.launch(self.sp)
-            for _, _, _, _, _, g, h, _, _, hg, hh in self.jobs:
-                torch.from_numpy(hg).copy_(g, non_blocking=True)
-                torch.from_numpy(hh).copy_(h, non_blocking=True)
-        ext.synchronize()
+        for ks, multi, st in self.e2e_groups:
+            with torch.cuda.stream(st):
+                for k in ks:
+                    _, _, _, dx, dv, _, _, hx, hv, _, _ = self.jobs[k]
+                    dx.copy_(torch.from_numpy(hx), non_blocking=True)
+                    dv.copy_(torch.from_numpy(hv), non_blocking=True)
+                multi.launch(st.cuda_stream)
+                for k in ks:
+                    _, _, _, _, _, g, h, _, _, hg, hh = self.jobs[k]
+                    torch.from_numpy(hg).copy_(g, non_blocking=True)
+                    torch.from_numpy(hh).copy_(h, non_blocking=True)
+        for _, _, st in self.e2e_groups:
+            st.synchronize()
 
     def io_bytes(self):
         h2d = sum(j[7].nbytes + j[8].nbytes for j in self.jobs)
