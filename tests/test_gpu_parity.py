@@ -76,7 +76,7 @@ def test_rosenbrock_grid_f32_and_f64(ctx):
 
 @pytest.mark.parametrize("B", [1, 31, 129, 1000])
 def test_rosenbrock_n100_gradient_f64(ctx, B):
-    # configs[0]: extended Rosenbrock n=100, f64; U[-2, 2]^100 from a fixed seed
+    # extended Rosenbrock n=100, f64; U[-2, 2]^100 from a fixed seed
     tape = configs.rosenbrock(100)
     o = OracleTape(tape)
     rng = np.random.default_rng(configs.SEEDS["rosenbrock"])
@@ -90,7 +90,7 @@ def test_rosenbrock_n100_gradient_f64(ctx, B):
 
 
 def test_mlp_gradient_and_hvp_f64(ctx):
-    # configs[1] tape at a reduced batch: f64 parity run
+    # the n=64 two-layer MLP tape at a reduced batch: f64 parity run
     tape = configs.mlp(64, 64)
     o = OracleTape(tape)
     rng = np.random.default_rng(configs.SEEDS["mlp"])
