@@ -490,7 +490,7 @@ template <class V, int P> struct FwdExec {
   // several L2 round trips (global slots) in flight; the additions stay in
   // term order.
   static constexpr int kWords = (int)(sizeof(V) * P / 4);
-  static constexpr int kLcGroup = kWords <= 4 ? 4 : (kWords <= 8 ? 8 : (kWords <= 16 ? 2 : 1));
+  static constexpr int kLcGroup = kWords <= 8 ? 4 : (kWords <= 16 ? 2 : 1);
   __device__ __forceinline__ bool chain_lc(Stream<32>& st, uint32_t ma, uint32_t ao, double imm, uint32_t n,
                                            V (&acc)[P]) const {
     ld(ma, ao, imm, acc);
