@@ -299,9 +299,13 @@ __device__ __forceinline__ V lc_const(uint32_t lo, uint32_t hi) {
 }
 
 // Per-kind input construction and output handling; the primary template is
-// the plain-value kind (forward, gradient).
+// the plain-value kind (forward, gradient).  `Info` is what a unit's inputs
+// depend on beyond the unit index, computed once per tile (empty for plain and
+// dual values).
 template <class T> struct Lane {
-  static __device__ __forceinline__ T make_input(const KParams& kp, uint64_t u, uint32_t i, bool valid) {
+  struct Info {};
+  static __device__ __forceinline__ Info info(const KParams&, uint64_t, bool) { return {}; }
+  static __device__ __forceinline__ T make_input(const KParams& kp, uint64_t u, const Info&, uint32_t i, bool valid) {
     if (!valid) return T(0);
     const T* x = (const T*)kp.x;
     return x[(kp.x_bcast ? 0 : u) * kp.ni + i];
@@ -311,7 +315,10 @@ template <class T> struct Lane {
   }
 };
 template <class T> struct Lane<dm::Dual<T>> {
-  static __device__ __forceinline__ dm::Dual<T> make_input(const KParams& kp, uint64_t u, uint32_t i, bool valid) {
+  struct Info {};
+  static __device__ __forceinline__ Info info(const KParams&, uint64_t, bool) { return {}; }
+  static __device__ __forceinline__ dm::Dual<T> make_input(const KParams& kp, uint64_t u, const Info&, uint32_t i,
+                                                           bool valid) {
     if (!valid) return {T(0), T(0)};
     const T* x = (const T*)kp.x;
     const T* v = (const T*)kp.v;
@@ -328,28 +335,44 @@ template <class T> struct Lane<dm::Dual<T>> {
 
 // Direction component for Taylor units; STDE units are (point = u / S, dir = u % S).
 template <class T, int K> struct Lane<dm::Jet<T, K>> {
-  static __device__ __forceinline__ T dir_component(const KParams& kp, uint64_t u, uint32_t i) {
+  // STDE units (point, direction): the point and direction index (the unit's
+  // inputs would otherwise repeat a 64-bit division per input), and in
+  // direction modes 4 / 5 the unit's coordinate or entry.  Points are < 2^32.
+  struct Info {
+    uint32_t pt, s, ent;
+  };
+  static __device__ __forceinline__ Info info(const KParams& kp, uint64_t u, bool valid) {
+    Info f{(uint32_t)u, 0u, 0u};
+    if (!valid) return f;
+    if (kp.S) {
+      const uint64_t pt = u / kp.S;
+      f.pt = (uint32_t)pt;
+      f.s = (uint32_t)(u - pt * kp.S);
+    }
+    if (kp.dir_mode == 4 || kp.dir_mode == 5) f.ent = reinterpret_cast<const uint32_t*>(kp.v)[u];
+    return f;
+  }
+  static __device__ __forceinline__ T dir_component(const KParams& kp, uint64_t u, const Info& f, uint32_t i) {
     const T* v = (const T*)kp.v;
     if (kp.S == 0 || kp.dir_mode == 0) return v[u * kp.ni + i];
-    const uint64_t pt = u / kp.S;
-    const uint32_t s = (uint32_t)(u - pt * kp.S);
-    if (kp.dir_mode == 1) return v[(uint64_t)s * kp.ni + i];
-    if (kp.dir_mode == 3) return (i == s) ? T(1) : T(0);
-    if (kp.dir_mode == 4) return (i == reinterpret_cast<const uint32_t*>(kp.v)[u]) ? T(1) : T(0);
-    return (philox_bits(kp.seed, pt, s, i) & 1u) ? T(1) : T(-1);
+    if (kp.dir_mode == 1) return v[(uint64_t)f.s * kp.ni + i];
+    if (kp.dir_mode == 3) return (i == f.s) ? T(1) : T(0);
+    if (kp.dir_mode == 4) return (i == f.ent) ? T(1) : T(0);
+    return (philox_bits(kp.seed, f.pt, f.s, i) & 1u) ? T(1) : T(-1);
   }
-  static __device__ __forceinline__ dm::Jet<T, K> make_input(const KParams& kp, uint64_t u, uint32_t i, bool valid) {
+  static __device__ __forceinline__ dm::Jet<T, K> make_input(const KParams& kp, uint64_t u, const Info& f, uint32_t i,
+                                                             bool valid) {
     dm::Jet<T, K> j;
 #pragma unroll
     for (int k = 0; k < K; ++k) j.c[k] = T(0);
     if (!valid) return j;
     const T* x = (const T*)kp.x;
-    const uint64_t xrow = kp.x_bcast ? 0 : (kp.S ? u / kp.S : u);
+    const uint64_t xrow = kp.x_bcast ? 0 : (kp.S ? (uint64_t)f.pt : u);
     j.c[0] = x[xrow * kp.ni + i];
     if (kp.dir_mode == 5) {
       // the unit's entry seeds coefficient `slot` of each of its active inputs
       // (seed_taylor_dyn_jets, src/taylor_dyn.rs); every other coefficient is 0
-      const uint32_t e = reinterpret_cast<const uint32_t*>(kp.v)[u];
+      const uint32_t e = f.ent;
       const SlotSeed* it = reinterpret_cast<const SlotSeed*>(kp.seed_items);
       for (uint32_t q = kp.seed_off[e]; q < kp.seed_off[e + 1]; ++q) {
         if (it[q].var != i) continue;
@@ -360,7 +383,7 @@ template <class T, int K> struct Lane<dm::Jet<T, K>> {
       }
       return j;
     }
-    if (K > 1) j.c[1] = dir_component(kp, u, i);
+    if (K > 1) j.c[1] = dir_component(kp, u, f, i);
     return j;
   }
   static __device__ __forceinline__ void store_output(const KParams& kp, uint64_t u, uint32_t j, const dm::Jet<T, K>& val,
@@ -401,6 +424,7 @@ template <class V, int P> struct FwdExec {
   unsigned char* tj;     // ... in the trajectory region
   uint64_t unit0;        // unit of point p = unit0 + p
   bool valid[P];
+  typename Lane<V>::Info ui[P];
 
   __device__ __forceinline__ void ld(uint32_t mode, uint32_t off, double imm, V (&v)[P]) const {
     if (mode == M_SMEM) C::ld(sm + off, v);
@@ -562,7 +586,7 @@ template <class V, int P> struct FwdExec {
     switch (opc) {
       case D_LDIN:
 #pragma unroll
-        for (int p = 0; p < P; ++p) r[p] = Lane<V>::make_input(kp, unit0 + p, (uint32_t)aux, valid[p]);
+        for (int p = 0; p < P; ++p) r[p] = Lane<V>::make_input(kp, unit0 + p, ui[p], (uint32_t)aux, valid[p]);
         put(w0.x >> 24, dof, save, r);
         return true;
       case D_STOUT:
@@ -1009,9 +1033,12 @@ __device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned
   unsigned char* tj = kp.traj_smem ? sm + (size_t)kp.smem_regs * tile * sizeof(V)
                                    : gbase + (size_t)kp.far_slots * tile * sizeof(V) + colb;
   const uint64_t unit0 = t * tile + (uint64_t)threadIdx.x * P;
-  FwdExec<V, P> fx{kp, sm, gs, tj, unit0, {}};
+  FwdExec<V, P> fx{kp, sm, gs, tj, unit0, {}, {}};
 #pragma unroll
-  for (int p = 0; p < P; ++p) fx.valid[p] = unit0 + p < kp.n_units;
+  for (int p = 0; p < P; ++p) {
+    fx.valid[p] = unit0 + p < kp.n_units;
+    fx.ui[p] = Lane<V>::info(kp, unit0 + p, fx.valid[p]);
+  }
   if (!run_program<32>(rg, reinterpret_cast<const unsigned char*>(kp.fwd), kp.n_fwd, kp.err, fx)) return false;
   if (REV) {
     RevExec<V, P> rx{kp, sm, gs, tj, unit0, {}};
