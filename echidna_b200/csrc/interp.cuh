@@ -884,10 +884,18 @@ template <class V, int P> struct RevExec {
 
   // Reverse gather (D_GATHER): for each target, its adjoint (+0 when this is
   // its first contribution) plus c * t for each contribution in order, with
-  // the zero-adjoint skip and the zero-multiplier guard, then one store.  t is
+  // the zero-adjoint skip (the zero-multiplier guard is the encoder's: it
+  // leaves zero-constant contributions out), then one store.  t is
   // a chain's adjoint after D_NORM.  Contribution loads are grouped so several
   // are in flight; the updates stay in order.
   static constexpr int kGather = kWords <= 4 ? 4 : (kWords <= 8 ? 2 : 1);
+  // c * t into cur unless t is zero (the zero-adjoint skip); gather constants
+  // are never zero (the encoder leaves zero contributions out)
+  __device__ __forceinline__ void gather_update(V (&cur)[P], const V (&t)[P], const V& c) const {
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+      if (!Kd::all_zero(t[p])) cur[p] = Kd::add(cur[p], Kd::mul(c, t[p]));
+  }
   __device__ __forceinline__ bool gather(Stream<48>& st, uint32_t ntargets) const {
 #pragma unroll 1
     for (uint32_t g = 0; g < ntargets; ++g) {
@@ -916,7 +924,7 @@ template <class V, int P> struct RevExec {
             cs[2 * k + 1] = lc_const<V>(cw.z, cw.w);
           }
 #pragma unroll
-          for (int j = 0; j < 2 * kGather; ++j) lc_update(cur, ts[j], cs[j]);
+          for (int j = 0; j < 2 * kGather; ++j) gather_update(cur, ts[j], cs[j]);
         }
       }
 #pragma unroll 1
@@ -927,11 +935,11 @@ template <class V, int P> struct RevExec {
         const uint4 aw = *reinterpret_cast<const uint4*>(r2 + 16);
         V t0[P];
         C::ld(loc(aw.z & CF_X_GLOB, aw.x), t0);
-        lc_update(cur, t0, lc_const<V>(cw.x, cw.y));
+        gather_update(cur, t0, lc_const<V>(cw.x, cw.y));
         if (q + 1 < nc) {
           V t1[P];
           C::ld(loc((aw.z >> 16) & CF_X_GLOB, aw.y), t1);
-          lc_update(cur, t1, lc_const<V>(cw.z, cw.w));
+          gather_update(cur, t1, lc_const<V>(cw.z, cw.w));
         }
       }
       C::st(px, cur);

@@ -1121,15 +1121,26 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, bool f32, DevPro
       out.rev.push_back(d);
       for (uint32_t h = 0, q = in.va; h < (uint32_t)in.aux; ++h) {
         const GRec& hd = p.gathers[q];
+        // a contribution whose constant is zero (after rounding to the value
+        // type) never changes the target: it is left out, so the kernel skips
+        // the zero-multiplier test
+        std::vector<const GRec*> kept;
+        for (uint32_t c = 0; c < hd.n; ++c) {
+          const GRec& g = p.gathers[q + 1 + c];
+          const double cv = lc_c(g.c);
+          const bool zero = f32 ? ([&] { float f; std::memcpy(&f, &cv, sizeof f); return f == 0.0f; })()
+                                : cv == 0.0;
+          if (!zero) kept.push_back(&g);
+        }
         DRTerm head{};
         head.flags = (uint16_t)(hd.flags | (hd.mode == M_GLOB ? CF_X_GLOB : 0));
         head.ax = off(hd.idx);
-        head.ay = hd.n;
+        head.ay = (uint32_t)kept.size();
         out.rev.push_back(as_record<DRIns>(head));
-        for (uint32_t c = 0; c < hd.n; c += 2) {
+        for (size_t c = 0; c < kept.size(); c += 2) {
           DRPair pr{};
-          for (uint32_t j = 0; j < 2 && c + j < hd.n; ++j) {
-            const GRec& g = p.gathers[q + 1 + c + j];
+          for (size_t j = 0; j < 2 && c + j < kept.size(); ++j) {
+            const GRec& g = *kept[c + j];
             pr.c[j] = lc_c(g.c);
             pr.ax[j] = off(g.idx);
             pr.flags[j] = g.mode == M_GLOB ? (uint16_t)CF_X_GLOB : (uint16_t)0;

@@ -86,3 +86,48 @@ def test_linear_combination_chain_bit_exact(ctx, case):
     ohg32, ohh32 = o32.hvp(X32, V32)
     assert _bits_equal(hg32.reshape(B, ni), ohg32), name
     assert _bits_equal(hh32.reshape(B, ni), ohh32), name
+
+
+@pytest.mark.parametrize("f64", [True, False])
+def test_dense_layers_with_zero_weights_bit_exact(ctx, f64):
+    # two dense layers whose reverses become gathers; a third of the weights
+    # are zero (and some round to zero in f32), so contributions are left out
+    rng = np.random.default_rng(13)
+    n, w = 6, 5
+    W1 = rng.normal(size=(w, n)) * (rng.random((w, n)) > 0.33)
+    W1[0, 0] = 1e-60  # zero once rounded to f32
+    W2 = rng.normal(size=(w, w)) * (rng.random((w, w)) > 0.33)
+
+    def f(v):
+        h = []
+        for j in range(w):
+            s = constant(0.1 * j)
+            for i in range(n):
+                s = s + constant(float(W1[j, i])) * v[i]
+            h.append(s * s)
+        out = constant(0.0)
+        for j in range(w):
+            s = constant(-0.2)
+            for i in range(w):
+                s = s + constant(float(W2[j, i])) * h[i]
+            out = out + s * s
+        return out
+    tape = record(f, [0.1] * n)[0]
+    X = rng.uniform(-1.0, 1.0, size=(300, n))
+    V = rng.choice([-1.0, 1.0], size=(300, n))
+    dt = np.float64 if f64 else np.float32
+    o = OracleTape(tape, dtype=dt)
+    gt = ctx.upload_tape_f64(tape) if f64 else ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(tape))
+    Xd, Vd = X.astype(dt), V.astype(dt)
+    if f64:
+        v, g = ctx.gradient_batch_f64(gt, Xd, 300)
+        hg, hh = ctx.hvp_batch_points_f64(gt, Xd, Vd, 300)
+    else:
+        v, g = ctx.gradient_batch(gt, Xd, 300)
+        hg, hh = ctx.hvp_batch_points(gt, Xd, Vd, 300)
+    ov, og = o.gradient(Xd)
+    ohg, ohh = o.hvp(Xd, Vd)
+    assert _bits_equal(v, ov[:, 0])
+    assert _bits_equal(g.reshape(300, n), og)
+    assert _bits_equal(hg.reshape(300, n), ohg)
+    assert _bits_equal(hh.reshape(300, n), ohh)
