@@ -13,6 +13,7 @@
 #include <map>
 #include <cmath>
 #include <memory>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <tuple>
@@ -108,6 +109,7 @@ struct ech_tape {
   struct HostProgram {
     Plan plan;
     DevProgram prog;
+    uint64_t id = 0;  // process-unique, never reused: identifies the program's bytes
   };
   std::map<std::tuple<int, int, uint32_t, uint32_t, uint32_t>, std::unique_ptr<HostProgram>> host_programs;
   // autotuned launch shapes, keyed (kind, K, log2 of the unit count)
@@ -2121,7 +2123,9 @@ ech_status prepare_gradient_host(ech_ctx* ctx, const ech_tape* tc, int f64, uint
     auto key = std::make_tuple(1, 0, c.cap, c.tile, (uint32_t)c.vbytes);
     auto it = t->host_programs.find(key);
     if (it == t->host_programs.end()) {
+      static std::atomic<uint64_t> next_id{1};
       std::unique_ptr<ech_tape::HostProgram> np(new ech_tape::HostProgram());
+      np->id = next_id.fetch_add(1);
       np->plan = build_plan(t->host, Kind::Gradient, c.cap);
       std::string err;
       if (!encode_plan(np->plan, c.tile, (uint32_t)c.vbytes, !t->f64, np->prog, err)) return fail(ECH_ERR_OTHER, err);
@@ -2136,6 +2140,7 @@ ech_status prepare_gradient_host(ech_ctx* ctx, const ech_tape* tc, int f64, uint
   out->smem = kRingBytes + (size_t)std::max<uint32_t>(hp->plan.smem_regs, 1) * c.tile * c.vbytes;
   out->plan = &hp->plan;
   out->prog = &hp->prog;
+  out->prog_id = hp->id;
   out->device = ctx->device;
   out->sm_count = ctx->sm_count;
   out->ni = t->host.ni;

@@ -24,6 +24,7 @@ struct HostSweep {
   size_t smem = 0;             // dynamic shared memory per CTA
   const Plan* plan = nullptr;
   const DevProgram* prog = nullptr;
+  uint64_t prog_id = 0;        // process-unique id of `prog` (never reused)
   int device = 0;
   int sm_count = 0;
   uint32_t ni = 0, no = 0;

@@ -343,14 +343,15 @@ ECH_API ech_status ech_mlp_create(ech_ctx* ctx, int n_in, int hidden, int n_out,
   return ECH_OK;
 }
 
-// One Adam step on a batch: x [B][n_in] and q [B][n_out] fp32 device arrays;
-// B a positive multiple of 64.  *loss_out (host) receives the batch loss.
-ECH_API ech_status ech_mlp_train_step(ech_mlp* m, const float* x, const float* q, int B, float lr, float* loss_out) {
-  if (!m || !x || !q) return set_error(ECH_ERR_INVALID_ARG, "null argument");
-  if (B <= 0 || B % 64) return set_error(ECH_ERR_INVALID_ARG, "batch must be a positive multiple of 64");
-  std::lock_guard<std::mutex> lk(m->mu);
-  CUE(cudaSetDevice(m->device));
-  cudaStream_t st = nullptr;
+}  // extern "C"
+
+namespace {
+
+// Forward with the loss and the backward pass of one batch: the parameter
+// gradients of the mean cross-entropy land in g_w1 .. g_b3 (fp32).  The
+// backward GEMMs read BF16 copies of the loss gradient and the activations,
+// as the forward GEMMs read BF16 weights; every GEMM accumulates in FP32.
+ech_status forward_backward(ech_mlp* m, const float* x, const float* q, int B, cudaStream_t st) {
   ech_status s = ensure_batch(m, B);
   if (s != ECH_OK) return s;
   const int nin = m->nin, h = m->h, nout = m->nout;
@@ -378,14 +379,61 @@ ECH_API ech_status ech_mlp_train_step(ech_mlp* m, const float* x, const float* q
   CUE(transpose(m->xb.p, m->xbT.p, B, nin, st));
   CUE(gemm(m->dz1bT.p, m->xbT.p, m->g_w1.p, nullptr, h, nin, B, B, B, nin, err, st));
   colsum_kernel<<<blocks_for(h, T), T, 0, st>>>(m->dz1.p, m->g_b1.p, B, h);
-  s = adam_all(m, lr, st);
-  if (s != ECH_OK) return s;
+  return cu(cudaGetLastError(), "backward");
+}
+
+// The batch loss into *loss_out (host) and the GEMMs' error word.
+ech_status finish_step(ech_mlp* m, float* loss_out) {
   float l = 0.0f;
   uint32_t e = 0;
   CUE(cudaMemcpy(&l, m->loss.p, sizeof l, cudaMemcpyDeviceToHost));
-  CUE(cudaMemcpy(&e, err, sizeof e, cudaMemcpyDeviceToHost));
+  CUE(cudaMemcpy(&e, m->err.p, sizeof e, cudaMemcpyDeviceToHost));
   if (e) return set_error(ECH_ERR_TIMEOUT, "device-side wait timed out in the MLP GEMM");
   if (loss_out) *loss_out = l;
+  return ECH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// One Adam step on a batch: x [B][n_in] and q [B][n_out] fp32 device arrays;
+// B a positive multiple of 64.  *loss_out (host) receives the batch loss.
+ECH_API ech_status ech_mlp_train_step(ech_mlp* m, const float* x, const float* q, int B, float lr, float* loss_out) {
+  if (!m || !x || !q) return set_error(ECH_ERR_INVALID_ARG, "null argument");
+  if (B <= 0 || B % 64) return set_error(ECH_ERR_INVALID_ARG, "batch must be a positive multiple of 64");
+  std::lock_guard<std::mutex> lk(m->mu);
+  CUE(cudaSetDevice(m->device));
+  cudaStream_t st = nullptr;
+  ech_status s = forward_backward(m, x, q, B, st);
+  if (s != ECH_OK) return s;
+  s = adam_all(m, lr, st);
+  if (s != ECH_OK) return s;
+  return finish_step(m, loss_out);
+}
+
+// The gradients one training step would apply, without applying them: the
+// same forward and backward kernels as ech_mlp_train_step, then copies of the
+// fp32 parameter gradients (host arrays of the create-time sizes; NULL skips
+// one) and the batch loss.  For checking the backward pass against a host
+// computation.
+ECH_API ech_status ech_mlp_gradients(ech_mlp* m, const float* x, const float* q, int B, float* g_w1, float* g_b1,
+                                     float* g_w2, float* g_b2, float* g_w3, float* g_b3, float* loss_out) {
+  if (!m || !x || !q) return set_error(ECH_ERR_INVALID_ARG, "null argument");
+  if (B <= 0 || B % 64) return set_error(ECH_ERR_INVALID_ARG, "batch must be a positive multiple of 64");
+  std::lock_guard<std::mutex> lk(m->mu);
+  CUE(cudaSetDevice(m->device));
+  cudaStream_t st = nullptr;
+  ech_status s = forward_backward(m, x, q, B, st);
+  if (s != ECH_OK) return s;
+  s = finish_step(m, loss_out);
+  if (s != ECH_OK) return s;
+  struct S {
+    float* h;
+    const DBuf<float>* d;
+  } o[6] = {{g_w1, &m->g_w1}, {g_b1, &m->g_b1}, {g_w2, &m->g_w2}, {g_b2, &m->g_b2}, {g_w3, &m->g_w3}, {g_b3, &m->g_b3}};
+  for (const S& e : o)
+    if (e.h) CUE(cudaMemcpy(e.h, e.d->p, e.d->n * sizeof(float), cudaMemcpyDeviceToHost));
   return ECH_OK;
 }
 

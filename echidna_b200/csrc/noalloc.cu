@@ -3,10 +3,12 @@
 //
 // Every device byte the call needs beyond the caller's own buffers comes from
 // one fixed region compiled into this library, `g_noalloc_region` below:
-//   [programs | per-CTA slot scratch]
-// The forward and reverse programs and the fused-chain term tables are copied
-// into the front of the region on the caller's stream; the rest holds the
-// per-CTA global slot files and trajectories of the sweep kernel (the same
+//   [forward program | reverse program | per-CTA slot scratch]
+// The two programs (fused-chain terms sit inline in their records) are copied
+// into the front of the region on the caller's stream when the region does not
+// already hold them: each device remembers the id of the program it last
+// received, and a call with the same program skips the copy.  The rest holds
+// the per-CTA global slot files and trajectories of the sweep kernel (the same
 // kernel the ordinary gradient entry points launch).  The grid is shrunk until
 // the CTAs' scratch fits, so batches of any size run; a tape whose program or
 // single-CTA scratch does not fit is rejected with ECH_ERR_OUT_OF_MEMORY.
@@ -16,6 +18,10 @@
 // errors are latched in the context's error word (allocated when the context
 // was created) and reported by ech_ctx_synchronize, as for the other
 // *_device entry points.
+//
+// The region's address is looked up once per device and kept for the life of
+// the process; a device reset (cudaDeviceReset) invalidates it, so the call
+// must not be used on a device after a reset.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -34,6 +40,7 @@ static __device__ __align__(256) unsigned char g_noalloc_region[kNoAllocBytes];
 
 std::mutex g_setup_mu;
 unsigned char* g_region_ptr[kMaxDevices] = {};
+uint64_t g_region_prog[kMaxDevices] = {};  // id of the program the region holds (0: none); under g_setup_mu
 
 size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
 
@@ -119,10 +126,17 @@ extern "C" ECH_API ech_status ech_gradient_batch_device_noalloc(ech_ctx* ctx, co
   if (stride > 0) grid = std::min<uint64_t>(grid, scratch_bytes / stride);
   if (grid == 0) return ECH_OK;
 
-  if (!pg.fwd.empty()) e = cudaMemcpyAsync(d_fwd, pg.fwd.data(), pg.fwd.size() * sizeof(DIns), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess && !pg.rev.empty())
-    e = cudaMemcpyAsync(d_rev, pg.rev.data(), pg.rev.size() * sizeof(DRIns), cudaMemcpyHostToDevice, st);
-  if (e != cudaSuccess) return set_error(ECH_ERR_OTHER, std::string("program copy: ") + cudaGetErrorString(e));
+  std::lock_guard<std::mutex> tag_lk(g_setup_mu);
+  if (g_region_prog[hs.device] != hs.prog_id) {
+    // the region holds another program (or none): copy this one in, stream-ordered
+    g_region_prog[hs.device] = 0;
+    if (!pg.fwd.empty())
+      e = cudaMemcpyAsync(d_fwd, pg.fwd.data(), pg.fwd.size() * sizeof(DIns), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && !pg.rev.empty())
+      e = cudaMemcpyAsync(d_rev, pg.rev.data(), pg.rev.size() * sizeof(DRIns), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return set_error(ECH_ERR_OTHER, std::string("program copy: ") + cudaGetErrorString(e));
+    g_region_prog[hs.device] = hs.prog_id;
+  }
   e = launch_sweep(hs.req, kp, (int)grid, hs.threads, hs.smem, st, &bps);
   if (e != cudaSuccess) return set_error(ECH_ERR_OTHER, std::string("kernel launch: ") + cudaGetErrorString(e));
   return ECH_OK;

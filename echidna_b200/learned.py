@@ -46,6 +46,15 @@ class ProposalMLP:
                                               ctypes.c_float(lr), ctypes.byref(loss)))
         return float(loss.value)
 
+    def gradients(self, x, q):
+        """(loss, [g_w1, g_b1, g_w2, g_b2, g_w3, g_b3]) of the mean cross-entropy on
+        device tensors x, q: the step ``train_step`` would take, not applied."""
+        grads = [np.empty(s, np.float32) for s in self.shapes]
+        loss = ctypes.c_float(0.0)
+        _check(_lib.load().ech_mlp_gradients(self._h, x.data_ptr(), q.data_ptr(), int(x.shape[0]),
+                                             *[_lib.ptr(a) for a in grads], ctypes.byref(loss)))
+        return float(loss.value), grads
+
     def probs(self, x, out=None, stream=None):
         """softmax(MLP(x)) for a device tensor x [B, n_in], on torch's current stream
         unless ``stream`` is given."""

@@ -210,7 +210,11 @@ ECH_API ech_status ech_ctx_synchronize(ech_ctx* ctx);
  * fixed device-memory budget or its own pool, or a latency-critical loop that
  * cannot take the device-wide synchronisation cudaMalloc/cudaFree may imply.
  * The first call on a device looks the region up (cudaGetSymbolAddress);
- * make it before any stream capture.  Large batches run with a smaller grid;
+ * make it before any stream capture.  The address is kept for the life of the
+ * process, so the call must not be used on a device after cudaDeviceReset.
+ * A call copies the tape's programs into the region (from pageable host
+ * memory, stream-ordered) only when the region holds a different program;
+ * repeated calls on one tape skip the copy.  Large batches run with a smaller grid;
  * a tape whose program plus one CTA's scratch exceeds the region fails with
  * ECH_ERR_OUT_OF_MEMORY.  Nothing in the region needs to start at zero.
  * Calls share the one region per device, so calls whose work overlaps in
@@ -369,6 +373,13 @@ ECH_API ech_status ech_mlp_create(ech_ctx* ctx, int n_in, int hidden, int n_out,
  * B a positive multiple of 64; synchronous; *loss_out = mean cross-entropy. */
 ECH_API ech_status ech_mlp_train_step(ech_mlp* mlp, const float* x, const float* q, int batch, float lr,
                                       float* loss_out);
+/* The parameter gradients (and loss) one ech_mlp_train_step would apply, without
+ * applying them: same forward / backward kernels, then fp32 copies into host
+ * arrays of the create-time sizes (NULL skips one).  For checking the backward
+ * pass against a host computation; synchronous. */
+ECH_API ech_status ech_mlp_gradients(ech_mlp* mlp, const float* x, const float* q, int batch, float* g_w1,
+                                     float* g_b1, float* g_w2, float* g_b2, float* g_w3, float* g_b3,
+                                     float* loss_out);
 /* probs [B][n_out] = softmax(MLP(x)), device arrays, enqueued on `stream`. */
 ECH_API ech_status ech_mlp_forward(ech_mlp* mlp, const float* x, int batch, float* probs, void* stream);
 ECH_API ech_status ech_mlp_get_weights(ech_mlp* mlp, float* w1, float* b1, float* w2, float* b2, float* w3,

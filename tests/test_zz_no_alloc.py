@@ -94,3 +94,62 @@ def test_noalloc_rejects_oversized_scratch(ctx):
                                                None)
     assert st == _lib.OUT_OF_MEMORY
     assert "no-alloc region too small" in _lib.last_error()
+
+
+def test_noalloc_rosenbrock_1024_points_bit_exact_against_oracle(ctx):
+    # extended Rosenbrock n=100, 1,024 points, f64: +, -, * only, so the sweep must
+    # equal the reference's CPU tape bit for bit; two calls in a row (the second
+    # finds the program already in the region and skips the copy)
+    from oracle.oracle import OracleTape
+    tape = configs.rosenbrock(100)
+    gt = ctx.upload_tape_f64(tape)
+    X = np.random.default_rng(configs.SEEDS["rosenbrock"]).uniform(-2.0, 2.0, size=(1024, 100))
+    ov, og = OracleTape(tape).gradient(X)
+    for _ in range(2):
+        v, g = _run(ctx, gt, True, X, 1, 100, noalloc=True)
+        np.testing.assert_array_equal(v, ov[:, 0])
+        np.testing.assert_array_equal(g.reshape(1024, 100), og)
+
+
+def test_noalloc_alternating_tapes_recopy_programs(ctx):
+    # two tapes alternating: each call must find its own program in the region
+    a = configs.rosenbrock(20)
+    b = configs.mlp(16, 16)
+    ga, gb = ctx.upload_tape_f64(a), ctx.upload_tape_f64(b)
+    rng = np.random.default_rng(12)
+    Xa, Xb = rng.uniform(-2, 2, size=(700, 20)), rng.normal(size=(500, 16))
+    ra = _run(ctx, ga, True, Xa, 1, 20, noalloc=False)
+    rb = _run(ctx, gb, True, Xb, 1, 16, noalloc=False)
+    for _ in range(2):
+        for gt, X, ni, ref in ((ga, Xa, 20, ra), (gb, Xb, 16, rb)):
+            v, g = _run(ctx, gt, True, X, 1, ni, noalloc=True)
+            np.testing.assert_array_equal(v, ref[0])
+            np.testing.assert_array_equal(g, ref[1])
+
+
+def test_noalloc_calls_leave_device_memory_unchanged(ctx):
+    # after the inputs and outputs exist, calls on a freshly uploaded tape (host
+    # lowering only) change the device's free memory by nothing
+    lib = _lib.load()
+    tape = configs.rosenbrock(60)
+    X = np.random.default_rng(13).uniform(-2.0, 2.0, size=(50_000, 60))
+    dX = torch.tensor(X, device="cuda")
+    out = torch.empty(50_000, dtype=torch.float64, device="cuda")
+    g = torch.empty(50_000 * 60, dtype=torch.float64, device="cuda")
+    # a warm-up call on another tape first: the first call in a process loads the
+    # module that holds the region and the kernel (lazy loading)
+    warm = ctx.upload_tape_f64(configs.rosenbrock(8))
+    st = lib.ech_gradient_batch_device_noalloc(ctx._h, warm._h, 1, dX.data_ptr(), 1000, out.data_ptr(),
+                                               g.data_ptr(), None)
+    assert st == _lib.OK, _lib.last_error()
+    assert lib.ech_ctx_synchronize(ctx._h) == _lib.OK, _lib.last_error()
+    torch.cuda.synchronize()
+    gt = ctx.upload_tape_f64(tape)
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        st = lib.ech_gradient_batch_device_noalloc(ctx._h, gt._h, 1, dX.data_ptr(), 50_000, out.data_ptr(),
+                                                   g.data_ptr(), None)
+        assert st == _lib.OK, _lib.last_error()
+    assert lib.ech_ctx_synchronize(ctx._h) == _lib.OK, _lib.last_error()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
