@@ -7,6 +7,7 @@ Workloads (``--workload``, default ``mlp``):
   baked in as tape constants, output 0.5*||h||^2; ~25k tape slots), 65,536 points
   x ~ N(0, I), Rademacher v.  One step = a gradient sweep and a per-point HVP sweep
   over the whole batch, FP32 (the throughput precision of that configuration).
+* ``mlp64`` — the same MLP workload in FP64 (the configuration's parity precision).
 * ``rosenbrock`` — extended Rosenbrock n=100 (bench-style recording), 1,024 points
   x ~ U[-2, 2]^100, f64; one step = one forward + gradient sweep.
 * ``stde`` — f(x) = logsumexp(tanh(W x + b)), n=256, W in R^{512x256}; 16,384
@@ -25,11 +26,15 @@ Reported per line:
 * ``value``: points/s with inputs resident in HBM (device-pointer C ABI calls),
   CUDA events on the launching stream, L2 flushed between steps (256 MiB write
   outside the timed events).
-* ``e2e``: the same step through the host-buffer C ABI: host->device copies of the
+* ``e2e``: the same step through the host-buffer C ABI with ordinary (pageable)
+  numpy arrays, as a drop-in caller passes them: host->device copies of the
   inputs and device->host copies of the results are inside the timed region.
+  ``detail.e2e_pinned_host_buffers`` repeats it with page-locked arrays.
 * ``roofline``: the dominant kernel's algorithmic bytes per launch (the
   store-all model, from the tape) over its event time, against the measured HBM
-  copy bandwidth; the scalar op rate is reported beside it.
+  copy bandwidth (``frac``); beside it the algorithmic scalar ops per launch
+  (``echidna_b200.opcost``, by value kind) against the CUDA-core pipe, and
+  ``t_roof`` = max(bytes / HBM, ops / pipe) over the measured time.
 * ``cpu_baseline``: the oracle (the reference's CPU sweeps restated in C++) on a
   bounded sample of the same workload, on all host cores.
 
@@ -77,14 +82,15 @@ class ClockSampler:
 
     def __init__(self, device: int):
         self.device = device
-        self.samples = []
+        self.samples = []       # (host time read, fields)
         self.proc = None
+        self.window = None      # (start, end) host times of the timed region
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
@@ -95,7 +101,11 @@ class ClockSampler:
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 8:
-                self.samples.append(parts)
+                self.samples.append((time.time(), parts))
+
+    def mark(self, start: float, end: float):
+        """The timed region; samples read up to 50 ms after its end belong to it."""
+        self.window = (start, end + 0.05)
 
     def __exit__(self, *exc):
         if self.proc:
@@ -109,7 +119,9 @@ class ClockSampler:
     def summary(self):
         mhz, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for s in self.samples:
+        for t, s in self.samples:
+            if self.window and not (self.window[0] <= t <= self.window[1]):
+                continue
             try:
                 mhz.append(float(s[0]))
                 mx = float(s[1])
@@ -133,74 +145,90 @@ class MlpWorkload:
     batch = 65536
     n = 64
     launches_per_step = 2
+    f64 = False
 
     def __init__(self, rank, world):
         from echidna_b200 import configs
         from echidna_b200.multi import rank_rows
         self.tape = configs.mlp(self.n, 64, dtype=np.float64)
+        self.dt = np.float64 if self.f64 else np.float32
         seed = configs.SEEDS["mlp"]
         total = world * self.batch
-        self.X = rank_rows(total, rank, world, seed, self.n, lambda g, s: g.normal(size=s)).astype(np.float32)
+        self.X = rank_rows(total, rank, world, seed, self.n, lambda g, s: g.normal(size=s)).astype(self.dt)
         self.V = rank_rows(total, rank, world, seed + 1, self.n,
-                           lambda g, s: g.choice([-1.0, 1.0], size=s)).astype(np.float32)
+                           lambda g, s: g.choice([-1.0, 1.0], size=s)).astype(self.dt)
 
     def describe(self):
         return {"workload": "mlp n=64 width=64 (~25k-slot tape): gradient + per-point HVP, Rademacher v",
-                "batch_per_gpu": self.batch}, "f32"
+                "batch_per_gpu": self.batch}, "f64" if self.f64 else "f32"
 
     def setup(self, ctx, lib, torch, sp):
         from echidna_b200.gpu import GpuTapeData
         self.ctx, self.lib, self.sp = ctx, lib, sp
-        self.gt = ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(self.tape))
+        self.gt = ctx.upload_tape_f64(self.tape) if self.f64 else ctx.upload_tape(
+            GpuTapeData.from_tape_f64_lossy(self.tape))
         B, n = self.batch, self.n
+        tdt = torch.float64 if self.f64 else torch.float32
         self.dX = torch.from_numpy(self.X).cuda()
         self.dV = torch.from_numpy(self.V).cuda()
-        self.d_out = torch.empty(B, device="cuda")
-        self.d_g = torch.empty(B * n, device="cuda")
-        self.d_g2 = torch.empty(B * n, device="cuda")
-        self.d_h = torch.empty(B * n, device="cuda")
+        self.d_out = torch.empty(B, dtype=tdt, device="cuda")
+        self.d_g = torch.empty(B * n, dtype=tdt, device="cuda")
+        self.d_g2 = torch.empty(B * n, dtype=tdt, device="cuda")
+        self.d_h = torch.empty(B * n, dtype=tdt, device="cuda")
+        # end to end with ordinary (pageable) numpy arrays, as a drop-in caller passes
+        # them; the pinned copies give the figure for callers that pin their buffers
+        self.pX, self.pV = self.X.copy(), self.V.copy()
+        self.po, self.pg = np.empty(B, self.dt), np.empty(B * n, self.dt)
+        self.pg2, self.ph = np.empty(B * n, self.dt), np.empty(B * n, self.dt)
         self.hX, self.hV = _pinned(torch, self.X), _pinned(torch, self.V)
-        self.ho = _pinned(torch, np.empty(B, np.float32))
-        self.hg = _pinned(torch, np.empty(B * n, np.float32))
-        self.hg2 = _pinned(torch, np.empty(B * n, np.float32))
-        self.hh = _pinned(torch, np.empty(B * n, np.float32))
+        self.ho = _pinned(torch, np.empty(B, self.dt))
+        self.hg = _pinned(torch, np.empty(B * n, self.dt))
+        self.hg2 = _pinned(torch, np.empty(B * n, self.dt))
+        self.hh = _pinned(torch, np.empty(B * n, self.dt))
 
     def kernels(self):
         from echidna_b200 import _lib
-        lib, ctx, gt, sp = self.lib, self.ctx, self.gt, self.sp
+        lib, ctx, gt, sp, f64 = self.lib, self.ctx, self.gt, self.sp, int(self.f64)
 
         def grad():
-            st = lib.ech_gradient_batch_device(ctx._h, gt._h, 0, self.dX.data_ptr(), self.batch,
+            st = lib.ech_gradient_batch_device(ctx._h, gt._h, f64, self.dX.data_ptr(), self.batch,
                                                self.d_out.data_ptr(), self.d_g.data_ptr(), sp)
             assert st == 0, _lib.last_error()
 
         def hvp():
-            st = lib.ech_hvp_batch_device(ctx._h, gt._h, 0, self.dX.data_ptr(), 1, self.dV.data_ptr(), self.batch,
+            st = lib.ech_hvp_batch_device(ctx._h, gt._h, f64, self.dX.data_ptr(), 1, self.dV.data_ptr(), self.batch,
                                           self.d_g2.data_ptr(), self.d_h.data_ptr(), sp)
             assert st == 0, _lib.last_error()
         return [("gradient sweep", grad), ("hvp sweep", hvp)]
 
-    def e2e_step(self):
+    def _e2e(self, X, V, o, g, g2, h):
         from echidna_b200 import _lib
         lib, ctx, gt, P, B = self.lib, self.ctx, self.gt, _lib.ptr, self.batch
-        st = lib.ech_gradient_batch_f32(ctx._h, gt._h, P(self.hX), self.hX.size, B, P(self.ho), self.ho.size,
-                                        P(self.hg), self.hg.size)
+        sfx = "f64" if self.f64 else "f32"
+        st = getattr(lib, f"ech_gradient_batch_{sfx}")(ctx._h, gt._h, P(X), X.size, B, P(o), o.size, P(g), g.size)
         assert st == 0, _lib.last_error()
-        st = lib.ech_hvp_batch_points_f32(ctx._h, gt._h, P(self.hX), self.hX.size, P(self.hV), self.hV.size, B,
-                                          P(self.hg2), self.hg2.size, P(self.hh), self.hh.size)
+        st = getattr(lib, f"ech_hvp_batch_points_{sfx}")(ctx._h, gt._h, P(X), X.size, P(V), V.size, B, P(g2),
+                                                           g2.size, P(h), h.size)
         assert st == 0, _lib.last_error()
+
+    def e2e_step(self):
+        self._e2e(self.pX, self.pV, self.po, self.pg, self.pg2, self.ph)
+
+    def e2e_step_pinned(self):
+        self._e2e(self.hX, self.hV, self.ho, self.hg, self.hg2, self.hh)
 
     def io_bytes(self):
         return (int(self.hX.nbytes * 2 + self.hV.nbytes),
                 int(self.ho.nbytes + self.hg.nbytes + self.hg2.nbytes + self.hh.nbytes))
 
     def roofline_inputs(self, kernel):
-        s, ni, no, B = 4, self.n, 1, self.batch
+        from echidna_b200 import opcost
+        s, ni, no, B = (8 if self.f64 else 4), self.n, 1, self.batch
         if kernel == "gradient sweep":
             st = self.ctx.plan_stats(self.gt, "gradient")
-            return B * (s * (2 * ni + no) + 2 * s * st["traj_values"]), B * (st["flops_fwd"] + st["flops_rev"])
+            return B * (s * (2 * ni + no) + 2 * s * st["traj_values"]), B * opcost.sweep_cost(self.tape, "gradient")[0]
         st = self.ctx.plan_stats(self.gt, "hvp")
-        return B * (s * (4 * ni + no) + 2 * s * 2 * st["traj_values"]), B * 4 * (st["flops_fwd"] + st["flops_rev"])
+        return B * (s * (4 * ni + no) + 2 * s * 2 * st["traj_values"]), B * opcost.sweep_cost(self.tape, "hvp")[0]
 
     def detail(self):
         return {"plan_gradient": self.ctx.plan_stats(self.gt, "gradient"),
@@ -208,10 +236,10 @@ class MlpWorkload:
                 "shape_gradient": self.ctx.launch_shape(self.gt, "gradient", self.batch),
                 "shape_hvp": self.ctx.launch_shape(self.gt, "hvp", self.batch)}
 
-    def cpu_reference(self, budget_s, nthreads):
+    def cpu_reference(self, budget_s, nthreads, dtype=np.float64):
         from oracle.oracle import OracleTape
-        o = OracleTape(self.tape)
-        Xd, Vd = self.X.astype(np.float64), self.V.astype(np.float64)
+        o = OracleTape(self.tape, dtype=dtype)
+        Xd, Vd = self.X.astype(dtype), self.V.astype(dtype)
         n = 64
         t0 = time.perf_counter()
         o.gradient(Xd[:n], nthreads)
@@ -222,7 +250,14 @@ class MlpWorkload:
         o.gradient(Xd[:n], nthreads)
         o.hvp(Xd[:n], Vd[:n], nthreads)
         dt = time.perf_counter() - t0
-        return n / dt, f"{n} points of the batch: oracle gradient + per-point HVP (f64), {dt:.1f} s"
+        prec = "f64" if dtype == np.float64 else "f32"
+        return n / dt, f"{n} points of the batch: oracle gradient + per-point HVP ({prec}), {dt:.1f} s"
+
+
+class Mlp64Workload(MlpWorkload):
+    """The same MLP workload in FP64 (the configuration's parity precision)."""
+    name = "mlp64"
+    f64 = True
 
 
 class RosenbrockWorkload:
@@ -249,6 +284,7 @@ class RosenbrockWorkload:
         self.dX = torch.from_numpy(self.X).cuda()
         self.d_out = torch.empty(B, dtype=torch.float64, device="cuda")
         self.d_g = torch.empty(B * n, dtype=torch.float64, device="cuda")
+        self.pX, self.po, self.pg = self.X.copy(), np.empty(B), np.empty(B * n)
         self.hX = _pinned(torch, self.X)
         self.ho = _pinned(torch, np.empty(B))
         self.hg = _pinned(torch, np.empty(B * n))
@@ -262,20 +298,27 @@ class RosenbrockWorkload:
             assert st == 0, _lib.last_error()
         return [("gradient sweep", grad)]
 
-    def e2e_step(self):
+    def _e2e(self, X, o, g):
         from echidna_b200 import _lib
         P = _lib.ptr
-        st = self.lib.ech_gradient_batch_f64(self.ctx._h, self.gt._h, P(self.hX), self.hX.size, self.batch,
-                                             P(self.ho), self.ho.size, P(self.hg), self.hg.size)
+        st = self.lib.ech_gradient_batch_f64(self.ctx._h, self.gt._h, P(X), X.size, self.batch, P(o), o.size, P(g),
+                                             g.size)
         assert st == 0, _lib.last_error()
+
+    def e2e_step(self):
+        self._e2e(self.pX, self.po, self.pg)
+
+    def e2e_step_pinned(self):
+        self._e2e(self.hX, self.ho, self.hg)
 
     def io_bytes(self):
         return int(self.hX.nbytes), int(self.ho.nbytes + self.hg.nbytes)
 
     def roofline_inputs(self, kernel):
+        from echidna_b200 import opcost
         st = self.ctx.plan_stats(self.gt, "gradient")
         s, B = 8, self.batch
-        return B * (s * (2 * self.n + 1) + 2 * s * st["traj_values"]), B * (st["flops_fwd"] + st["flops_rev"])
+        return B * (s * (2 * self.n + 1) + 2 * s * st["traj_values"]), B * opcost.sweep_cost(self.tape, "gradient")[0]
 
     def detail(self):
         return {"plan_gradient": self.ctx.plan_stats(self.gt, "gradient"),
@@ -321,6 +364,7 @@ class StdeWorkload:
         self.gt = ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(self.tape))
         self.dX = torch.from_numpy(self.X).cuda()
         self.d_res = torch.empty(self.batch * 5, dtype=torch.float64, device="cuda")
+        self.pX = self.X.copy()
         self.hX = _pinned(torch, self.X)
         self.h_res = (_lib.EstimatorResultC * self.batch)()
 
@@ -333,25 +377,78 @@ class StdeWorkload:
             assert st == 0, _lib.last_error()
         return [("taylor-3 sweep + reduction", lap)]
 
-    def e2e_step(self):
+    def _e2e(self, X):
         from echidna_b200 import _lib
-        st = self.lib.ech_laplacian_batch_f32(self.ctx._h, self.gt._h, _lib.ptr(self.hX), self.hX.size, self.batch,
+        st = self.lib.ech_laplacian_batch_f32(self.ctx._h, self.gt._h, _lib.ptr(X), X.size, self.batch,
                                               None, 0, self.S, 2, self.seed, self.h_res)
         assert st == 0, _lib.last_error()
+
+    def e2e_step(self):
+        self._e2e(self.pX)
+
+    def e2e_step_pinned(self):
+        self._e2e(self.hX)
 
     def io_bytes(self):
         return int(self.hX.nbytes), int(self.batch * 40)
 
     def roofline_inputs(self, kernel):
-        st = self.ctx.plan_stats(self.gt, "taylor", 3)
+        from echidna_b200 import opcost
         s, K = 4, 3
         units = self.batch * self.S
         # per unit: x amortised over the S directions, no direction bytes (device RNG), K coefficients out
-        return int(units * s * (self.n / self.S + K)), units * st["flops_fwd"]
+        return int(units * s * (self.n / self.S + K)), units * opcost.sweep_cost(self.tape, "taylor", K)[0]
 
     def detail(self):
         return {"plan_taylor3": self.ctx.plan_stats(self.gt, "taylor", 3),
+                "plan_taylor3_input_direct": self.ctx.plan_stats(self.gt, "taylor_direct", 3),
                 "shape_taylor3": self.ctx.launch_shape(self.gt, "taylor", self.batch * self.S, 3)}
+
+    accuracy_points = 256
+
+    def extra(self, torch, stream, flush, steps):
+        """Accuracy on a 256-point subset of the batch: the FP32 estimates against the
+        exact Hessian trace of the oracle's dense tape Hessian (FP64), as relative
+        error and z-score; and each FP32 option against the FP64 sweep with the same
+        device directions (an FP64 GPU run, parity-tested against the oracle)."""
+        import concurrent.futures as cf
+        from echidna_b200 import stde_gpu
+        from oracle.oracle import OracleTape
+        k = self.accuracy_points
+        X = self.X[:k]
+        o = OracleTape(self.tape)
+        t0 = time.perf_counter()
+        with cf.ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+            traces = np.array(list(ex.map(lambda x: float(np.trace(o.hessian(x.astype(np.float64))[2])), X)))
+        t_oracle = time.perf_counter() - t0
+        g64 = self.ctx.upload_tape_f64(self.tape)
+        ref = stde_gpu.laplacian_batch(self.ctx, g64, X.astype(np.float64), self.S, None,
+                                       stde_gpu.DIR_RADEMACHER, seed=self.seed)["estimate"]
+        modes = {"fp32 jets, fp64 welford (default)": 0,
+                 "fp32 jets, fp32 welford": self.ctx.FP32_PLAIN_MEANS,
+                 "fp32 jets, compensated fp32 means": self.ctx.FP32_COMPENSATED_MEANS,
+                 "compensated fp32 jets and means": self.ctx.FP32_COMPENSATED_JETS | self.ctx.FP32_COMPENSATED_MEANS}
+        out = {}
+        for name, flags in modes.items():
+            self.ctx.set_fp32_mode(flags)
+            r = stde_gpu.laplacian_batch(self.ctx, self.gt, X, self.S, None, stde_gpu.DIR_RADEMACHER, seed=self.seed)
+            rel64 = np.abs(r["estimate"] - ref) / np.abs(ref)
+            entry = {"vs_fp64_sweep_rel_err_median": float(np.median(rel64)), "vs_fp64_sweep_rel_err_max":
+                     float(np.max(rel64))}
+            if flags == 0:
+                z = (r["estimate"] - traces) / r["standard_error"]
+                rel = np.abs(r["estimate"] - traces) / np.abs(traces)
+                entry.update({"vs_exact_trace_rel_err_median": float(np.median(rel)),
+                              "vs_exact_trace_rel_err_max": float(np.max(rel)),
+                              "z_abs_max": float(np.max(np.abs(z))), "z_mean": float(np.mean(z)),
+                              "z_std": float(np.std(z))})
+            out[name] = entry
+        self.ctx.set_fp32_mode(0)
+        rel64 = np.abs(ref - traces) / np.abs(traces)
+        return {"accuracy_256_points": {"exact_trace": "trace of the oracle's dense tape Hessian (FP64), "
+                                                       f"{t_oracle:.1f} s on the host",
+                                        "fp64_sweep_vs_exact_trace_rel_err_median": float(np.median(rel64)),
+                                        **out}}
 
     def cpu_reference(self, budget_s, nthreads):
         from oracle.oracle import OracleTape
@@ -489,12 +586,13 @@ class UnevenWorkload:
         return int(h2d), int(d2h)
 
     def roofline_inputs(self, kernel):
+        from echidna_b200 import opcost
         s, total_b, total_f = 4, 0, 0
         for tape, gt, n, *_ in self.jobs:
             st = self.ctx.plan_stats(gt, "hvp")
             ni = tape.num_inputs
             total_b += n * (s * (4 * ni + 1) + 2 * s * 2 * st["traj_values"])
-            total_f += n * 4 * (st["flops_fwd"] + st["flops_rev"])
+            total_f += n * opcost.sweep_cost(tape, "hvp")[0]
         return total_b, total_f
 
     def detail(self):
@@ -651,9 +749,9 @@ class LearnedWorkload:
         return int(self.hX.nbytes), int(self.batch * 40)
 
     def roofline_inputs(self, kernel):
-        st = self.ctx.plan_stats(self.g32, "taylor", 3)
+        from echidna_b200 import opcost
         units = self.batch * self.S
-        return int(units * 4 * (self.n / self.S + 3)), units * st["flops_fwd"]
+        return int(units * 4 * (self.n / self.S + 3)), units * opcost.sweep_cost(self.tape, "taylor", 3)[0]
 
     def detail(self):
         return {"plan_taylor3": self.ctx.plan_stats(self.g32, "taylor", 3)}
@@ -671,7 +769,7 @@ class LearnedWorkload:
         return pts / dt, f"{pts} points x {self.S} uniform samples: oracle diagonal_kth_order_stochastic (k=2, f64, 1 thread), {dt:.1f} s"
 
 
-WORKLOADS = {"mlp": MlpWorkload, "rosenbrock": RosenbrockWorkload, "stde": StdeWorkload, "uneven": UnevenWorkload,
+WORKLOADS = {"mlp": MlpWorkload, "mlp64": Mlp64Workload, "rosenbrock": RosenbrockWorkload, "stde": StdeWorkload, "uneven": UnevenWorkload,
              "learned": LearnedWorkload}
 
 
@@ -691,7 +789,11 @@ def run_reference(args):
         v, sample = wl.cpu_reference(3.0, nth)
         vals.append(v)
     value = float(np.median(vals))
-    cfg, _ = wl.describe()
+    cfg, dtype = wl.describe()
+    detail = {}
+    if dtype == "f32" and "dtype" in wl.cpu_reference.__code__.co_varnames:
+        v32, s32 = wl.cpu_reference(3.0, nth, dtype=np.float32)
+        detail["same_precision_f32"] = {"value": v32, "unit": UNIT, "sample": s32}
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
@@ -699,6 +801,8 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if detail:
+        line["detail"] = detail
     print(json.dumps(line), flush=True)
     return 0
 
@@ -711,6 +815,9 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default="mlp", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-one-step", action="store_true",
+                    help="after the warm-up, run one step between cudaProfilerStart/Stop and exit "
+                         "(for ncu --profile-from-start off); prints no JSON line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -743,11 +850,24 @@ def main():
     kernels = wl.kernels()
     flush = torch.empty(L2_FLUSH_BYTES // 4, device="cuda")
 
+    clk = ClockSampler(local).__enter__()  # sampling from the warm-up on; only the timed region is kept
     for _ in range(args.warmup):
         for _, k in kernels:
             k()
     torch.cuda.synchronize()
     assert lib.ech_ctx_synchronize(ctx._h) == 0, _lib.last_error()
+    if args.profile_one_step:
+        clk.__exit__(None, None, None)
+        torch.cuda.cudart().cudaProfilerStart()
+        for _, k in kernels:
+            k()
+        torch.cuda.synchronize()
+        assert lib.ech_ctx_synchronize(ctx._h) == 0, _lib.last_error()
+        torch.cuda.cudart().cudaProfilerStop()
+        print(f"profiled one step of {args.workload}: " + ", ".join(name for name, _ in kernels), flush=True)
+        del kernels, wl
+        ctx.close()
+        return 0
 
     def barrier():
         if world > 1:
@@ -757,18 +877,21 @@ def main():
     # device-resident timing, per kernel, L2 flushed between steps
     times = {name: [] for name, _ in kernels}
     barrier()
-    with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            flush.zero_()
-            ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(kernels) + 1)]
-            ev[0].record(stream)
-            for i, (_, k) in enumerate(kernels):
-                k()
-                ev[i + 1].record(stream)
-            ev[-1].synchronize()
-            for i, (name, _) in enumerate(kernels):
-                times[name].append(ev[i].elapsed_time(ev[i + 1]))
-        barrier()
+    t_start = time.time()
+    for _ in range(args.steps):
+        flush.zero_()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(kernels) + 1)]
+        ev[0].record(stream)
+        for i, (_, k) in enumerate(kernels):
+            k()
+            ev[i + 1].record(stream)
+        ev[-1].synchronize()
+        for i, (name, _) in enumerate(kernels):
+            times[name].append(ev[i].elapsed_time(ev[i + 1]))
+    barrier()
+    clk.mark(t_start, time.time())
+    time.sleep(0.1)
+    clk.__exit__(None, None, None)
     assert lib.ech_ctx_synchronize(ctx._h) == 0, _lib.last_error()
     step_ms = float(sum(np.sum(v) for v in times.values())) / args.steps
     if world > 1:
@@ -776,19 +899,24 @@ def main():
 
     extra = wl.extra(torch, stream, flush, args.steps) if hasattr(wl, "extra") else {}
 
-    # end-to-end through the host-buffer ABI (pinned host buffers)
-    wl.e2e_step()
-    barrier()
-    e2e_ms = []
-    for _ in range(max(3, args.steps // 2)):
-        flush.zero_()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        wl.e2e_step()
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e_step_ms = float(np.median(e2e_ms))
-    if world > 1:
-        e2e_step_ms = max_over_ranks(e2e_step_ms, "cuda")
+    # end-to-end through the host-buffer ABI: ordinary (pageable) host arrays, as a
+    # drop-in caller passes them; with pinned arrays beside it where the workload has both
+    def e2e_time(step):
+        step()
+        barrier()
+        ts = []
+        for _ in range(max(3, args.steps // 2)):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            step()
+            ts.append((time.perf_counter() - t0) * 1e3)
+        ms = float(np.median(ts))
+        return max_over_ranks(ms, "cuda") if world > 1 else ms
+    e2e_step_ms = e2e_time(wl.e2e_step)
+    if hasattr(wl, "e2e_step_pinned"):
+        pinned_ms = e2e_time(wl.e2e_step_pinned)
+        extra["e2e_pinned_host_buffers"] = {"value": world * wl.batch / (pinned_ms * 1e-3), "unit": UNIT}
 
     # roofline of the dominant kernel
     mean_ms = {name: float(np.mean(v)) for name, v in times.items()}
@@ -797,15 +925,19 @@ def main():
     peak, peak_kind = _peaks()
     dom_ms = mean_ms[dom]
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
-    # the interpreted sweeps are issue / latency bound: the scalar pipe is the
-    # compute roof (each +, -, *, / and libm call counted once; -fmad=false)
+    # compute roof: the CUDA-core pipe, one scalar op per lane per clock (the sweeps
+    # round each + and * separately, -fmad=false); flops per unit by value kind
+    # (echidna_b200.opcost), libm calls not counted
+    from echidna_b200 import opcost
     sm_mhz = 1965.0
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             sm_mhz = float(json.load(f).get("sm_max_mhz", sm_mhz))
     except OSError:
         pass
-    pipe_peak = 148 * 128 * sm_mhz * 1e6 / 1e12 * (0.5 if wl.describe()[1] == "f64" else 1.0)
+    pipe_ops = opcost.pipe_peak_ops(wl.describe()[1] == "f64", sm_mhz)
+    pipe_peak = pipe_ops / 1e12
+    combined = opcost.roofline(dom_bytes, dom_ops, dom_ms * 1e-3, peak, pipe_ops)
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
@@ -827,7 +959,8 @@ def main():
                      "scalar_ops_per_launch": dom_ops, "scalar_tops": dom_ops / (dom_ms * 1e-3) / 1e12,
                      "scalar_pipe_peak_tops": pipe_peak, "scalar_pipe_frac": dom_ops / (dom_ms * 1e-3) / 1e12 / pipe_peak,
                      "scalar_pipe_peak_source": "nominal: 148 SMs x 128 FP32 lanes x max SM clock "
-                                                "(FP64: x 1/2); one op per lane per clock, no FMA"},
+                                                "(FP64: x 1/2); one op per lane per clock, no FMA",
+                     "t_roof": combined},
         "e2e": {"value": world * wl.batch / (e2e_step_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "clocks": clk.summary(),
@@ -837,6 +970,10 @@ def main():
         nth = os.cpu_count() or 1
         v, sample = wl.cpu_reference(10.0, nth)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample}
+        if dtype == "f32" and "dtype" in wl.cpu_reference.__code__.co_varnames:
+            # the same CPU path in FP32, so the FP32 GPU figure has a same-precision CPU number beside it
+            v32, sample32 = wl.cpu_reference(5.0, nth, dtype=np.float32)
+            line["cpu_baseline"]["same_precision_f32"] = {"value": v32, "sample": sample32}
     if rank == 0:
         print(json.dumps(line), flush=True)
     del kernels, wl

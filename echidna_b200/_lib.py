@@ -95,6 +95,7 @@ _SIGS = {
     "ech_mlp_train_step": ([_P, _P, _P, _I, ctypes.c_float, _P], _I),
     "ech_mlp_forward": ([_P, _P, _I, _P, _P], _I),
     "ech_mlp_gradients": ([_P, _P, _P, _I, _P, _P, _P, _P, _P, _P, _P], _I),
+    "ech_ctx_set_fp32_mode": ([_P, _U32], _I),
     "ech_mlp_get_weights": ([_P, _P, _P, _P, _P, _P, _P], _I),
     "ech_mlp_destroy": ([_P], None),
     "ech_multi_create": ([_P, _I, _P, _U32, _I, _P], _I),
@@ -118,7 +119,7 @@ _SIGS = {
     "ech_gradient_batch_device_noalloc": ([_P, _P, _I, _P, _U32, _P, _P, _P], _I),
     "ech_tape_plan_stats": ([_P, _P, _I, _U32, _I, ctypes.POINTER(_U64)], _I),
     "ech_plan_dump": ([_P, _P, _P, _P, _U32, _U32, _U32, _P, _U32, _I, _U32, _P, _SZ, _P, _SZ, _P, _SZ, _P, _SZ,
-                       _P, _SZ, ctypes.POINTER(_U64)], _I),
+                       _P, _SZ, _P, _SZ, _U32, ctypes.POINTER(_U64)], _I),
 }
 
 

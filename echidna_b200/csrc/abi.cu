@@ -16,6 +16,7 @@
 #include <atomic>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -62,6 +63,20 @@ struct DevBuf {
   }
 };
 
+// Page-locked host staging memory (cudaHostAlloc), grown on demand.
+struct PinnedBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~PinnedBuf() { if (p) cudaFreeHost(p); }
+  cudaError_t ensure(size_t n) {
+    if (n <= bytes) return cudaSuccess;
+    if (p) { cudaFreeHost(p); p = nullptr; bytes = 0; }
+    cudaError_t e = cudaHostAlloc(&p, n, cudaHostAllocDefault);
+    if (e == cudaSuccess) bytes = n;
+    return e;
+  }
+};
+
 struct DevPlan {
   Plan host;
   DIns* d_fwd = nullptr;
@@ -88,9 +103,12 @@ struct ech_ctx {
   cudaStream_t pipe[kPipe] = {};
   cudaEvent_t pipe_ev = nullptr;
   DevBuf pipe_scratch[kPipe];
+  PinnedBuf pipe_stage[kPipe];   // staging for chunks of pageable host arrays
   uint32_t* d_err = nullptr;
   // launch overrides (0 = automatic)
   uint32_t ov_threads = 0, ov_ppt = 0, ov_cap = 0;
+  // ECH_FP32_* options of the FP32 batch STDE calls (0: reference rounding, FP64 reduction)
+  uint32_t fp32_mode = 0;
 };
 
 // Launch shape: block size, points per thread, and how many CTAs should share
@@ -104,14 +122,14 @@ struct ech_tape {
   bool f64 = true;
   HostTape host;
   std::mutex mu;
-  std::map<std::tuple<int, int, uint32_t, uint32_t, uint32_t>, std::unique_ptr<DevPlan>> plans;  // (kind, K, cap, tile, vbytes)
+  std::map<std::tuple<int, int, uint32_t, uint32_t, uint32_t, uint32_t>, std::unique_ptr<DevPlan>> plans;  // (kind, K, cap, tile, vbytes, P)
   // host-encoded programs for entry points that place them in their own memory
   struct HostProgram {
     Plan plan;
     DevProgram prog;
     uint64_t id = 0;  // process-unique, never reused: identifies the program's bytes
   };
-  std::map<std::tuple<int, int, uint32_t, uint32_t, uint32_t>, std::unique_ptr<HostProgram>> host_programs;
+  std::map<std::tuple<int, int, uint32_t, uint32_t, uint32_t, uint32_t>, std::unique_ptr<HostProgram>> host_programs;
   // autotuned launch shapes, keyed (kind, K, log2 of the unit count)
   std::map<std::tuple<int, int, int>, Shape> shapes;
   // for a step map x -> step(x): the tape of sum_j w_j step(x)_j over inputs (x, w)
@@ -164,6 +182,17 @@ extern "C" ECH_API ech_status ech_ctx_set_launch(ech_ctx* ctx, uint32_t threads,
   ctx->ov_threads = threads;
   ctx->ov_ppt = ppt;
   ctx->ov_cap = cap;
+  return ECH_OK;
+}
+
+extern "C" ECH_API ech_status ech_ctx_set_fp32_mode(ech_ctx* ctx, uint32_t flags) {
+  if (!ctx) return fail(ECH_ERR_INVALID_ARG, "ctx is null");
+  if (flags & ~(uint32_t)(ECH_FP32_COMPENSATED_JETS | ECH_FP32_COMPENSATED_MEANS | ECH_FP32_PLAIN_MEANS))
+    return fail(ECH_ERR_INVALID_ARG, "unknown FP32 mode flag");
+  if ((flags & ECH_FP32_COMPENSATED_MEANS) && (flags & ECH_FP32_PLAIN_MEANS))
+    return fail(ECH_ERR_INVALID_ARG, "ECH_FP32_COMPENSATED_MEANS and ECH_FP32_PLAIN_MEANS exclude each other");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->fp32_mode = flags;
   return ECH_OK;
 }
 
@@ -280,6 +309,7 @@ static Kind kind_of(int k) {
     case 1: return Kind::Gradient;
     case 2: return Kind::Hvp;
     case 3: return Kind::Jvp;
+    case 5: return Kind::TaylorDirect;
     default: return Kind::Taylor;
   }
 }
@@ -319,16 +349,17 @@ static LaunchCfg choose_cfg(ech_ctx* ctx, const ech_tape* t, int kind, int K) {
   return cfg_for(ctx, t, kind, K, sh);
 }
 
-static ech_status get_plan(ech_tape* t, int kind, int K, uint32_t cap, uint32_t tile, uint32_t vbytes, DevPlan** out) {
+static ech_status get_plan(ech_tape* t, int kind, int K, uint32_t cap, uint32_t tile, uint32_t vbytes, uint32_t P,
+                           DevPlan** out) {
   std::lock_guard<std::mutex> lk(t->mu);
-  auto key = std::make_tuple(kind, K, cap, tile, vbytes);
+  auto key = std::make_tuple(kind, K, cap, tile, vbytes, P);
   auto it = t->plans.find(key);
   if (it != t->plans.end()) {
     *out = it->second.get();
     return ECH_OK;
   }
   std::unique_ptr<DevPlan> dp(new DevPlan());
-  dp->host = build_plan(t->host, kind_of(kind), cap);
+  dp->host = build_plan(t->host, kind_of(kind), cap, dense_group_max(vbytes, P));
   DevProgram prog;
   std::string err;
   if (!encode_plan(dp->host, tile, vbytes, !t->f64, prog, err)) return fail(ECH_ERR_OTHER, err);
@@ -358,17 +389,37 @@ struct SweepIO {
   uint64_t seed = 0;
   const uint32_t* seed_off = nullptr;  // dir_mode 5
   const void* seed_items = nullptr;
+  int compensated = 0;                 // jets: compensated sums in linear chains (FP32 batch STDE option)
 };
+
+// Point-direction jet launches whose directions the kernel can evaluate per
+// input (shared host directions, device Rademacher signs, basis vectors) run
+// the input-direct program (Kind::TaylorDirect, plan kind 5): linear
+// combinations of inputs read each input jet at its source instead of from a
+// slot.  Device Rademacher signs are drawn once per tile into shared memory,
+// ceil(ni/32) words per unit, taken from the shared-register budget.
+static bool input_direct(int kind, const SweepIO& io) {
+  return kind == 4 && io.S > 0 && io.dir_mode >= 1 && io.dir_mode <= 4;
+}
 
 static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n_units, const SweepIO& io,
                              cudaStream_t st, LaunchCfg c, DevBuf* scratch = nullptr) {
   if (!scratch) scratch = &ctx->scratch;
+  const bool direct = input_direct(kind, io);
+  const size_t bits_bytes = (direct && io.dir_mode == 2) ? (size_t)((t->host.ni + 31) / 32) * c.tile * 4 : 0;
+  if (bits_bytes) {
+    const uint32_t reserve = (uint32_t)((bits_bytes + (size_t)c.tile * c.vbytes - 1) / ((size_t)c.tile * c.vbytes));
+    c.cap = c.cap > reserve ? c.cap - reserve : 1;
+  }
   DevPlan* dp = nullptr;
-  ech_status s = get_plan(t, kind, K, c.cap, c.tile, (uint32_t)c.vbytes, &dp);
+  ech_status s = get_plan(t, direct ? 5 : kind, K, c.cap, c.tile, (uint32_t)c.vbytes, (uint32_t)c.req.P, &dp);
   if (s != ECH_OK) return s;
   const Plan& p = dp->host;
   const uint32_t regs = std::max<uint32_t>(p.smem_regs, 1);
   c.smem = kRingBytes + (size_t)regs * c.tile * c.vbytes;
+  const uint32_t dir_bits = bits_bytes ? (uint32_t)c.smem : 0u;
+  c.smem += bits_bytes;
+  if (c.smem > ctx->smem_optin) return fail(ECH_ERR_OTHER, "tape live set does not fit the shared-memory slot file");
   // the trajectory goes to shared memory when it fits the shape's share beside
   // the registers (narrow CTAs on small batches): the reverse then reads it at
   // shared-memory latency
@@ -399,6 +450,8 @@ static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_
   kp.seed = io.seed;
   kp.seed_off = io.seed_off;
   kp.seed_items = io.seed_items;
+  kp.dir_bits = dir_bits;
+  kp.compensated = (uint32_t)io.compensated;
   int bps = 0;
   cudaError_t e = launch_sweep(c.req, kp, 0, c.threads, c.smem, st, &bps);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
@@ -515,6 +568,36 @@ struct PipeArray {
 };
 static constexpr uint64_t kPipeMinUnits = 16384;
 
+// True for host memory the CUDA runtime has not page-locked (ordinary allocations).
+static bool host_pageable(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // clear the sticky-free error of an unknown pointer
+    return true;
+  }
+  return a.type == cudaMemoryTypeUnregistered;
+}
+
+// memcpy on a few host threads for large copies (staging of pageable arrays).
+static void host_copy(void* dst, const void* src, size_t bytes) {
+  constexpr size_t kPart = 1u << 20;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t parts = std::min<size_t>(std::min<size_t>(hw, 8), (bytes + kPart - 1) / kPart);
+  if (parts <= 1) {
+    memcpy(dst, src, bytes);
+    return;
+  }
+  const size_t step = (bytes + parts - 1) / parts;
+  std::vector<std::thread> th;
+  for (size_t i = 1; i < parts; ++i) {
+    const size_t b = i * step;
+    if (b >= bytes) break;
+    th.emplace_back([=] { memcpy((char*)dst + b, (const char*)src + b, std::min(step, bytes - b)); });
+  }
+  memcpy(dst, src, std::min(step, bytes));
+  for (std::thread& t : th) t.join();
+}
+
 static ech_status run_pipelined(ech_ctx* ctx, ech_tape* t, int kind, uint64_t n_units, const SweepIO& io,
                                 const size_t io_unit_bytes[5], const std::vector<PipeArray>& arrays, bool* done) {
   *done = false;
@@ -536,17 +619,43 @@ static ech_status run_pipelined(ech_ctx* ctx, ech_tape* t, int kind, uint64_t n_
   const int nc = ech_ctx::kPipe;
   uint64_t per = (n_units + nc - 1) / nc;
   per = (per + c.tile - 1) / c.tile * c.tile;
+  // Pageable host arrays (what a caller's ordinary allocations are) go through
+  // the context's page-locked staging buffers, one per chunk: the host copies a
+  // chunk's inputs in while earlier chunks' copies and sweeps run, and copies
+  // each chunk's outputs out as soon as its stream is done.
+  std::vector<uint8_t> staged(arrays.size(), 0);
+  size_t stage_bytes = 0;
+  for (size_t q = 0; q < arrays.size(); ++q) {
+    staged[q] = host_pageable(arrays[q].host) ? 1 : 0;
+    if (staged[q]) stage_bytes += per * arrays[q].unit_bytes;
+  }
+  if (stage_bytes)
+    for (PinnedBuf& b : ctx->pipe_stage) CU(b.ensure(stage_bytes));
+  auto stage_at = [&](int k, size_t q) {
+    size_t o = 0;
+    for (size_t r = 0; r < q; ++r)
+      if (staged[r]) o += per * arrays[r].unit_bytes;
+    return (unsigned char*)ctx->pipe_stage[k].p + o;
+  };
   ech_status first = ECH_OK;
+  int issued = 0;
   for (int k = 0; k < nc; ++k) {
     const uint64_t off = (uint64_t)k * per;
     if (off >= n_units) break;
     const uint64_t n = std::min<uint64_t>(per, n_units - off);
     cudaStream_t st = ctx->pipe[k];
     cudaError_t e = cudaStreamWaitEvent(st, ctx->pipe_ev, 0);
-    for (const PipeArray& a : arrays) {
+    issued = k + 1;
+    for (size_t q = 0; q < arrays.size(); ++q) {
+      const PipeArray& a = arrays[q];
       if (e != cudaSuccess || !a.in) continue;
-      e = cudaMemcpyAsync((unsigned char*)a.dev + off * a.unit_bytes, (const unsigned char*)a.host + off * a.unit_bytes,
-                          n * a.unit_bytes, cudaMemcpyHostToDevice, st);
+      const unsigned char* src = (const unsigned char*)a.host + off * a.unit_bytes;
+      if (staged[q]) {
+        host_copy(stage_at(k, q), src, n * a.unit_bytes);
+        src = stage_at(k, q);
+      }
+      e = cudaMemcpyAsync((unsigned char*)a.dev + off * a.unit_bytes, src, n * a.unit_bytes, cudaMemcpyHostToDevice,
+                          st);
     }
     if (e != cudaSuccess) {
       first = cuda_fail(e, "chunk copy");
@@ -566,20 +675,31 @@ static ech_status run_pipelined(ech_ctx* ctx, ech_tape* t, int kind, uint64_t n_
       first = s;
       break;
     }
-    for (const PipeArray& a : arrays) {
+    for (size_t q = 0; q < arrays.size(); ++q) {
+      const PipeArray& a = arrays[q];
       if (e != cudaSuccess || a.in) continue;
-      e = cudaMemcpyAsync((unsigned char*)a.host + off * a.unit_bytes, (const unsigned char*)a.dev + off * a.unit_bytes,
-                          n * a.unit_bytes, cudaMemcpyDeviceToHost, st);
+      unsigned char* dst = staged[q] ? stage_at(k, q) : (unsigned char*)a.host + off * a.unit_bytes;
+      e = cudaMemcpyAsync(dst, (const unsigned char*)a.dev + off * a.unit_bytes, n * a.unit_bytes,
+                          cudaMemcpyDeviceToHost, st);
     }
     if (e != cudaSuccess) {
       first = cuda_fail(e, "chunk copy");
       break;
     }
   }
-  // every chunk's copies finish before the host buffers are handed back
-  for (cudaStream_t st : ctx->pipe) {
-    cudaError_t e = cudaStreamSynchronize(st);
+  // every chunk's copies finish before the host buffers are handed back;
+  // staged outputs are copied out chunk by chunk as their streams finish
+  for (int k = 0; k < ech_ctx::kPipe; ++k) {
+    cudaError_t e = cudaStreamSynchronize(ctx->pipe[k]);
     if (e != cudaSuccess && first == ECH_OK) first = cuda_fail(e, "chunk sync");
+    if (e != cudaSuccess || first != ECH_OK || k >= issued) continue;
+    const uint64_t off = (uint64_t)k * per;
+    const uint64_t n = std::min<uint64_t>(per, n_units - off);
+    for (size_t q = 0; q < arrays.size(); ++q) {
+      const PipeArray& a = arrays[q];
+      if (a.in || !staged[q]) continue;
+      host_copy((unsigned char*)a.host + off * a.unit_bytes, stage_at(k, q), n * a.unit_bytes);
+    }
   }
   if (first != ECH_OK) return first;
   *done = true;
@@ -927,14 +1047,17 @@ static ech_status stde_checks(const ech_tape* t, size_t n, const char* caller, c
   return ECH_OK;
 }
 
-// Taylor order K (default 3) over npoints*S units, then the per-point Welford
+// Taylor order K (default 3) over npoints*S units, then the per-point
 // reduction of scale*c_kk (default 2*c2).
 // dir_mode: 0 dirs per unit, 1 shared [S][n], 2 device Rademacher, 3 basis e_s.
+// reduce: 0 Welford in the sample type (the reference's), 1 Welford in FP64,
+// 2 FP32 compensated sums (FP32 samples, no control term).
+// comp_jets: FP32 jets with compensated linear chains.
 template <class T>
 static ech_status stde_run(ech_ctx* ctx, ech_tape* t, const T* d_x, bool x_bcast, uint64_t npoints, uint32_t S,
-                           const T* d_dirs, int dir_mode, uint64_t seed, bool acc64, const T* d_cv, double trace,
+                           const T* d_dirs, int dir_mode, uint64_t seed, int reduce, const T* d_cv, double trace,
                            int control, ech_estimator_result* d_res, T* d_c0_out, T* d_c2_out, int K = 3,
-                           int kk = 2, double scale = 2.0, const T* d_wmul = nullptr) {
+                           int kk = 2, double scale = 2.0, const T* d_wmul = nullptr, bool comp_jets = false) {
   const uint64_t units = npoints * S;
   CU(ctx->stde_tmp.ensure(units * (uint64_t)K * sizeof(T)));
   SweepIO io;
@@ -945,12 +1068,16 @@ static ech_status stde_run(ech_ctx* ctx, ech_tape* t, const T* d_x, bool x_bcast
   io.S = S;
   io.dir_mode = dir_mode;
   io.seed = seed;
+  io.compensated = (comp_jets && sizeof(T) == 4) ? 1 : 0;
   CHECK(enqueue(ctx, t, 4, K, units, io, ctx->stream));
   const T* c0 = (const T*)ctx->stde_tmp.p;
   const T* c2 = c0 + (uint64_t)kk * units;
   if (d_res) {
-    CU(launch_stde_reduce_t(sizeof(T) == 8, acc64, c0, c2, scale, npoints, S, d_cv, trace, control, d_wmul, d_res,
-                            ctx->stream));
+    if (reduce == 2 && sizeof(T) == 4 && !control)
+      CU(launch_stde_reduce_comp(c0, c2, scale, npoints, S, d_wmul, d_res, ctx->stream));
+    else
+      CU(launch_stde_reduce_t(sizeof(T) == 8, reduce != 0, c0, c2, scale, npoints, S, d_cv, trace, control, d_wmul,
+                              d_res, ctx->stream));
   }
   if (d_c0_out) CU(cudaMemcpyAsync(d_c0_out, c0, units * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
   if (d_c2_out) CU(cudaMemcpyAsync(d_c2_out, c2, units * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
@@ -1031,6 +1158,15 @@ ECH_API ech_status ech_laplacian_with_control_gpu_f32(ech_ctx* ctx, const ech_ta
   return check_err_word(ctx);
 }
 
+// Reduction of the FP32 batch STDE calls: FP64 Welford unless the context
+// asks for FP32 (compensated or plain) sample means.  FP64 samples always
+// reduce in FP64.
+static int batch_reduce(const ech_ctx* ctx) {
+  if (ctx->fp32_mode & ECH_FP32_COMPENSATED_MEANS) return 2;
+  if (ctx->fp32_mode & ECH_FP32_PLAIN_MEANS) return 0;
+  return 1;
+}
+
 template <class T>
 static ech_status do_laplacian_batch(ech_ctx* ctx, const ech_tape* tc, const T* xs, size_t n_xs, uint32_t B,
                                      const T* dirs, size_t n_dirs, uint32_t S, int dir_mode, uint64_t seed,
@@ -1057,8 +1193,9 @@ static ech_status do_laplacian_batch(ech_ctx* ctx, const ech_tape* tc, const T* 
     CU(cudaMemcpyAsync(ctx->io_in2.p, dirs, n_dirs * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
     d_dirs = (const T*)ctx->io_in2.p;
   }
-  CHECK(stde_run<T>(ctx, t, (const T*)ctx->io_in.p, false, B, S, d_dirs, dir_mode, seed, true, nullptr, 0.0, 0,
-                    (ech_estimator_result*)ctx->io_out3.p, nullptr, nullptr));
+  CHECK(stde_run<T>(ctx, t, (const T*)ctx->io_in.p, false, B, S, d_dirs, dir_mode, seed, batch_reduce(ctx), nullptr,
+                    0.0, 0, (ech_estimator_result*)ctx->io_out3.p, nullptr, nullptr, 3, 2, 2.0, nullptr,
+                    (ctx->fp32_mode & ECH_FP32_COMPENSATED_JETS) != 0));
   CU(cudaMemcpyAsync(res, ctx->io_out3.p, (size_t)B * sizeof(ech_estimator_result), cudaMemcpyDeviceToHost,
                      ctx->stream));
   CU(cudaStreamSynchronize(ctx->stream));
@@ -1081,11 +1218,12 @@ ECH_API ech_status ech_laplacian_batch_device(ech_ctx* ctx, const ech_tape* tc, 
   ctx->stream = stream ? (cudaStream_t)stream : ctx->stream;  // stde_run enqueues on the context's stream
   ech_status s;
   if (f64)
-    s = stde_run<double>(ctx, t, (const double*)xs, false, B, S, (const double*)dirs, dir_mode, seed, true, nullptr,
+    s = stde_run<double>(ctx, t, (const double*)xs, false, B, S, (const double*)dirs, dir_mode, seed, 1, nullptr,
                          0.0, 0, results, nullptr, nullptr);
   else
-    s = stde_run<float>(ctx, t, (const float*)xs, false, B, S, (const float*)dirs, dir_mode, seed, true, nullptr, 0.0,
-                        0, results, nullptr, nullptr);
+    s = stde_run<float>(ctx, t, (const float*)xs, false, B, S, (const float*)dirs, dir_mode, seed, batch_reduce(ctx),
+                        nullptr, 0.0, 0, results, nullptr, nullptr, 3, 2, 2.0, nullptr,
+                        (ctx->fp32_mode & ECH_FP32_COMPENSATED_JETS) != 0);
   ctx->stream = saved;
   return s;
 }
@@ -1820,11 +1958,12 @@ ECH_API ech_status ech_plan_dump(const uint32_t* op, const uint32_t* a0, const u
                                  uint32_t nv, uint32_t ni, uint32_t output_index, const uint32_t* outs,
                                  uint32_t nouts, int kind, uint32_t cap, void* fwd, size_t fwd_cap, void* rev,
                                  size_t rev_cap, double* pool, size_t pool_cap, void* terms, size_t terms_cap,
-                                 void* gathers, size_t gathers_cap, uint64_t* counts) {
+                                 void* gathers, size_t gathers_cap, void* dense, size_t dense_cap,
+                                 uint32_t dense_max, uint64_t* counts) {
   if (!op || !a0 || !a1 || !values || !counts) return fail(ECH_ERR_INVALID_ARG, "null argument");
   std::string m = validate_bytecode_tape(op, a0, a1, nv, ni, output_index, outs, nouts, false);
   if (!m.empty()) return fail(ECH_ERR_OTHER, "invalid bytecode tape: " + m);
-  if (kind < 0 || kind > 4) return fail(ECH_ERR_INVALID_ARG, "kind must be 0..4");
+  if (kind < 0 || kind > 5) return fail(ECH_ERR_INVALID_ARG, "kind must be 0..5");
   HostTape h;
   h.nv = nv;
   h.ni = ni;
@@ -1835,7 +1974,9 @@ ECH_API ech_status ech_plan_dump(const uint32_t* op, const uint32_t* a0, const u
   h.vals.assign(values, values + nv);
   if (nouts == 0) h.outs.assign(1, output_index);
   else h.outs.assign(outs, outs + nouts);
-  Plan p = build_plan(h, kind_of(kind), cap);
+  Plan p = build_plan(h, kind_of(kind), cap, dense_max);
+  counts[8] = p.dense.size();
+  if (dense) memcpy(dense, p.dense.data(), std::min(dense_cap, p.dense.size()) * sizeof(PDenseOut));
   counts[0] = p.fwd.size();
   counts[1] = p.rev.size();
   counts[2] = p.pool.size();
@@ -1855,11 +1996,11 @@ ECH_API ech_status ech_plan_dump(const uint32_t* op, const uint32_t* a0, const u
 ECH_API ech_status ech_tape_plan_stats(ech_ctx* ctx, const ech_tape* tc, int kind, uint32_t order, int f64,
                                        uint64_t* stats) {
   if (!ctx || !tc || !stats) return fail(ECH_ERR_INVALID_ARG, "null argument");
-  if (kind < 0 || kind > 4) return fail(ECH_ERR_INVALID_ARG, "kind must be 0..4");
+  if (kind < 0 || kind > 5) return fail(ECH_ERR_INVALID_ARG, "kind must be 0..5");
   (void)f64;
   ech_tape* t = const_cast<ech_tape*>(tc);
   LaunchCfg c = choose_cfg(ctx, t, kind, (int)order);
-  Plan p = build_plan(t->host, kind_of(kind), c.cap);
+  Plan p = build_plan(t->host, kind_of(kind), c.cap, dense_group_max((uint32_t)c.vbytes, (uint32_t)c.req.P));
   const PlanStats& s = p.stats;
   uint64_t v[12] = {s.fwd_ops, s.rev_ops, s.max_live_fwd, s.max_live_rev, s.traj_values, s.flops_fwd, s.flops_rev,
                     s.specials_fwd, s.specials_rev, p.smem_regs, p.far_slots, p.fwd.size() + p.rev.size()};
@@ -1881,7 +2022,7 @@ ECH_API ech_status ech_tape_launch_shape(ech_ctx* ctx, const ech_tape* tc, int k
     if (it != t->shapes.end()) { sh = it->second; tuned = 1; }
   }
   c = tuned ? cfg_for(ctx, t, kind, (int)order, sh) : choose_cfg(ctx, t, kind, (int)order);
-  Plan p = build_plan(t->host, kind_of(kind), c.cap);
+  Plan p = build_plan(t->host, kind_of(kind), c.cap, dense_group_max((uint32_t)c.vbytes, (uint32_t)c.req.P));
   uint64_t v[8] = {(uint64_t)c.threads, (uint64_t)c.req.P, tuned ? sh.ctas : 0, c.cap, p.smem_regs, p.far_slots,
                    p.traj_slots, tuned};
   memcpy(shape, v, sizeof v);
@@ -1939,7 +2080,7 @@ static ech_status multi_prepare(ech_multi* m, Shape sh) {
     if (it.n_points == 0) continue;
     ech_tape* t = const_cast<ech_tape*>(it.tape);
     DevPlan* dp = nullptr;
-    CHECK(get_plan(t, 2, 0, c.cap, c.tile, (uint32_t)c.vbytes, &dp));
+    CHECK(get_plan(t, 2, 0, c.cap, c.tile, (uint32_t)c.vbytes, (uint32_t)c.req.P, &dp));
     const Plan& p = dp->host;
     regs = std::max<uint32_t>(regs, p.smem_regs);
     slots = std::max<uint64_t>(slots, (uint64_t)p.far_slots + p.traj_slots);
@@ -2120,13 +2261,13 @@ ech_status prepare_gradient_host(ech_ctx* ctx, const ech_tape* tc, int f64, uint
   const ech_tape::HostProgram* hp = nullptr;
   {
     std::lock_guard<std::mutex> lk(t->mu);
-    auto key = std::make_tuple(1, 0, c.cap, c.tile, (uint32_t)c.vbytes);
+    auto key = std::make_tuple(1, 0, c.cap, c.tile, (uint32_t)c.vbytes, (uint32_t)c.req.P);
     auto it = t->host_programs.find(key);
     if (it == t->host_programs.end()) {
       static std::atomic<uint64_t> next_id{1};
       std::unique_ptr<ech_tape::HostProgram> np(new ech_tape::HostProgram());
       np->id = next_id.fetch_add(1);
-      np->plan = build_plan(t->host, Kind::Gradient, c.cap);
+      np->plan = build_plan(t->host, Kind::Gradient, c.cap, dense_group_max((uint32_t)c.vbytes, (uint32_t)c.req.P));
       std::string err;
       if (!encode_plan(np->plan, c.tile, (uint32_t)c.vbytes, !t->f64, np->prog, err)) return fail(ECH_ERR_OTHER, err);
       it = t->host_programs.emplace(key, std::move(np)).first;

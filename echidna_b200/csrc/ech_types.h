@@ -22,6 +22,8 @@ enum OpCode : uint8_t {
   XI_CHAIN = 69,  // fused linear chain: dst <- acc0 (+|-) term_1 (+|-) ... ; terms in the chain table
   XI_NORM = 84,   // reverse: adj(r) <- adj(r) passed through a unit Add (the chain's term adjoint)
   XI_GATHER = 85, // reverse: each target adjoint accumulated over its chain contributions, stored once
+  XI_DENSE = 86,  // forward: m linear-combination chains over one operand list (a dense layer), one pass
+                  // over the operands: a = first output in the plan's dense table, aux = m
 };
 
 // One term of a fused chain s_t = s_{t-1} (+|-) term_t.  `kind` says how the
@@ -49,6 +51,8 @@ enum Mode : uint8_t {
   M_GLOB = 1,  // slot in the block's L2-resident global scratch ([slot][point])
   M_IMM = 2,   // constant: Ins::imm (forward) or RIns pool index (reverse)
   M_NONE = 3,
+  M_INPUT = 4, // (linear-combination term of a jet program) input `x` read from the launch's
+               // primal inputs and direction source, never materialised in a slot
 };
 
 // Forward instruction, 32 bytes.
@@ -101,6 +105,7 @@ enum DOp : uint8_t {
   D_MUL_RR, D_MUL_IR, D_MUL_RI, D_DIV_RR, D_DIV_IR, D_DIV_RI,  // .. 83
   D_CHAIN = 69,     // fused linear chain (forward and reverse)
   D_CHAIN_LC = 70,  // fused chain whose terms are all c*x or x*c added to the running value
+  D_DENSE = 86,     // forward: XI_DENSE; followed by its DDenseInit, term and DDenseFin records
   D_NORM = 84,      // reverse: XI_NORM
   D_GATHER = 85,    // reverse: XI_GATHER; per target a DRTerm header (ax, flags, ay = contributions)
                     // followed by DRPair records (ax = the chain adjoint's offset, c)
@@ -163,7 +168,7 @@ static_assert(sizeof(DRTerm) == sizeof(DRIns), "reverse term records are instruc
 struct alignas(16) DFPair {
   double c[2];
   uint32_t x[2];              // operand byte offsets
-  uint8_t m[2];               // M_SMEM / M_GLOB
+  uint8_t m[2];               // M_SMEM / M_GLOB, or M_INPUT (x = input index)
   uint8_t cx[2];              // 1: Mul(c, x), 0: Mul(x, c)
   uint32_t pad;
 };
@@ -176,6 +181,42 @@ struct alignas(16) DRPair {
   uint64_t pad2[2];
 };
 static_assert(sizeof(DRPair) == sizeof(DRIns), "reverse term records are instruction-sized");
+
+// A dense group (D_DENSE: aux = m outputs, a = n terms) in the forward stream:
+//   ceil(m/2) DDenseInit   the outputs' acc0
+//   per block of 4 terms: one DDenseOps (the terms' operands), then for each
+//     term of the block its m constants, 8 f32 or 4 f64 to a record
+//   ceil(m/2) DDenseFin    the outputs' destinations and trajectory saves
+struct alignas(16) DDenseInit {
+  double imm[2];
+  uint32_t off[2];            // byte offsets (M_SMEM / M_GLOB)
+  uint8_t mode[2];            // M_SMEM / M_GLOB / M_IMM
+  uint8_t pad[6];
+};
+static_assert(sizeof(DDenseInit) == 32, "dense records are instruction-sized");
+struct alignas(16) DDenseOps {
+  uint32_t x[4];              // byte offsets, or the input index (M_INPUT)
+  uint8_t m[4];               // M_SMEM / M_GLOB / M_INPUT
+  uint32_t pad[3];
+};
+static_assert(sizeof(DDenseOps) == 32, "dense records are instruction-sized");
+struct alignas(16) DDenseFin {
+  uint32_t d[2];              // byte offsets of the results
+  uint32_t save[2];           // byte offsets in the trajectory region, or kNone
+  uint8_t md[2];              // M_SMEM / M_GLOB
+  uint8_t pad[14];
+};
+static_assert(sizeof(DDenseFin) == 32, "dense records are instruction-sized");
+
+// Largest dense group for a value of `vbytes` bytes and `P` points per thread:
+// the group's running values stay in registers, 64 words per thread at most;
+// an even number, at most 16 (below 2: no groups).
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+constexpr uint32_t dense_group_max(uint32_t vbytes, uint32_t P) {
+  return ((256u / (vbytes * P)) > 16u ? 16u : (256u / (vbytes * P))) & ~1u;
+}
 
 // One seeded input coefficient of a slot-seeded jet (sparse STDE over a
 // differential operator): input `var` gets coefficient `slot` = `coef`.

@@ -57,6 +57,11 @@ struct KParams {
   uint64_t seed;
   const uint32_t* seed_off;  // dir_mode 5: entry e's seeds are seed_items[seed_off[e] .. seed_off[e+1])
   const void* seed_items;    // SlotSeed records
+  uint32_t dir_bits;         // dir_mode 2 with input-direct terms: byte offset in shared memory of the
+                             // tile's direction signs, [ceil(ni/32) words][tile units] (0: none)
+  uint32_t compensated;      // order-3 jets: Neumaier-compensated additions in fused chains (an FP32
+                             // option of the batch Laplacian; results then differ from the
+                             // reference's rounding)
 };
 
 // ───────────────────────────── bounded mbarrier waits ───────────────────────
@@ -298,6 +303,34 @@ __device__ __forceinline__ V lc_const(uint32_t lo, uint32_t hi) {
   else return dm::VT<V>::cst(__hiloint2double((int)hi, (int)lo));
 }
 
+// Scalar constant of a linear-combination term record (see lc_const).
+template <class T>
+__device__ __forceinline__ T lc_scalar(uint32_t lo, uint32_t hi) {
+  if constexpr (sizeof(T) == 4) return __uint_as_float(lo);
+  else return __hiloint2double((int)hi, (int)lo);
+}
+
+// Order of a jet value kind (0 for the other kinds).
+template <class V> struct JetOrder { static constexpr int K = 0; };
+template <class T, int K_> struct JetOrder<dm::Jet<T, K_>> { static constexpr int K = K_; };
+
+// x * 0 + z with one rounding: z unchanged (+0 stays +0) when x is finite, NaN otherwise.
+__device__ __forceinline__ float fma_zero(float x, float z) { return __fmaf_rn(x, 0.0f, z); }
+__device__ __forceinline__ double fma_zero(double x, double z) { return __fma_rn(x, 0.0, z); }
+
+// s + x with Neumaier's compensation (Neumaier, 1974): the rounding error of
+// the addition accumulates in c.
+template <class T>
+__device__ __forceinline__ void neumaier_add(T& s, T& c, T x) {
+  const T t = s + x;
+  c = c + ((fabs(s) >= fabs(x)) ? ((s - t) + x) : ((x - t) + s));
+  s = t;
+}
+
+// Dual value kind detection (the dense group's shared zero product).
+template <class V> struct IsDual { static constexpr bool v = false; };
+template <class T> struct IsDual<dm::Dual<T>> { static constexpr bool v = true; };
+
 // Per-kind input construction and output handling; the primary template is
 // the plain-value kind (forward, gradient).  `Info` is what a unit's inputs
 // depend on beyond the unit index, computed once per tile (empty for plain and
@@ -423,8 +456,13 @@ template <class V, int P> struct FwdExec {
   unsigned char* gs;     // ... in the global slots
   unsigned char* tj;     // ... in the trajectory region
   uint64_t unit0;        // unit of point p = unit0 + p
+  const uint32_t* bits;  // this thread's column of the direction-sign words (dir_bits)
   bool valid[P];
   typename Lane<V>::Info ui[P];
+  // jets of point-direction launches, per point of the thread (set per tile):
+  const void* xrow[P];   // the unit's primal row
+  const void* vrow[P];   // dir_mode 1: the unit's direction row
+  uint32_t sel[P];       // dir_mode 3 / 4: the coordinate of the basis direction
 
   __device__ __forceinline__ void ld(uint32_t mode, uint32_t off, double imm, V (&v)[P]) const {
     if (mode == M_SMEM) C::ld(sm + off, v);
@@ -455,6 +493,9 @@ template <class V, int P> struct FwdExec {
   // (kind|op|xm|ym, x, y, pad | c, pad).
   __device__ __forceinline__ bool chain(Stream<32>& st, uint32_t ma, uint32_t ao, double imm, uint32_t n,
                                         V (&acc)[P]) const {
+    if constexpr (JetOrder<V>::K == 3) {  // the compensated option serves the order-3 batch Laplacian
+      if (kp.compensated) return chain_comp(st, ma, ao, imm, n, acc);
+    }
     ld(ma, ao, imm, acc);
 #pragma unroll 1
     for (uint32_t q = 0; q < n; ++q) {
@@ -507,6 +548,64 @@ template <class V, int P> struct FwdExec {
     return true;
   }
 
+  // The fused chain over jets with compensated additions: every coefficient of
+  // the running value carries a Neumaier compensation term, folded in at the
+  // end.  A subtraction adds the negated term; t - acc negates the running
+  // value and its compensation first (negation is exact).
+  __device__ __forceinline__ bool chain_comp(Stream<32>& st, uint32_t ma, uint32_t ao, double imm, uint32_t n,
+                                             V (&acc)[P]) const {
+    using T = typename dm::VT<V>::S;
+    constexpr int K = JetOrder<V>::K;
+    ld(ma, ao, imm, acc);
+    T cmp[P][K];
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+#pragma unroll
+      for (int k = 0; k < K; ++k) cmp[p][k] = T(0);
+#pragma unroll 1
+    for (uint32_t q = 0; q < n; ++q) {
+      const unsigned char* rec = st.next();
+      if (rec == nullptr) return false;
+      const uint4 w0 = *reinterpret_cast<const uint4*>(rec);
+      const uint2 w1 = *reinterpret_cast<const uint2*>(rec + 16);
+      const uint32_t kind = w0.x & 0xFFu, op = (w0.x >> 8) & 0xFFu;
+      V t[P], x[P];
+      if (kind == CK_C) {
+        const V c = dm::VT<V>::cst(__hiloint2double((int)w1.y, (int)w1.x));
+#pragma unroll
+        for (int p = 0; p < P; ++p) t[p] = c;
+      } else {
+        ldv((w0.x >> 16) & 0xFFu, w0.y, kind == CK_X ? t : x);
+        if (kind == CK_CX || kind == CK_XC) {
+          const V c = dm::VT<V>::cst(__hiloint2double((int)w1.y, (int)w1.x));
+#pragma unroll
+          for (int p = 0; p < P; ++p) t[p] = kind == CK_CX ? Kd::mul(c, x[p]) : Kd::mul(x[p], c);
+        } else if (kind == CK_XY) {
+          V y[P];
+          ldv(w0.x >> 24, w0.z, y);
+#pragma unroll
+          for (int p = 0; p < P; ++p) t[p] = Kd::mul(x[p], y[p]);
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          if (op == 3) {
+            acc[p].c[k] = -acc[p].c[k];
+            cmp[p][k] = -cmp[p][k];
+          }
+          neumaier_add(acc[p].c[k], cmp[p][k], op == 2 ? -t[p].c[k] : t[p].c[k]);
+        }
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+#pragma unroll
+      for (int k = 0; k < K; ++k) acc[p].c[k] = acc[p].c[k] + cmp[p][k];
+    return true;
+  }
+
   // Linear-combination chain: every term is Mul(c, x) or Mul(x, c) added to the
   // running value, in tape order.  DFPair records carry two terms each
   // (c0, c1 | x0, x1, m0|m1|cx0|cx1, pad).  kLcGroup records at a time: all
@@ -517,6 +616,7 @@ template <class V, int P> struct FwdExec {
   static constexpr int kLcGroup = kWords <= 8 ? 4 : (kWords <= 16 ? 2 : 1);
   __device__ __forceinline__ bool chain_lc(Stream<32>& st, uint32_t ma, uint32_t ao, double imm, uint32_t n,
                                            V (&acc)[P]) const {
+    if constexpr (JetOrder<V>::K > 0) return chain_lc_jet(st, ma, ao, imm, n, acc);
     ld(ma, ao, imm, acc);
     uint32_t q = 0;
     if constexpr (kLcGroup > 1) {
@@ -575,6 +675,336 @@ template <class V, int P> struct FwdExec {
     return true;
   }
 
+  // Linear-combination chain over jets.  The reference multiplies a constant c
+  // and a jet x as the truncated Cauchy product of the constant jet (c, 0, ..)
+  // with x, in either operand order:
+  //   t_k = ((0 + c x_k) + 0 x_{k-1}) + ... + 0 x_0.
+  // With x_0..x_{k-1} finite the zero products change nothing and t_k is c x_k
+  // with a -0 turned into +0; a non-finite x_j (j < k) makes t_k NaN.  So the
+  // running value starts as acc0 + 0 (after which no coefficient is ever -0,
+  // and adding c x_k equals adding t_k), each term adds c x_k to coefficient
+  // k, and per coefficient j below the top a tracker z_j = x_j * 0 + z_j (one
+  // fused, exact step: +0 while every x_j is finite, NaN after) is added to
+  // every higher coefficient at the end.  Results equal the per-op product bit
+  // for bit; each term costs K multiplies, K adds and K-1 fused steps instead
+  // of the product's K(K+1) operations.
+  // Primal x_i and direction component v_i of point p's unit: the input jet
+  // (x_i, v_i, 0, ..) of an M_INPUT term, read at its source.  Programs with
+  // such terms run for point-direction launches (S > 0) with directions shared
+  // over points (dir_mode 1), device Rademacher signs (2, from the tile's sign
+  // words) or basis vectors (3, 4).
+  __device__ __forceinline__ void input_xv(uint32_t i, int p, typename dm::VT<V>::S& x0,
+                                           typename dm::VT<V>::S& v) const {
+    using T = typename dm::VT<V>::S;
+    if (!valid[p]) {
+      x0 = T(0);
+      v = T(0);
+      return;
+    }
+    x0 = reinterpret_cast<const T*>(xrow[p])[i];
+    if (kp.dir_mode == 2) v = ((bits[(i >> 5) * kp.tile + p] >> (i & 31u)) & 1u) ? T(1) : T(-1);
+    else if (kp.dir_mode == 1) v = reinterpret_cast<const T*>(vrow[p])[i];
+    else v = (i == sel[p]) ? T(1) : T(0);
+  }
+  // An M_INPUT term: coefficients 0 and 1 of the input jet are x_i and v_i, the
+  // rest +0, whose products add nothing to a running value that is never -0;
+  // only the trackers of x_i and v_i remain for the higher coefficients.
+  template <bool COMP>
+  __device__ __forceinline__ void lc_jet_input_term(V (&acc)[P], typename dm::VT<V>::S (&z)[P][JetOrder<V>::K],
+                                                    typename dm::VT<V>::S (&cmp)[P][JetOrder<V>::K],
+                                                    const V (&x)[P], typename dm::VT<V>::S c) const {
+    constexpr int K = JetOrder<V>::K;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      if constexpr (COMP) neumaier_add(acc[p].c[0], cmp[p][0], c * x[p].c[0]);
+      else acc[p].c[0] = acc[p].c[0] + c * x[p].c[0];
+      if constexpr (K > 1) {
+        if constexpr (COMP) neumaier_add(acc[p].c[1], cmp[p][1], c * x[p].c[1]);
+        else acc[p].c[1] = acc[p].c[1] + c * x[p].c[1];
+        z[p][0] = fma_zero(x[p].c[0], z[p][0]);
+      }
+      if constexpr (K > 2) z[p][1] = fma_zero(x[p].c[1], z[p][1]);
+    }
+  }
+  // Operand j of a linear-combination term record into x: a slot load, or the
+  // input jet at its source (returns true for M_INPUT).
+  __device__ __forceinline__ bool lc_jet_operand(uint32_t mode, uint32_t off, V (&x)[P]) const {
+    if (mode == M_INPUT) {
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        typename dm::VT<V>::S x0, v;
+        input_xv(off, p, x0, v);
+        x[p].c[0] = x0;
+        if constexpr (JetOrder<V>::K > 1) x[p].c[1] = v;
+      }
+      return true;
+    }
+    ldv(mode, off, x);
+    return false;
+  }
+  template <bool COMP>
+  __device__ __forceinline__ void lc_jet_term(V (&acc)[P], typename dm::VT<V>::S (&z)[P][JetOrder<V>::K],
+                                              typename dm::VT<V>::S (&cmp)[P][JetOrder<V>::K],
+                                              const V (&x)[P], typename dm::VT<V>::S c) const {
+    constexpr int K = JetOrder<V>::K;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if constexpr (COMP) neumaier_add(acc[p].c[k], cmp[p][k], c * x[p].c[k]);
+        else acc[p].c[k] = acc[p].c[k] + c * x[p].c[k];
+      }
+#pragma unroll
+      for (int k = 0; k + 1 < K; ++k) z[p][k] = fma_zero(x[p].c[k], z[p][k]);
+    }
+  }
+  __device__ __forceinline__ bool chain_lc_jet(Stream<32>& st, uint32_t ma, uint32_t ao, double imm, uint32_t n,
+                                               V (&acc)[P]) const {
+    if constexpr (JetOrder<V>::K == 3) {  // the compensated option serves the order-3 batch Laplacian
+      if (kp.compensated) return chain_lc_jet_impl<true>(st, ma, ao, imm, n, acc);
+    }
+    return chain_lc_jet_impl<false>(st, ma, ao, imm, n, acc);
+  }
+  // COMP: every coefficient's additions carry a Neumaier compensation term
+  // (the FP32 compensated option), folded in before the trackers.
+  template <bool COMP>
+  __device__ __forceinline__ bool chain_lc_jet_impl(Stream<32>& st, uint32_t ma, uint32_t ao, double imm, uint32_t n,
+                                                    V (&acc)[P]) const {
+    using T = typename dm::VT<V>::S;
+    constexpr int K = JetOrder<V>::K;
+    ld(ma, ao, imm, acc);
+    T z[P][K], cmp[P][K];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        acc[p].c[k] = acc[p].c[k] + T(0);
+        z[p][k] = T(0);
+        cmp[p][k] = T(0);
+      }
+    }
+    uint32_t q = 0;
+    if constexpr (kLcGroup > 1) {
+#pragma unroll 1
+      for (; q + 2 * kLcGroup <= n; q += 2 * kLcGroup) {
+        V xs[2 * kLcGroup][P];
+        T cs[2 * kLcGroup];
+        bool direct[2 * kLcGroup];
+#pragma unroll
+        for (int k = 0; k < kLcGroup; ++k) {
+          const unsigned char* rec = st.next();
+          if (rec == nullptr) return false;
+          const uint4 cw = *reinterpret_cast<const uint4*>(rec);
+          const uint4 xw = *reinterpret_cast<const uint4*>(rec + 16);
+          direct[2 * k] = lc_jet_operand(xw.z & 0xFFu, xw.x, xs[2 * k]);
+          direct[2 * k + 1] = lc_jet_operand((xw.z >> 8) & 0xFFu, xw.y, xs[2 * k + 1]);
+          cs[2 * k] = lc_scalar<T>(cw.x, cw.y);
+          cs[2 * k + 1] = lc_scalar<T>(cw.z, cw.w);
+        }
+#pragma unroll
+        for (int j = 0; j < 2 * kLcGroup; ++j) {
+          if (direct[j]) lc_jet_input_term<COMP>(acc, z, cmp, xs[j], cs[j]);
+          else lc_jet_term<COMP>(acc, z, cmp, xs[j], cs[j]);
+        }
+      }
+    }
+#pragma unroll 1
+    for (; q < n; q += 2) {
+      const unsigned char* rec = st.next();
+      if (rec == nullptr) return false;
+      const uint4 cw = *reinterpret_cast<const uint4*>(rec);
+      const uint4 xw = *reinterpret_cast<const uint4*>(rec + 16);
+      V xa[P];
+      if (lc_jet_operand(xw.z & 0xFFu, xw.x, xa)) lc_jet_input_term<COMP>(acc, z, cmp, xa, lc_scalar<T>(cw.x, cw.y));
+      else lc_jet_term<COMP>(acc, z, cmp, xa, lc_scalar<T>(cw.x, cw.y));
+      if (q + 1 < n) {
+        V xb[P];
+        if (lc_jet_operand((xw.z >> 8) & 0xFFu, xw.y, xb))
+          lc_jet_input_term<COMP>(acc, z, cmp, xb, lc_scalar<T>(cw.z, cw.w));
+        else
+          lc_jet_term<COMP>(acc, z, cmp, xb, lc_scalar<T>(cw.z, cw.w));
+      }
+    }
+    if constexpr (COMP) {
+#pragma unroll
+      for (int p = 0; p < P; ++p)
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc[p].c[k] = acc[p].c[k] + cmp[p][k];
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      T zs = T(0);
+#pragma unroll
+      for (int k = 1; k < K; ++k) {
+        zs = zs + z[p][k - 1];
+        acc[p].c[k] = acc[p].c[k] + zs;
+      }
+    }
+    return true;
+  }
+
+  // Dense group (D_DENSE): m linear-combination chains over the same n
+  // operands, outputs j = 0..m-1:  z_j = acc0_j + c_j0 x_0 + .. + c_j,n-1 x_n-1,
+  // each added in term order as the chains do, but with one operand load per
+  // term for the whole group.  The m running values live in registers; the
+  // results are stored after every operand has been read (a result may take an
+  // operand's register).  Products follow the kinds' exact forms:
+  //   plain  c x;
+  //   Dual   (c re, c eps + 0 re), the zero product shared by the group;
+  //   jets   the scaled, normalised form with per-term trackers (chain_lc_jet).
+  static constexpr int kDenseMax = (int)dense_group_max((uint32_t)sizeof(V), (uint32_t)P);
+  __device__ __forceinline__ bool dense(Stream<32>& st, uint32_t m, uint32_t n) const {
+    if constexpr (kDenseMax < 2) {
+      if (threadIdx.x == 0) atomicOr(kp.err, (uint32_t)KERR_BADINS);
+      ring_drain(*st.rg);
+      return false;
+    } else {
+      if constexpr (JetOrder<V>::K == 3) {
+        if (kp.compensated) return dense_impl<true>(st, m, n);
+      }
+      return dense_impl<false>(st, m, n);
+    }
+  }
+  template <bool COMP>
+  __device__ __forceinline__ bool dense_impl(Stream<32>& st, uint32_t m, uint32_t n) const {
+    using T = typename dm::VT<V>::S;
+    constexpr int MX = kDenseMax > 1 ? kDenseMax : 2;
+    constexpr int KJ = JetOrder<V>::K > 0 ? JetOrder<V>::K : 1;
+    constexpr int PER = sizeof(T) == 4 ? 8 : 4;  // constants per record
+    if (m < 1 || m > (uint32_t)kDenseMax) {
+      if (threadIdx.x == 0) atomicOr(kp.err, (uint32_t)KERR_BADINS);
+      ring_drain(*st.rg);
+      return false;
+    }
+    V acc[MX][P];
+#pragma unroll
+    for (int jj = 0; jj < MX; jj += 2) {
+      if ((uint32_t)jj < m) {
+        const unsigned char* rec = st.next();
+        if (rec == nullptr) return false;
+        const double2 imm = *reinterpret_cast<const double2*>(rec);
+        const uint4 w = *reinterpret_cast<const uint4*>(rec + 16);
+        ld(w.z & 0xFFu, w.x, imm.x, acc[jj]);
+        if ((uint32_t)jj + 1 < m) ld((w.z >> 8) & 0xFFu, w.y, imm.y, acc[jj + 1]);
+      }
+    }
+    T z[P][KJ], cmp[COMP ? MX : 1][P][KJ];
+    if constexpr (JetOrder<V>::K > 0) {
+#pragma unroll
+      for (int p = 0; p < P; ++p)
+#pragma unroll
+        for (int k = 0; k < KJ; ++k) z[p][k] = T(0);
+#pragma unroll
+      for (int j = 0; j < MX; ++j)
+#pragma unroll
+        for (int p = 0; p < P; ++p)
+#pragma unroll
+          for (int k = 0; k < KJ; ++k) {
+            acc[j][p].c[k] = acc[j][p].c[k] + T(0);
+            if constexpr (COMP) cmp[j][p][k] = T(0);
+          }
+    }
+#pragma unroll 1
+    for (uint32_t q0 = 0; q0 < n; q0 += 4) {
+      const unsigned char* orec = st.next();
+      if (orec == nullptr) return false;
+      const uint4 xw = *reinterpret_cast<const uint4*>(orec);
+      const uint32_t mw = *reinterpret_cast<const uint32_t*>(orec + 16);
+      const uint32_t xo[4] = {xw.x, xw.y, xw.z, xw.w};
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        if (q0 + t >= n) break;
+        const uint32_t mode = (mw >> (8 * t)) & 0xFFu;
+        V x[P];
+        bool direct = false;
+        if constexpr (JetOrder<V>::K > 0) direct = lc_jet_operand(mode, xo[t], x);
+        else ldv(mode, xo[t], x);
+        T zr[P];
+        if constexpr (IsDual<V>::v) {
+#pragma unroll
+          for (int p = 0; p < P; ++p) zr[p] = x[p].re * T(0);
+        }
+#pragma unroll
+        for (int jj = 0; jj < MX; jj += PER) {
+          if ((uint32_t)jj < m) {
+            const unsigned char* crec = st.next();
+            if (crec == nullptr) return false;
+            T cs[PER];
+#pragma unroll
+            for (int j = 0; j < PER; ++j) cs[j] = reinterpret_cast<const T*>(crec)[j];
+#pragma unroll
+            for (int j = 0; j < PER; ++j) {
+              if (jj + j < MX && (uint32_t)(jj + j) < m) {
+                const T c = cs[j];
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                  V& a = acc[jj + j < MX ? jj + j : 0][p];
+                  if constexpr (JetOrder<V>::K > 0) {
+                    const int kmax = direct ? (KJ > 1 ? 2 : 1) : KJ;
+#pragma unroll
+                    for (int k = 0; k < KJ; ++k) {
+                      if (k < kmax) {
+                        if constexpr (COMP) neumaier_add(a.c[k], cmp[jj + j < MX ? jj + j : 0][p][k], c * x[p].c[k]);
+                        else a.c[k] = a.c[k] + c * x[p].c[k];
+                      }
+                    }
+                  } else if constexpr (IsDual<V>::v) {
+                    a.re = a.re + c * x[p].re;
+                    a.eps = a.eps + (c * x[p].eps + zr[p]);
+                  } else {
+                    a = a + c * x[p];
+                  }
+                }
+              }
+            }
+          }
+        }
+        if constexpr (JetOrder<V>::K > 1) {
+#pragma unroll
+          for (int p = 0; p < P; ++p) {
+            if (direct) {
+              z[p][0] = fma_zero(x[p].c[0], z[p][0]);
+              if constexpr (KJ > 2) z[p][1] = fma_zero(x[p].c[1], z[p][1]);
+            } else {
+#pragma unroll
+              for (int k = 0; k + 1 < KJ; ++k) z[p][k] = fma_zero(x[p].c[k], z[p][k]);
+            }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int jj = 0; jj < MX; jj += 2) {
+      if ((uint32_t)jj < m) {
+        const unsigned char* rec = st.next();
+        if (rec == nullptr) return false;
+        const uint4 w0 = *reinterpret_cast<const uint4*>(rec);
+        const uint32_t mdw = *reinterpret_cast<const uint32_t*>(rec + 16);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j = jj + h;
+          if (j >= MX || (uint32_t)j >= m) continue;
+          if constexpr (JetOrder<V>::K > 0) {
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+              T zs = T(0);
+#pragma unroll
+              for (int k = 0; k < KJ; ++k) {
+                if constexpr (COMP) acc[j][p].c[k] = acc[j][p].c[k] + cmp[j][p][k];
+                if (k > 0) {
+                  zs = zs + z[p][k - 1];
+                  acc[j][p].c[k] = acc[j][p].c[k] + zs;
+                }
+              }
+            }
+          }
+          put((mdw >> (8 * h)) & 0xFFu, h == 0 ? w0.x : w0.y, h == 0 ? w0.z : w0.w, acc[j]);
+        }
+      }
+    }
+    return true;
+  }
+
   __device__ __forceinline__ bool operator()(const unsigned char* raw, Stream<32>& st) const {
     const uint4 w0 = *reinterpret_cast<const uint4*>(raw);
     const uint4 w1 = *reinterpret_cast<const uint4*>(raw + 16);
@@ -606,6 +1036,8 @@ template <class V, int P> struct FwdExec {
         if (!chain_lc(st, (w0.x >> 8) & 0xFFu, ao, imm, (uint32_t)aux, r)) return false;
         put(w0.x >> 24, dof, save, r);
         return true;
+      case D_DENSE:
+        return dense(st, (uint32_t)aux, ao);
 #define ECH_FB(NAME, FN)                                                     \
   case D_##NAME##_RR:                                                        \
     C::ld(sm + ao, a);                                                       \
@@ -1041,11 +1473,41 @@ __device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned
   unsigned char* tj = kp.traj_smem ? sm + (size_t)kp.smem_regs * tile * sizeof(V)
                                    : gbase + (size_t)kp.far_slots * tile * sizeof(V) + colb;
   const uint64_t unit0 = t * tile + (uint64_t)threadIdx.x * P;
-  FwdExec<V, P> fx{kp, sm, gs, tj, unit0, {}, {}};
+  uint32_t* bits = kp.dir_bits ? reinterpret_cast<uint32_t*>(rg.buf + kp.dir_bits) + threadIdx.x * P : nullptr;
+  FwdExec<V, P> fx{kp, sm, gs, tj, unit0, bits, {}, {}, {}, {}, {}};
 #pragma unroll
   for (int p = 0; p < P; ++p) {
     fx.valid[p] = unit0 + p < kp.n_units;
     fx.ui[p] = Lane<V>::info(kp, unit0 + p, fx.valid[p]);
+  }
+  if constexpr (JetOrder<V>::K > 0) {
+    // source rows of the input jets that input-direct terms read (S > 0 launches)
+    using T = typename dm::VT<V>::S;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const uint64_t row = kp.x_bcast ? 0 : (kp.S ? (uint64_t)fx.ui[p].pt : unit0 + p);
+      fx.xrow[p] = reinterpret_cast<const T*>(kp.x) + row * kp.ni;
+      fx.vrow[p] = kp.dir_mode == 1 ? reinterpret_cast<const T*>(kp.v) + (uint64_t)fx.ui[p].s * kp.ni : nullptr;
+      fx.sel[p] = kp.dir_mode == 3 ? fx.ui[p].s : fx.ui[p].ent;
+    }
+    // the tile's Rademacher signs, one bit per input and unit (the same stream
+    // as the per-input draw); each thread writes and reads its own units' words
+    if (bits) {
+      const uint32_t nw = (kp.ni + 31) / 32;
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+#pragma unroll 1
+        for (uint32_t w = 0; w < nw; ++w) {
+          uint32_t word = 0;
+          if (fx.valid[p]) {
+#pragma unroll 1
+            for (uint32_t b = 0; b < 32 && w * 32 + b < kp.ni; ++b)
+              word |= (philox_bits(kp.seed, fx.ui[p].pt, fx.ui[p].s, w * 32 + b) & 1u) << b;
+          }
+          bits[w * tile + p] = word;
+        }
+      }
+    }
   }
   if (!run_program<32>(rg, reinterpret_cast<const unsigned char*>(kp.fwd), kp.n_fwd, kp.err, fx)) return false;
   if (REV) {

@@ -36,6 +36,19 @@ cudaError_t launch_by_p(const LaunchReq& r, const KParams& kp, int grid, int blo
   }
 }
 
+// Forward-only kinds (jets): no reverse instantiations.
+template <class V>
+cudaError_t launch_by_p_fwd(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
+                            int* bps) {
+  if (r.rev) return cudaErrorInvalidValue;
+  switch (r.P) {
+    case 1: return launch_one<V, 1, false>(kp, grid, block, smem, st, bps);
+    case 2: return launch_one<V, 2, false>(kp, grid, block, smem, st, bps);
+    case 4: return launch_one<V, 4, false>(kp, grid, block, smem, st, bps);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 // One point per thread only (wide jets used by the sparse STDE path).
 template <class V>
 cudaError_t launch_p1(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,

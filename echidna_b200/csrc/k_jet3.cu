@@ -5,7 +5,7 @@ namespace ech {
 cudaError_t launch_jet3(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
                         int* bps) {
   if (r.rev) return cudaErrorInvalidValue;
-  return r.f64 ? launch_by_p<dm::Jet<double, 3>>(r, kp, grid, block, smem, st, bps)
-               : launch_by_p<dm::Jet<float, 3>>(r, kp, grid, block, smem, st, bps);
+  return r.f64 ? launch_by_p_fwd<dm::Jet<double, 3>>(r, kp, grid, block, smem, st, bps)
+               : launch_by_p_fwd<dm::Jet<float, 3>>(r, kp, grid, block, smem, st, bps);
 }
 }  // namespace ech

@@ -48,6 +48,10 @@ cudaError_t launch_multi_hvp(bool f64, int P, const MultiParams& mp, int grid, i
 cudaError_t launch_stde_reduce_t(bool f64, bool acc64, const void* c0, const void* ck, double scale, uint64_t npoints,
                                  uint32_t S, const void* cv, double trace, int control, const void* wmul,
                                  void* results, cudaStream_t st);
+// The same per-point reduction of FP32 samples in FP32 with compensated sums
+// (mean, then the corrected two-pass variance); no control term.
+cudaError_t launch_stde_reduce_comp(const void* c0, const void* ck, double scale, uint64_t npoints, uint32_t S,
+                                    const void* wmul, void* results, cudaStream_t st);
 // S coordinates per point from probability rows (or uniform when probs is null),
 // with their importance weights; y *= a.
 cudaError_t launch_sample_coords(bool f64, const float* probs, uint32_t n, uint64_t npoints, uint32_t S,

@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cmath>
 #include <cstring>
 #include <set>
 #include <sstream>
@@ -254,7 +255,7 @@ struct LinearScan {
 
 }  // namespace
 
-Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
+Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap, uint32_t dense_max) {
   const uint32_t nv = t.nv, ni = t.ni;
   const bool reverse = (kind == Kind::Gradient || kind == Kind::Hvp);
   const bool emit_outputs = (kind != Kind::Hvp);
@@ -436,6 +437,79 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
     }
   }
 
+  // ---------------- direct input terms (TaylorDirect) ----------------
+  // In a linear-combination chain (every term c*x or x*c added) a term whose x
+  // is an input and whose constant is finite reads the input jet at its source;
+  // an input whose every use is such a term is never loaded into a slot.
+  std::vector<uint8_t> term_direct(pl.terms.size(), 0);
+  std::vector<uint32_t> direct_uses(kind == Kind::TaylorDirect ? ni : 0, 0);
+  if (kind == Kind::TaylorDirect) {
+    for (const Chain& ch : chains) {
+      bool lc = ch.tn > 0;
+      for (uint32_t q = ch.tb; q < ch.tb + ch.tn && lc; ++q) {
+        const PTerm& pt = pl.terms[q];
+        lc = (pt.kind == CK_CX || pt.kind == CK_XC) && pt.op == 0;
+      }
+      if (!lc) continue;
+      for (uint32_t q = ch.tb; q < ch.tb + ch.tn; ++q) {
+        const PTerm& pt = pl.terms[q];
+        if (pt.xs < ni && t.op[pt.xs] == OP_INPUT && std::isfinite(pt.c)) {
+          term_direct[q] = 1;
+          direct_uses[pt.xs]++;
+        }
+      }
+    }
+  }
+
+  // ---------------- dense groups ----------------
+  // Consecutive linear-combination chains that read the same operands in the
+  // same order (a dense layer: z_j = b_j + sum_i W_ji x_i) run as one forward
+  // instruction that loads each operand once for the whole group.  Each
+  // chain's additions keep their order, so results are those of the chains;
+  // the reverse program still sees the chains one by one.  The group runs
+  // where its first chain would, so every later chain's acc0 must be a
+  // constant or a value defined before the first chain's ops.
+  struct DenseGroup {
+    uint32_t c0, m;
+  };
+  std::vector<DenseGroup> groups;
+  std::vector<int32_t> group_of(chains.size(), -1);
+  if (dense_max > 1) {
+    auto lc_chain = [&](const Chain& ch) {
+      if (ch.tn == 0) return false;
+      for (uint32_t q = ch.tb; q < ch.tb + ch.tn; ++q) {
+        const PTerm& pt = pl.terms[q];
+        if ((pt.kind != CK_CX && pt.kind != CK_XC) || pt.op != 0) return false;
+      }
+      return true;
+    };
+    auto same_operands = [&](const Chain& a, const Chain& b) {
+      if (a.tn != b.tn) return false;
+      for (uint32_t q = 0; q < a.tn; ++q) {
+        if (pl.terms[a.tb + q].xs != pl.terms[b.tb + q].xs) return false;
+        if (term_direct[a.tb + q] != term_direct[b.tb + q]) return false;
+      }
+      return true;
+    };
+    uint32_t c = 0;
+    while (c < chains.size()) {
+      if (!lc_chain(chains[c])) { ++c; continue; }
+      const Chain& lead = chains[c];
+      uint32_t m = 1;
+      while (c + m < chains.size() && m < dense_max) {
+        const Chain& ch = chains[c + m];
+        if (!lc_chain(ch) || !same_operands(lead, ch)) break;
+        if (ch.acc0 >= 0 && (uint64_t)ch.acc0 >= lead.first) break;
+        ++m;
+      }
+      if (m >= 2) {
+        for (uint32_t k = 0; k < m; ++k) group_of[c + k] = (int32_t)groups.size();
+        groups.push_back({c, m});
+      }
+      c += m;
+    }
+  }
+
   // ---------------- forward program (symbolic) ----------------
   struct FSym {
     uint8_t opc;
@@ -496,7 +570,32 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
     f.b = -1;
     f.chain = -1;
     if (absorbed[i] && chain_end[i] < 0) continue;  // inside a fused chain
-    if (chain_end[i] >= 0) {
+    if (chain_end[i] >= 0 && group_of[chain_end[i]] >= 0) {
+      const DenseGroup& g = groups[group_of[chain_end[i]]];
+      if ((uint32_t)chain_end[i] != g.c0) {  // computed with its group's first chain
+        emit_outputs_for(i);
+        continue;
+      }
+      const int64_t pos = (int64_t)fs.size();
+      f.opc = XI_DENSE;
+      f.chain = group_of[chain_end[i]];
+      f.aux = (int32_t)g.m;
+      f.a = -1;
+      f.save = kNone;
+      const Chain& lead = chains[g.c0];
+      for (uint32_t q = 0; q < lead.tn; ++q)
+        if (!term_direct[lead.tb + q]) use(pl.terms[lead.tb + q].xs, pos);
+      for (uint32_t k = 0; k < g.m; ++k) {
+        const Chain& ch = chains[g.c0 + k];
+        if (ch.acc0 >= 0) use((uint32_t)ch.acc0, pos);
+        if (k > 0) def_pos[ch.last] = pos;
+        for (uint32_t q = ch.first; q <= ch.last; ++q) {
+          if (!absorbed[q]) continue;
+          op_cost(t.op[q], pl.stats.flops_fwd, pl.stats.specials_fwd);
+          pl.stats.fwd_ops++;
+        }
+      }
+    } else if (chain_end[i] >= 0) {
       const Chain& ch = chains[chain_end[i]];
       const int64_t pos = (int64_t)fs.size();
       f.opc = XI_CHAIN;
@@ -506,6 +605,7 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
       else { f.a = -1; f.a_imm = true; f.a_val = ch.acc0_val; }
       for (uint32_t q = 0; q < ch.tn; ++q) {
         const PTerm& pt = pl.terms[ch.tb + q];
+        if (term_direct[ch.tb + q]) continue;  // read at the source, not from a slot
         if (pt.xs != kNone) use(pt.xs, pos);
         if (pt.ys != kNone) use(pt.ys, pos);
       }
@@ -515,6 +615,7 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
         pl.stats.fwd_ops++;
       }
     } else if (o == OP_INPUT) {
+      if (!direct_uses.empty() && direct_uses[i] == uses[i]) continue;  // every use reads the source
       f.opc = XI_LDIN; f.aux = (int32_t)i; f.a = -1;
     } else {
       f.opc = (uint8_t)o;
@@ -571,7 +672,27 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
     if (f.a >= 0) { in.ma = lsf.loc[f.a].mode; in.a = lsf.loc[f.a].idx; }
     else if (f.a_imm) { in.ma = M_IMM; in.a = 0; in.imm = f.a_val; }
     else { in.ma = M_NONE; in.a = kNone; }
-    if (f.opc == XI_CHAIN) {
+    if (f.opc == XI_DENSE) {
+      const DenseGroup& g = groups[f.chain];
+      in.a = (uint32_t)pl.dense.size();
+      in.ma = M_NONE;
+      in.mb = M_NONE;
+      in.md = M_NONE;
+      in.d = kNone;
+      in.save = kNone;
+      for (uint32_t k = 0; k < g.m; ++k) {
+        const Chain& ch = chains[g.c0 + k];
+        PDenseOut o{};
+        o.tb = ch.tb;
+        o.tn = ch.tn;
+        if (ch.acc0 >= 0) { o.am = lsf.loc[ch.acc0].mode; o.ai = lsf.loc[ch.acc0].idx; o.a_val = 0.0; }
+        else { o.am = M_IMM; o.ai = 0; o.a_val = ch.acc0_val; }
+        o.dm = lsf.loc[ch.last].mode;
+        o.di = lsf.loc[ch.last].idx;
+        o.save = traj[ch.last];
+        pl.dense.push_back(o);
+      }
+    } else if (f.opc == XI_CHAIN) {
       in.mb = M_NONE;
       in.b = chains[f.chain].tb;  // first term
     } else if (f.b >= 0) { in.mb = lsf.loc[f.b].mode; in.b = lsf.loc[f.b].idx; }
@@ -579,10 +700,12 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap) {
     else { in.mb = M_NONE; in.b = kNone; }
     pl.fwd.push_back(in);
   }
-  for (PTerm& pt : pl.terms) {
+  for (size_t q = 0; q < pl.terms.size(); ++q) {
+    PTerm& pt = pl.terms[q];
     pt.fxm = pt.fym = M_NONE;
     pt.fxi = pt.fyi = kNone;
-    if (pt.xs != kNone) { pt.fxm = lsf.loc[pt.xs].mode; pt.fxi = lsf.loc[pt.xs].idx; }
+    if (term_direct[q]) { pt.fxm = M_INPUT; pt.fxi = pt.xs; }
+    else if (pt.xs != kNone) { pt.fxm = lsf.loc[pt.xs].mode; pt.fxi = lsf.loc[pt.xs].idx; }
     if (pt.ys != kNone) { pt.fym = lsf.loc[pt.ys].mode; pt.fyi = lsf.loc[pt.ys].idx; }
     pt.rxm = pt.rym = M_NONE;
     pt.rxi = pt.ryi = kNone;
@@ -1065,6 +1188,68 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, bool f32, DevPro
     d.imm = in.imm;
     uint8_t opc = in.opc;
     const bool dsm = in.md == M_SMEM;
+    if (opc == XI_DENSE) {
+      const uint32_t first = in.a, m = (uint32_t)in.aux;
+      const PDenseOut& lead = p.dense[first];
+      const uint32_t n = lead.tn;
+      DIns h{};
+      h.opc = D_DENSE;
+      h.aux = (int32_t)m;
+      h.a = n;
+      h.ma = h.mb = h.md = M_NONE;
+      h.save = kNone;
+      out.fwd.push_back(h);
+      for (uint32_t k = 0; k < m; k += 2) {
+        DDenseInit r{};
+        for (uint32_t j = 0; j < 2 && k + j < m; ++j) {
+          const PDenseOut& o = p.dense[first + k + j];
+          r.mode[j] = o.am;
+          r.off[j] = o.am == M_IMM ? 0u : off(o.ai);
+          r.imm[j] = o.a_val;
+        }
+        out.fwd.push_back(as_record<DIns>(r));
+      }
+      const uint32_t per_rec = f32 ? 8u : 4u;
+      for (uint32_t q0 = 0; q0 < n; q0 += 4) {
+        DDenseOps ops{};
+        for (uint32_t j = 0; j < 4 && q0 + j < n; ++j) {
+          const PTerm& pt = p.terms[lead.tb + q0 + j];
+          ops.m[j] = pt.fxm;
+          ops.x[j] = pt.fxm == M_INPUT ? pt.fxi : off(pt.fxi);
+        }
+        out.fwd.push_back(as_record<DIns>(ops));
+        for (uint32_t q = q0; q < q0 + 4 && q < n; ++q) {
+          for (uint32_t k = 0; k < m; k += per_rec) {
+            unsigned char rec[32] = {};
+            for (uint32_t j = 0; j < per_rec && k + j < m; ++j) {
+              const double c = p.terms[p.dense[first + k + j].tb + q].c;
+              if (f32) {
+                const float fc = (float)c;
+                std::memcpy(rec + 4 * j, &fc, 4);
+              } else {
+                std::memcpy(rec + 8 * j, &c, 8);
+              }
+            }
+            DIns r;
+            std::memcpy(&r, rec, sizeof r);
+            out.fwd.push_back(r);
+          }
+        }
+      }
+      for (uint32_t k = 0; k < m; k += 2) {
+        DDenseFin r{};
+        for (uint32_t j = 0; j < 2; ++j) {
+          r.save[j] = kNone;
+          if (k + j >= m) continue;
+          const PDenseOut& o = p.dense[first + k + j];
+          r.md[j] = o.dm;
+          r.d[j] = off(o.di);
+          r.save[j] = off(o.save);
+        }
+        out.fwd.push_back(as_record<DIns>(r));
+      }
+      continue;
+    }
     if (opc == XI_CHAIN) {
       // the terms follow the instruction in the stream
       const uint32_t first = in.b, n = (uint32_t)in.aux;
@@ -1079,7 +1264,7 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, bool f32, DevPro
           for (uint32_t j = 0; j < 2 && k + j < n; ++j) {
             const PTerm& pt = p.terms[first + k + j];
             pr.c[j] = lc_c(pt.c);
-            pr.x[j] = off(pt.fxi);
+            pr.x[j] = pt.fxm == M_INPUT ? pt.fxi : off(pt.fxi);
             pr.m[j] = pt.fxm;
             pr.cx[j] = pt.kind == CK_CX ? 1 : 0;
           }

@@ -17,7 +17,11 @@ struct HostTape {
   std::vector<uint32_t> outs;
 };
 
-enum class Kind { Forward, Gradient, Hvp, Jvp, Taylor };
+// TaylorDirect: a Taylor program for launches whose input jets are (x, v, 0, ..)
+// with v from a direction source the kernel can evaluate per input (shared host
+// directions, device Rademacher, basis vectors): linear-combination terms over
+// inputs read the input jet at its source (M_INPUT) instead of a slot.
+enum class Kind { Forward, Gradient, Hvp, Jvp, Taylor, TaylorDirect };
 
 struct PlanStats {
   uint64_t fwd_ops = 0;        // tape ops executed per unit in the forward program
@@ -64,8 +68,22 @@ struct GRec {
 };
 static_assert(sizeof(GRec) == 32, "GRec must be 32 bytes");
 
+// One output of a dense group (XI_DENSE): a linear-combination chain whose
+// terms (tb .. tb+tn in Plan::terms) read the same operands in the same order
+// as every other output of the group.  Locations after allocation.
+struct PDenseOut {
+  uint32_t tb, tn;      // the chain's terms
+  uint8_t am, dm;       // modes of acc0 (M_SMEM / M_GLOB / M_IMM) and of the result
+  uint16_t pad;
+  uint32_t ai, di;      // register / slot indices
+  uint32_t save;        // trajectory slot of the result, or kNone
+  double a_val;         // acc0 when am == M_IMM
+};
+static_assert(sizeof(PDenseOut) == 32, "PDenseOut must be 32 bytes");
+
 struct Plan {
   std::vector<PTerm> terms;  // fused-chain terms, shared by both programs
+  std::vector<PDenseOut> dense;  // outputs of dense groups (XI_DENSE: a = first, aux = count)
   std::vector<GRec> gathers; // reverse gather records (XI_GATHER: va = first header, aux = targets)
   std::vector<Ins> fwd;
   std::vector<RIns> rev;
@@ -77,7 +95,9 @@ struct Plan {
 };
 
 // Builds the programs for `kind` with at most `smem_cap` shared registers.
-Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap);
+// `dense_max` > 1 groups up to that many consecutive linear-combination chains
+// over one operand list into one XI_DENSE instruction (1: no groups).
+Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap, uint32_t dense_max = 1);
 
 // Device encoding of a plan for a launch geometry (`tile` points per CTA,
 // `vbytes` bytes per slot value).  Returns false (with `err`) if an offset does

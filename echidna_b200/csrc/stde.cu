@@ -83,6 +83,81 @@ __global__ void stde_reduce_kernel(const T* c0, const T* ck, T scale, uint64_t n
   out[p] = r;
 }
 
+// Neumaier's compensated summation (Neumaier, 1974): the running sum s plus
+// the accumulated rounding errors c.
+template <class T>
+struct Neumaier {
+  T s = T(0), c = T(0);
+  __device__ __forceinline__ void add(T x) {
+    const T t = s + x;
+    if (fabs(s) >= fabs(x)) c = c + ((s - t) + x);
+    else c = c + ((x - t) + s);
+    s = t;
+  }
+  __device__ __forceinline__ T value() const { return s + c; }
+};
+
+// The batch extension's compensated FP32 reduction, one thread per point: the
+// mean of the finite samples from a compensated sum, then the corrected
+// two-pass variance (Chan, Golub and LeVeque, 1983) from compensated sums of
+// the deviations and of their squares.  Count, NaN mean at count 0, the clamp
+// at 0 and the standard error are as in the Welford reduction.
+template <class T>
+__global__ void stde_reduce_comp_kernel(const T* c0, const T* ck, T scale, uint64_t npoints, uint32_t S,
+                                        const T* wmul, ech_estimator_result* out) {
+  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npoints) return;
+  Neumaier<T> sum;
+  uint64_t count = 0;
+  for (uint32_t s = 0; s < S; ++s) {
+    T x = scale * ck[p * S + s];
+    if (wmul) x = x * wmul[p * S + s];
+    if (!isfinite(x)) continue;
+    sum.add(x);
+    count += 1;
+  }
+  ech_estimator_result r;
+  r.value = (double)c0[p * S];
+  r.num_samples = count;
+  if (count == 0) {
+    r.estimate = __longlong_as_double(0x7ff8000000000000ll);
+    r.sample_variance = 0.0;
+    r.standard_error = 0.0;
+    out[p] = r;
+    return;
+  }
+  const T nf = (T)count;
+  const T mean = sum.value() / nf;
+  T var = T(0);
+  if (count > 1) {
+    Neumaier<T> dev, sq;
+    for (uint32_t s = 0; s < S; ++s) {
+      T x = scale * ck[p * S + s];
+      if (wmul) x = x * wmul[p * S + s];
+      if (!isfinite(x)) continue;
+      const T d = x - mean;
+      dev.add(d);
+      sq.add(d * d);
+    }
+    const T dv = dev.value();
+    var = fmax((sq.value() - dv * dv / nf) / (nf - T(1)), T(0));
+  }
+  r.estimate = (double)mean;
+  r.sample_variance = (double)var;
+  r.standard_error = (double)sqrt(var / nf);
+  out[p] = r;
+}
+
+cudaError_t launch_stde_reduce_comp(const void* c0, const void* ck, double scale, uint64_t npoints, uint32_t S,
+                                    const void* wmul, void* results, cudaStream_t st) {
+  const int threads = 128;
+  const unsigned blocks = (unsigned)((npoints + threads - 1) / threads);
+  if (blocks == 0) return cudaSuccess;
+  stde_reduce_comp_kernel<float><<<blocks, threads, 0, st>>>((const float*)c0, (const float*)ck, (float)scale, npoints,
+                                                             S, (const float*)wmul, (ech_estimator_result*)results);
+  return cudaGetLastError();
+}
+
 // stde_sparse (src/stde/sparse.rs:37-78), per point: for each sampled entry e
 // in order, raw = c_{k_e} * prefactor_e and sample = sign_e * Z * raw, Welford in
 // the sample type; the value is c0 of the point's last sample.  Coefficients

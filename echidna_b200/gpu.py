@@ -226,6 +226,14 @@ class CudaContext:
     def set_launch(self, threads: int = 0, points_per_thread: int = 0, smem_reg_cap: int = 0):
         _check(_lib.load().ech_ctx_set_launch(self._h, threads, points_per_thread, smem_reg_cap))
 
+    FP32_COMPENSATED_JETS, FP32_COMPENSATED_MEANS, FP32_PLAIN_MEANS = 1, 2, 4
+
+    def set_fp32_mode(self, flags: int = 0):
+        """FP32 options of the batch STDE calls (``ech_ctx_set_fp32_mode``): compensated
+        linear chains in the jet sweep, and FP32 compensated or plain per-point means
+        instead of the FP64 Welford reduction."""
+        _check(_lib.load().ech_ctx_set_fp32_mode(self._h, int(flags)))
+
     def set_autotune(self, enable: bool):
         _check(_lib.load().ech_ctx_set_autotune(self._h, 1 if enable else 0))
 
@@ -238,7 +246,7 @@ class CudaContext:
         return dict(zip(keys, [int(v) for v in buf]))
 
     def plan_stats(self, tape: _TapeHandle, kind: str, order: int = 0) -> dict:
-        kinds = {"forward": 0, "gradient": 1, "hvp": 2, "tangent": 3, "taylor": 4}
+        kinds = {"forward": 0, "gradient": 1, "hvp": 2, "tangent": 3, "taylor": 4, "taylor_direct": 5}
         buf = (ctypes.c_uint64 * 12)()
         _check(_lib.load().ech_tape_plan_stats(self._h, tape._h, kinds[kind], order, int(tape.f64), buf))
         keys = ["fwd_ops", "rev_ops", "max_live_fwd", "max_live_rev", "traj_values", "flops_fwd", "flops_rev",

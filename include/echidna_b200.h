@@ -416,8 +416,26 @@ ECH_API ech_status ech_column_coloring(uint32_t num_outputs, uint32_t num_inputs
 ECH_API ech_status ech_row_coloring(uint32_t num_outputs, uint32_t num_inputs, const uint32_t* rows,
                                     const uint32_t* cols, size_t nnz, uint32_t* colors, uint32_t* num_colors);
 
+/* ── FP32 precision options of the batch STDE calls (extension) ─────────────
+ * Flags for ech_ctx_set_fp32_mode, applied to the FP32 calls of
+ * ech_laplacian_batch_f32 / ech_laplacian_batch_device (the drop-in
+ * laplacian_gpu family keeps the reference's rounding and f32 Welford):
+ *   ECH_FP32_COMPENSATED_JETS   the jet sweep sums linear combinations with
+ *                               Neumaier-compensated additions per coefficient
+ *   ECH_FP32_COMPENSATED_MEANS  per-point mean and variance in FP32 from
+ *                               compensated sums (corrected two-pass variance)
+ *   ECH_FP32_PLAIN_MEANS        per-point FP32 Welford, uncompensated
+ * 0 (the default): reference rounding in the sweep, FP64 Welford per point.
+ * The two MEANS flags exclude each other. */
+#define ECH_FP32_COMPENSATED_JETS 1u
+#define ECH_FP32_COMPENSATED_MEANS 2u
+#define ECH_FP32_PLAIN_MEANS 4u
+ECH_API ech_status ech_ctx_set_fp32_mode(ech_ctx* ctx, uint32_t flags);
+
 /* ── introspection ────────────────────────────────────────────────────────── */
-/* kind: 0 forward, 1 gradient, 2 hvp, 3 tangent, 4 taylor(order).  Fills
+/* kind: 0 forward, 1 gradient, 2 hvp, 3 tangent, 4 taylor(order), 5 taylor with
+ * linear combinations of inputs read at their source (the program that
+ * point-direction jet launches with shared, Rademacher or basis directions run).  Fills
  * stats[12]: fwd_ops, rev_ops, max_live_fwd, max_live_rev, traj_values,
  * flops_fwd, flops_rev, specials_fwd, specials_rev, smem_regs, far_slots,
  * n_instructions. */
@@ -425,16 +443,18 @@ ECH_API ech_status ech_tape_plan_stats(ech_ctx* ctx, const ech_tape* tape, int k
                                        uint64_t* stats);
 /* Host-only lowering dump (no device needed): the forward / reverse programs
  * (32-byte records) and constant pool for `kind` with `smem_reg_cap` shared
- * registers, plus the fused-chain terms (48-byte records) and the reverse
- * gather records (32-byte).  counts[8]: n_fwd, n_rev, n_pool, smem_regs,
- * far_slots, traj_slots, n_terms, n_gather_records.  Used to check the
- * lowering on machines without a GPU. */
+ * registers, plus the fused-chain terms (48-byte records), the reverse
+ * gather records (32-byte) and the outputs of dense groups (32-byte records;
+ * groups of up to `dense_max` chains, 1 = none).  counts[9]: n_fwd, n_rev,
+ * n_pool, smem_regs, far_slots, traj_slots, n_terms, n_gather_records,
+ * n_dense_outputs.  Used to check the lowering on machines without a GPU. */
 ECH_API ech_status ech_plan_dump(const uint32_t* opcodes, const uint32_t* arg0, const uint32_t* arg1,
                                  const double* values, uint32_t num_variables, uint32_t num_inputs,
                                  uint32_t output_index, const uint32_t* output_indices, uint32_t n_output_indices,
                                  int kind, uint32_t smem_reg_cap, void* fwd, size_t fwd_cap, void* rev,
                                  size_t rev_cap, double* pool, size_t pool_cap, void* terms, size_t terms_cap,
-                                 void* gathers, size_t gathers_cap, uint64_t* counts);
+                                 void* gathers, size_t gathers_cap, void* dense, size_t dense_cap,
+                                 uint32_t dense_max, uint64_t* counts);
 /* Launch configuration override for tuning (0 = automatic): threads per CTA,
  * points per thread and the shared-register cap. */
 ECH_API ech_status ech_ctx_set_launch(ech_ctx* ctx, uint32_t threads, uint32_t points_per_thread,

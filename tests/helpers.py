@@ -7,6 +7,7 @@ import math
 import numpy as np
 
 from echidna_b200 import constant, record
+from echidna_b200.rng import philox_bits  # noqa: F401  (re-exported for the tests)
 
 
 def ulp_diff(a, b, dtype=np.float64):
@@ -103,3 +104,4 @@ def rosenbrock_2(v):
     dx = v[0] - one
     t = v[1] - v[0] * v[0]
     return dx * dx + hundred * t * t
+

@@ -19,34 +19,37 @@ INS = struct.Struct("<BBBBIIIIid")
 RINS = struct.Struct("<BBHIIIIIIi")
 TERM = struct.Struct("<BBHIIBBBBIIIIIId")   # PTerm, 48 bytes
 GREC = struct.Struct("<IIHBBIdQ")            # GRec, 32 bytes
+DOUT = struct.Struct("<IIBBHIIId")           # PDenseOut, 32 bytes
 XI_LDIN, XI_STOUT, XI_MOV, XI_SEED, XI_STGRAD, XI_CHAIN = 64, 65, 66, 67, 68, 69
-XI_NORM, XI_GATHER = 84, 85
+XI_NORM, XI_GATHER, XI_DENSE = 84, 85, 86
 CK_X, CK_CX, CK_XC, CK_XY, CK_C = range(5)
 CF = dict(X_INIT=1, Y_INIT=2, X_GLOB=4, Y_GLOB=8, X_ADJ=16, Y_ADJ=32)
 M_SMEM, M_GLOB, M_IMM, M_NONE = 0, 1, 2, 3
 NONE = 0xFFFFFFFF
 RF = dict(R_GLOB=1, A_GLOB=2, B_GLOB=4, A_INIT=8, B_INIT=16, VA_IMM=32, VB_IMM=64, HAS_A=128, HAS_B=256)
-KIND = {"forward": 0, "gradient": 1, "hvp": 2, "tangent": 3, "taylor": 4}
+KIND = {"forward": 0, "gradient": 1, "hvp": 2, "tangent": 3, "taylor": 4, "taylor_direct": 5}
 
 
-def plan_dump(tape, kind: str, cap: int):
+def plan_dump(tape, kind: str, cap: int, dense_max: int = 16):
     lib = _lib.load()
     op, a0, a1, vals = tape.arrays()
     vals = np.ascontiguousarray(vals, dtype=np.float64)
     outs = np.asarray(tape.output_indices, dtype=np.uint32)
-    counts = (ctypes.c_uint64 * 8)()
+    counts = (ctypes.c_uint64 * 9)()
     args = [_lib.ptr(op), _lib.ptr(a0), _lib.ptr(a1), _lib.ptr(vals), len(op), tape.num_inputs, tape.output_index,
             _lib.ptr(outs), len(outs), KIND[kind], cap]
-    st = lib.ech_plan_dump(*args, None, 0, None, 0, None, 0, None, 0, None, 0, counts)
+    st = lib.ech_plan_dump(*args, None, 0, None, 0, None, 0, None, 0, None, 0, None, 0, dense_max, counts)
     assert st == 0, _lib.last_error()
-    nf, nr, npool, nt, ng = counts[0], counts[1], counts[2], counts[6], counts[7]
+    nf, nr, npool, nt, ng, nd = counts[0], counts[1], counts[2], counts[6], counts[7], counts[8]
+    db = ctypes.create_string_buffer(max(nd, 1) * 32)
     gb = ctypes.create_string_buffer(max(ng, 1) * 32)
     fb = ctypes.create_string_buffer(max(nf, 1) * 32)
     rb = ctypes.create_string_buffer(max(nr, 1) * 32)
     tb = ctypes.create_string_buffer(max(nt, 1) * 48)
     pool = np.zeros(max(npool, 1), dtype=np.float64)
     st = lib.ech_plan_dump(*args, ctypes.addressof(fb), nf, ctypes.addressof(rb), nr, _lib.ptr(pool), npool,
-                           ctypes.addressof(tb), nt, ctypes.addressof(gb), ng, counts)
+                           ctypes.addressof(tb), nt, ctypes.addressof(gb), ng, ctypes.addressof(db), nd, dense_max,
+                           counts)
     assert st == 0, _lib.last_error()
     fwd = [INS.unpack_from(fb, 32 * k) for k in range(nf)]
     rev = [RINS.unpack_from(rb, 32 * k) for k in range(nr)]
@@ -59,8 +62,12 @@ def plan_dump(tape, kind: str, cap: int):
     for k in range(ng):
         s, n, flags, mode, _pad, idx, c, _p2 = GREC.unpack_from(gb, 32 * k)
         gathers.append(dict(s=s, n=n, flags=flags, mode=mode, idx=idx, c=c))
+    dense = []
+    for k in range(nd):
+        tb_, tn, am, dm, _pad, ai, di, save, a_val = DOUT.unpack_from(db, 32 * k)
+        dense.append(dict(tb=tb_, tn=tn, am=am, dm=dm, ai=ai, di=di, save=save, a_val=a_val))
     return fwd, rev, pool, dict(smem_regs=counts[3], far_slots=counts[4], traj_slots=counts[5], terms=terms,
-                                gathers=gathers)
+                                gathers=gathers, dense=dense)
 
 
 def _fwd(op, a, b, aux):
@@ -117,9 +124,9 @@ def _partials(op, a, b, r, aux):
     raise NotImplementedError(OpCode(op).name)
 
 
-def run_gradient(tape, X, cap):
+def run_gradient(tape, X, cap, dense_max: int = 16):
     """Emulates the gradient programs; returns (outputs, grads)."""
-    fwd, rev, pool, info = plan_dump(tape, "gradient", cap)
+    fwd, rev, pool, info = plan_dump(tape, "gradient", cap, dense_max)
     terms = info["terms"]
     X = np.asarray(X, dtype=np.float64)
     B = X.shape[0]
@@ -141,6 +148,22 @@ def run_gradient(tape, X, cap):
             continue
         elif opc == XI_MOV:
             v = ld(ma, a, imm)
+        elif opc == XI_DENSE:
+            # every output's chain over the shared operands, results written
+            # only after all operands are read (as the kernel does)
+            results = []
+            for o in info["dense"][a:a + aux]:
+                acc = ld(o["am"], o["ai"], o["a_val"])
+                for tm in terms[o["tb"]:o["tb"] + o["tn"]]:
+                    x = regs[tm["fxm"]][tm["fxi"]]
+                    with np.errstate(all="ignore"):
+                        acc = acc + (tm["c"] * x if tm["kind"] == CK_CX else x * tm["c"])
+                results.append((o, acc))
+            for o, acc in results:
+                regs[o["dm"]][o["di"]] = acc
+                if o["save"] != NONE:
+                    traj[o["save"]] = acc
+            continue
         elif opc == XI_CHAIN:
             acc = ld(ma, a, imm)
             for tm in terms[b:b + aux]:

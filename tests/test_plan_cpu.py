@@ -49,12 +49,13 @@ def _tapes():
     yield "unused_input", record(lambda v: v[0].sin() * v[0], [2.0, 5.0])[0]
 
 
+@pytest.mark.parametrize("dense_max", [1, 2, 16])
 @pytest.mark.parametrize("cap", [1, 2, 3, 8, 4096])
 @pytest.mark.parametrize("name,tape", list(_tapes()))
-def test_lowered_gradient_matches_oracle(name, tape, cap):
+def test_lowered_gradient_matches_oracle(name, tape, cap, dense_max):
     rng = np.random.default_rng(3)
     X = rng.uniform(-1.5, 1.5, size=(7, tape.num_inputs))
-    out, grad = run_gradient(tape, X, cap)
+    out, grad = run_gradient(tape, X, cap, dense_max)
     o = OracleTape(tape)
     ref_out, ref_grad = o.gradient(X)
     np.testing.assert_array_equal(out, ref_out)
@@ -76,6 +77,14 @@ def test_register_caps_respected(cap):
                 assert i < info["far_slots"]
         if save != 0xFFFFFFFF:
             assert save < info["traj_slots"]
+    for o in info["dense"]:
+        for m, i in ((o["am"], o["ai"]), (o["dm"], o["di"])):
+            if m == 0:
+                assert i < info["smem_regs"]
+            elif m == 1:
+                assert i < info["far_slots"]
+        if o["save"] != 0xFFFFFFFF:
+            assert o["save"] < info["traj_slots"]
 
 
 def test_mlp_trajectory_is_three_layers_of_width():
@@ -97,3 +106,33 @@ def test_dense_layers_reverse_as_gathers():
         headers.append(info["gathers"][q])
         q += 1 + info["gathers"][q]["n"]
     assert sorted(h["n"] for h in headers) == [8] * 16
+
+
+@pytest.mark.parametrize("dense_max,groups", [(16, 8), (8, 16), (2, 64), (1, 0)])
+def test_mlp_dense_layers_become_groups(dense_max, groups):
+    # each width-64 layer's 64 dot products read the same 64 operands: groups of
+    # dense_max chains (one forward instruction each), nothing else grouped
+    tape = configs.mlp(64, 64)
+    fwd, _, _, info = plan_dump(tape, "gradient", 4096, dense_max)
+    dense = [ins for ins in fwd if ins[0] == 86]
+    assert len(dense) == groups
+    assert sum(ins[8] for ins in dense) == (128 if groups else 0)
+    assert all(ins[8] <= dense_max for ins in dense)
+
+
+def test_dense_group_waits_for_acc0_defined_later():
+    # the second dot product's constant term is an earlier result computed after
+    # the first dot product starts: it cannot join the group
+    def f(v):
+        a = constant(0.5) + 2.0 * v[0] + 3.0 * v[1]
+        t = a.sin()
+        b = t + 4.0 * v[0] + 5.0 * v[1]
+        return a * b
+    tape = record(f, [0.1, 0.2])[0]
+    fwd, _, _, info = plan_dump(tape, "gradient", 4096, 16)
+    assert not any(ins[0] == 86 for ins in fwd)
+    X = np.random.default_rng(4).uniform(-1, 1, size=(5, 2))
+    out, grad = run_gradient(tape, X, 4096, 16)
+    ref_out, ref_grad = OracleTape(tape).gradient(X)
+    np.testing.assert_array_equal(out, ref_out)
+    np.testing.assert_array_equal(grad, ref_grad)
