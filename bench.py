@@ -73,6 +73,17 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+def _cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle-reason samples during the timed region."""
 
@@ -798,7 +809,8 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
         "data": "synthetic", "scaling": "weak", "vs_baseline": None, "config": cfg,
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample,
+                         "cpu_model": _cpu_model()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     if detail:
@@ -969,7 +981,10 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         nth = os.cpu_count() or 1
         v, sample = wl.cpu_reference(10.0, nth)
-        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample}
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample,
+                                "cpu_model": _cpu_model()}
+        v1, sample1 = wl.cpu_reference(3.0, 1)
+        line["cpu_baseline"]["single_thread"] = {"value": v1, "sample": sample1}
         if dtype == "f32" and "dtype" in wl.cpu_reference.__code__.co_varnames:
             # the same CPU path in FP32, so the FP32 GPU figure has a same-precision CPU number beside it
             v32, sample32 = wl.cpu_reference(5.0, nth, dtype=np.float32)

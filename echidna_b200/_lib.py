@@ -11,7 +11,9 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libechidna_b200.so")
+# ECHIDNA_B200_VARIANT=bounds selects the device bounds-checked build of the same engine
+LIB_PATH = os.path.join(_HERE, "libechidna_b200_bounds.so" if os.environ.get("ECHIDNA_B200_VARIANT") == "bounds"
+                        else "libechidna_b200.so")
 
 
 class EngineNotBuilt(RuntimeError):

@@ -5,6 +5,11 @@ Every CUDA translation unit is compiled for sm_100a only
 ``a*b+c`` rounds like the reference's CPU sweeps, then linked with the host
 lowering (plan.cpp) into one library that exports the C ABI of
 ``include/echidna_b200.h``.  Compilation is incremental on file timestamps.
+
+``build(variant="bounds")`` builds ``libechidna_b200_bounds.so`` with
+``-DECH_DEVICE_BOUNDS``: the same engine with every slot access and every
+input / output index checked on the device (``ECHIDNA_B200_VARIANT=bounds``
+makes ``echidna_b200._lib`` load it).
 """
 from __future__ import annotations
 
@@ -20,6 +25,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libechidna_b200.so")
+VARIANTS = {"": (BUILD, LIB, []),
+            "bounds": (os.path.join(HERE, "_build_bounds"), os.path.join(HERE, "libechidna_b200_bounds.so"),
+                       ["-DECH_DEVICE_BOUNDS"])}
 
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -67,33 +75,33 @@ def _compile(cmd):
     return r.stdout + r.stderr
 
 
-def build(verbose: bool = False, jobs: int | None = None) -> str:
-    os.makedirs(BUILD, exist_ok=True)
+def build(verbose: bool = False, jobs: int | None = None, variant: str = "") -> str:
+    build_dir, lib, extra = VARIANTS[variant]
+    os.makedirs(build_dir, exist_ok=True)
     cmds, objs = [], []
     for s in CU_SOURCES:
         src = os.path.join(CSRC, s)
-        obj = os.path.join(BUILD, s + ".o")
+        obj = os.path.join(build_dir, s + ".o")
         objs.append(obj)
         if _newer(src, obj, _deps(src)):
-            cmds.append([NVCC, *ARCH, *NVFLAGS, "-c", src, "-o", obj])
+            cmds.append([NVCC, *ARCH, *NVFLAGS, *extra, "-c", src, "-o", obj])
     for s in CXX_SOURCES:
         src = os.path.join(CSRC, s)
-        obj = os.path.join(BUILD, s + ".o")
+        obj = os.path.join(build_dir, s + ".o")
         objs.append(obj)
         if _newer(src, obj, _deps(src)):
-            cmds.append(["g++", *CXXFLAGS, "-c", src, "-o", obj])
+            cmds.append(["g++", *CXXFLAGS, *extra, "-c", src, "-o", obj])
     if cmds:
         with cf.ThreadPoolExecutor(max_workers=jobs or min(8, os.cpu_count() or 4)) as ex:
             for out in ex.map(_compile, cmds):
                 if verbose and out.strip():
                     print(out)
-    if cmds or not os.path.exists(LIB):
-        tmp = LIB + ".tmp"
+    if cmds or not os.path.exists(lib):
+        tmp = lib + ".tmp"
         _compile([NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lpthread"])
-        os.replace(tmp, LIB)
-    return LIB
+        os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":
-    build(verbose="-v" in sys.argv)
-    print(LIB)
+    print(build(verbose="-v" in sys.argv, variant="bounds" if "--bounds" in sys.argv else ""))

@@ -349,17 +349,20 @@ static LaunchCfg choose_cfg(ech_ctx* ctx, const ech_tape* t, int kind, int K) {
   return cfg_for(ctx, t, kind, K, sh);
 }
 
+// `dense`: form dense groups (up to dense_group_max(vbytes, P) chains); launches
+// with compensated jet chains use plans without them.
 static ech_status get_plan(ech_tape* t, int kind, int K, uint32_t cap, uint32_t tile, uint32_t vbytes, uint32_t P,
-                           DevPlan** out) {
+                           bool dense, DevPlan** out) {
   std::lock_guard<std::mutex> lk(t->mu);
-  auto key = std::make_tuple(kind, K, cap, tile, vbytes, P);
+  const uint32_t dmax = dense ? dense_group_max(vbytes, P) : 1u;
+  auto key = std::make_tuple(kind, K, cap, tile, vbytes, dmax);
   auto it = t->plans.find(key);
   if (it != t->plans.end()) {
     *out = it->second.get();
     return ECH_OK;
   }
   std::unique_ptr<DevPlan> dp(new DevPlan());
-  dp->host = build_plan(t->host, kind_of(kind), cap, dense_group_max(vbytes, P));
+  dp->host = build_plan(t->host, kind_of(kind), cap, dmax);
   DevProgram prog;
   std::string err;
   if (!encode_plan(dp->host, tile, vbytes, !t->f64, prog, err)) return fail(ECH_ERR_OTHER, err);
@@ -412,7 +415,8 @@ static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_
     c.cap = c.cap > reserve ? c.cap - reserve : 1;
   }
   DevPlan* dp = nullptr;
-  ech_status s = get_plan(t, direct ? 5 : kind, K, c.cap, c.tile, (uint32_t)c.vbytes, (uint32_t)c.req.P, &dp);
+  ech_status s = get_plan(t, direct ? 5 : kind, K, c.cap, c.tile, (uint32_t)c.vbytes, (uint32_t)c.req.P,
+                          io.compensated == 0, &dp);
   if (s != ECH_OK) return s;
   const Plan& p = dp->host;
   const uint32_t regs = std::max<uint32_t>(p.smem_regs, 1);
@@ -432,6 +436,7 @@ static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_
   kp.rev = dp->d_rev;
   kp.n_rev = c.req.rev ? dp->n_rev : 0u;
   kp.far_slots = p.far_slots;
+  kp.traj_slots = p.traj_slots;
   kp.smem_regs = regs;
   kp.traj_smem = traj_smem ? 1u : 0u;
   kp.tile = c.tile;
@@ -712,6 +717,7 @@ static ech_status check_err_word(ech_ctx* ctx) {
   if (h) {
     CU(cudaMemset(ctx->d_err, 0, sizeof(uint32_t)));
     if (h & KERR_TIMEOUT) return fail(ECH_ERR_TIMEOUT, "device-side wait timed out");
+    if (h & KERR_BOUNDS) return fail(ECH_ERR_OTHER, "device bounds check failed: a slot or index out of its region");
     return fail(ECH_ERR_OTHER, "device reported a malformed instruction");
   }
   return ECH_OK;
@@ -2080,7 +2086,7 @@ static ech_status multi_prepare(ech_multi* m, Shape sh) {
     if (it.n_points == 0) continue;
     ech_tape* t = const_cast<ech_tape*>(it.tape);
     DevPlan* dp = nullptr;
-    CHECK(get_plan(t, 2, 0, c.cap, c.tile, (uint32_t)c.vbytes, (uint32_t)c.req.P, &dp));
+    CHECK(get_plan(t, 2, 0, c.cap, c.tile, (uint32_t)c.vbytes, (uint32_t)c.req.P, true, &dp));
     const Plan& p = dp->host;
     regs = std::max<uint32_t>(regs, p.smem_regs);
     slots = std::max<uint64_t>(slots, (uint64_t)p.far_slots + p.traj_slots);
@@ -2091,6 +2097,7 @@ static ech_status multi_prepare(ech_multi* m, Shape sh) {
     kp.rev = dp->d_rev;
     kp.n_rev = dp->n_rev;
     kp.far_slots = p.far_slots;
+    kp.traj_slots = p.traj_slots;
     kp.tile = c.tile;
     kp.n_units = it.n_points;
     kp.ni = t->host.ni;

@@ -236,6 +236,7 @@ constexpr int kRingBytes = kStages * kChunk * 48;  // sized for the larger recor
 enum KErr : uint32_t {
   KERR_TIMEOUT = 1u << 0,     // a bounded wait gave up
   KERR_BADINS = 1u << 1,      // malformed instruction
+  KERR_BOUNDS = 1u << 2,      // (checked build) a slot or index out of its region
 };
 
 }  // namespace ech

@@ -59,10 +59,44 @@ struct KParams {
   const void* seed_items;    // SlotSeed records
   uint32_t dir_bits;         // dir_mode 2 with input-direct terms: byte offset in shared memory of the
                              // tile's direction signs, [ceil(ni/32) words][tile units] (0: none)
+  uint32_t traj_slots;       // trajectory slots (bounds of the checked build)
   uint32_t compensated;      // order-3 jets: Neumaier-compensated additions in fused chains (an FP32
                              // option of the batch Laplacian; results then differ from the
                              // reference's rounding)
 };
+
+// ───────────────────────────── device bounds checks ─────────────────────────
+// Built with ECH_DEVICE_BOUNDS (the library variant libechidna_b200_bounds.so),
+// every slot access of the sweeps checks its offset against its region (shared
+// registers, global far slots, trajectory) and every input / output / gradient
+// index against the unit's sizes.  An access out of its region sets KERR_BOUNDS
+// in the error word and goes to the thread's first shared register instead (no
+// fault); ech_ctx_synchronize reports it.  Without the macro the checks compile
+// to plain pointer arithmetic.
+#ifdef ECH_DEVICE_BOUNDS
+constexpr bool kBoundsChecked = true;
+#else
+constexpr bool kBoundsChecked = false;
+#endif
+__device__ __forceinline__ unsigned char* bounded(unsigned char* base, uint32_t off, uint64_t limit,
+                                                  unsigned char* fallback, uint32_t* err) {
+  if constexpr (kBoundsChecked) {
+    if ((uint64_t)off >= limit) {
+      atomicOr(err, (uint32_t)KERR_BOUNDS);
+      return fallback;
+    }
+  }
+  return base + off;
+}
+__device__ __forceinline__ bool index_ok(uint32_t i, uint32_t n, uint32_t* err) {
+  if constexpr (kBoundsChecked) {
+    if (i >= n) {
+      atomicOr(err, (uint32_t)KERR_BOUNDS);
+      return false;
+    }
+  }
+  return true;
+}
 
 // ───────────────────────────── bounded mbarrier waits ───────────────────────
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -464,9 +498,34 @@ template <class V, int P> struct FwdExec {
   const void* vrow[P];   // dir_mode 1: the unit's direction row
   uint32_t sel[P];       // dir_mode 3 / 4: the coordinate of the basis direction
 
+  // slot addresses (bounds-checked in the checked build; plain pointer
+  // arithmetic otherwise)
+#ifdef ECH_DEVICE_BOUNDS
+  __device__ __forceinline__ uint64_t row_bytes() const { return (uint64_t)kp.tile * sizeof(V); }
+  __device__ __forceinline__ unsigned char* sp(uint32_t off) const {
+    return bounded(sm, off, (uint64_t)kp.smem_regs * row_bytes(), sm, kp.err);
+  }
+  __device__ __forceinline__ unsigned char* gp(uint32_t off) const {
+    return bounded(gs, off, (uint64_t)kp.far_slots * row_bytes(), sm, kp.err);
+  }
+  __device__ __forceinline__ unsigned char* tp(uint32_t off) const {
+    return bounded(tj, off, (uint64_t)kp.traj_slots * row_bytes(), sm, kp.err);
+  }
+  __device__ __forceinline__ unsigned char* vp(uint32_t mode, uint32_t off) const {
+    return mode == M_GLOB ? gp(off) : sp(off);
+  }
+#else
+  __device__ __forceinline__ unsigned char* sp(uint32_t off) const { return sm + off; }
+  __device__ __forceinline__ unsigned char* gp(uint32_t off) const { return gs + off; }
+  __device__ __forceinline__ unsigned char* tp(uint32_t off) const { return tj + off; }
+  __device__ __forceinline__ unsigned char* vp(uint32_t mode, uint32_t off) const {
+    return (mode == M_GLOB ? gs : sm) + off;
+  }
+#endif
+
   __device__ __forceinline__ void ld(uint32_t mode, uint32_t off, double imm, V (&v)[P]) const {
-    if (mode == M_SMEM) C::ld(sm + off, v);
-    else if (mode == M_GLOB) C::ld(gs + off, v);
+    if (mode == M_SMEM) C::ld(sp(off), v);
+    else if (mode == M_GLOB) C::ld(gp(off), v);
     else {
       const V c = dm::VT<V>::cst(imm);
 #pragma unroll
@@ -474,17 +533,17 @@ template <class V, int P> struct FwdExec {
     }
   }
   __device__ __forceinline__ void put(uint32_t md, uint32_t d, uint32_t save, const V (&r)[P]) const {
-    if (md == M_SMEM) C::st(sm + d, r);
-    else if (md == M_GLOB) C::st(gs + d, r);
-    if (save != kNone) C::st(tj + save, r);
+    if (md == M_SMEM) C::st(sp(d), r);
+    else if (md == M_GLOB) C::st(gp(d), r);
+    if (save != kNone) C::st(tp(save), r);
   }
   __device__ __forceinline__ void put_sm(uint32_t d, uint32_t save, const V (&r)[P]) const {
-    C::st(sm + d, r);
-    if (save != kNone) C::st(tj + save, r);
+    C::st(sp(d), r);
+    if (save != kNone) C::st(tp(save), r);
   }
 
   __device__ __forceinline__ void ldv(uint32_t mode, uint32_t off, V (&v)[P]) const {
-    C::ld((mode == M_GLOB ? gs : sm) + off, v);
+    C::ld(vp(mode, off), v);
   }
 
   // Fused chain s_t = s_{t-1} (+|-) term_t, t = 1..n, s_0 = acc0: the same
@@ -701,6 +760,7 @@ template <class V, int P> struct FwdExec {
       v = T(0);
       return;
     }
+    if (!index_ok(i, kp.ni, kp.err)) i = 0;
     x0 = reinterpret_cast<const T*>(xrow[p])[i];
     if (kp.dir_mode == 2) v = ((bits[(i >> 5) * kp.tile + p] >> (i & 31u)) & 1u) ? T(1) : T(-1);
     else if (kp.dir_mode == 1) v = reinterpret_cast<const T*>(vrow[p])[i];
@@ -729,6 +789,13 @@ template <class V, int P> struct FwdExec {
   // Operand j of a linear-combination term record into x: a slot load, or the
   // input jet at its source (returns true for M_INPUT).
   __device__ __forceinline__ bool lc_jet_operand(uint32_t mode, uint32_t off, V (&x)[P]) const {
+    if constexpr (kBoundsChecked) {
+      if (mode != M_INPUT && mode != M_SMEM && mode != M_GLOB) {
+        atomicOr(kp.err, (uint32_t)KERR_BOUNDS);
+        mode = M_SMEM;
+        off = 0;
+      }
+    }
     if (mode == M_INPUT) {
 #pragma unroll
       for (int p = 0; p < P; ++p) {
@@ -859,13 +926,10 @@ template <class V, int P> struct FwdExec {
       ring_drain(*st.rg);
       return false;
     } else {
-      if constexpr (JetOrder<V>::K == 3) {
-        if (kp.compensated) return dense_impl<true>(st, m, n);
-      }
-      return dense_impl<false>(st, m, n);
+      // (launches with compensated chains run plans without dense groups)
+      return dense_impl(st, m, n);
     }
   }
-  template <bool COMP>
   __device__ __forceinline__ bool dense_impl(Stream<32>& st, uint32_t m, uint32_t n) const {
     using T = typename dm::VT<V>::S;
     constexpr int MX = kDenseMax > 1 ? kDenseMax : 2;
@@ -888,7 +952,7 @@ template <class V, int P> struct FwdExec {
         if ((uint32_t)jj + 1 < m) ld((w.z >> 8) & 0xFFu, w.y, imm.y, acc[jj + 1]);
       }
     }
-    T z[P][KJ], cmp[COMP ? MX : 1][P][KJ];
+    T z[P][KJ];
     if constexpr (JetOrder<V>::K > 0) {
 #pragma unroll
       for (int p = 0; p < P; ++p)
@@ -899,10 +963,7 @@ template <class V, int P> struct FwdExec {
 #pragma unroll
         for (int p = 0; p < P; ++p)
 #pragma unroll
-          for (int k = 0; k < KJ; ++k) {
-            acc[j][p].c[k] = acc[j][p].c[k] + T(0);
-            if constexpr (COMP) cmp[j][p][k] = T(0);
-          }
+          for (int k = 0; k < KJ; ++k) acc[j][p].c[k] = acc[j][p].c[k] + T(0);
     }
 #pragma unroll 1
     for (uint32_t q0 = 0; q0 < n; q0 += 4) {
@@ -932,6 +993,24 @@ template <class V, int P> struct FwdExec {
             T cs[PER];
 #pragma unroll
             for (int j = 0; j < PER; ++j) cs[j] = reinterpret_cast<const T*>(crec)[j];
+            // an input jet (x_i, v_i, 0, ..) read at its source changes
+            // coefficients 0 and 1 only (its zero products add nothing)
+            if constexpr (JetOrder<V>::K > 0) {
+              if (direct) {
+#pragma unroll
+                for (int j = 0; j < PER; ++j) {
+                  if (jj + j < MX && (uint32_t)(jj + j) < m) {
+#pragma unroll
+                    for (int p = 0; p < P; ++p) {
+                      V& a = acc[jj + j < MX ? jj + j : 0][p];
+                      a.c[0] = a.c[0] + cs[j] * x[p].c[0];
+                      if constexpr (KJ > 1) a.c[1] = a.c[1] + cs[j] * x[p].c[1];
+                    }
+                  }
+                }
+                continue;
+              }
+            }
 #pragma unroll
             for (int j = 0; j < PER; ++j) {
               if (jj + j < MX && (uint32_t)(jj + j) < m) {
@@ -940,14 +1019,8 @@ template <class V, int P> struct FwdExec {
                 for (int p = 0; p < P; ++p) {
                   V& a = acc[jj + j < MX ? jj + j : 0][p];
                   if constexpr (JetOrder<V>::K > 0) {
-                    const int kmax = direct ? (KJ > 1 ? 2 : 1) : KJ;
 #pragma unroll
-                    for (int k = 0; k < KJ; ++k) {
-                      if (k < kmax) {
-                        if constexpr (COMP) neumaier_add(a.c[k], cmp[jj + j < MX ? jj + j : 0][p][k], c * x[p].c[k]);
-                        else a.c[k] = a.c[k] + c * x[p].c[k];
-                      }
-                    }
+                    for (int k = 0; k < KJ; ++k) a.c[k] = a.c[k] + c * x[p].c[k];
                   } else if constexpr (IsDual<V>::v) {
                     a.re = a.re + c * x[p].re;
                     a.eps = a.eps + (c * x[p].eps + zr[p]);
@@ -990,7 +1063,6 @@ template <class V, int P> struct FwdExec {
               T zs = T(0);
 #pragma unroll
               for (int k = 0; k < KJ; ++k) {
-                if constexpr (COMP) acc[j][p].c[k] = acc[j][p].c[k] + cmp[j][p][k];
                 if (k > 0) {
                   zs = zs + z[p][k - 1];
                   acc[j][p].c[k] = acc[j][p].c[k] + zs;
@@ -1016,13 +1088,16 @@ template <class V, int P> struct FwdExec {
     switch (opc) {
       case D_LDIN:
 #pragma unroll
-        for (int p = 0; p < P; ++p) r[p] = Lane<V>::make_input(kp, unit0 + p, ui[p], (uint32_t)aux, valid[p]);
+        for (int p = 0; p < P; ++p)
+          r[p] = Lane<V>::make_input(kp, unit0 + p, ui[p], (uint32_t)aux,
+                                     valid[p] && index_ok((uint32_t)aux, kp.ni, kp.err));
         put(w0.x >> 24, dof, save, r);
         return true;
       case D_STOUT:
         ld((w0.x >> 8) & 0xFFu, ao, imm, a);
 #pragma unroll
-        for (int p = 0; p < P; ++p) Lane<V>::store_output(kp, unit0 + p, (uint32_t)aux, a[p], valid[p]);
+        for (int p = 0; p < P; ++p)
+          Lane<V>::store_output(kp, unit0 + p, (uint32_t)aux, a[p], valid[p] && index_ok((uint32_t)aux, kp.no, kp.err));
         return true;
       case D_MOV:
         ld((w0.x >> 8) & 0xFFu, ao, imm, a);
@@ -1040,21 +1115,21 @@ template <class V, int P> struct FwdExec {
         return dense(st, (uint32_t)aux, ao);
 #define ECH_FB(NAME, FN)                                                     \
   case D_##NAME##_RR:                                                        \
-    C::ld(sm + ao, a);                                                       \
-    C::ld(sm + bo, b);                                                       \
+    C::ld(sp(ao), a);                                                        \
+    C::ld(sp(bo), b);                                                        \
     _Pragma("unroll") for (int p = 0; p < P; ++p) r[p] = Kd::FN(a[p], b[p]); \
     put_sm(dof, save, r);                                                    \
     return true;                                                                  \
   case D_##NAME##_IR: {                                                      \
     const V c = dm::VT<V>::cst(imm);                                         \
-    C::ld(sm + bo, b);                                                       \
+    C::ld(sp(bo), b);                                                        \
     _Pragma("unroll") for (int p = 0; p < P; ++p) r[p] = Kd::FN(c, b[p]);    \
     put_sm(dof, save, r);                                                    \
     return true;                                                                  \
   }                                                                          \
   case D_##NAME##_RI: {                                                      \
     const V c = dm::VT<V>::cst(imm);                                         \
-    C::ld(sm + ao, a);                                                       \
+    C::ld(sp(ao), a);                                                        \
     _Pragma("unroll") for (int p = 0; p < P; ++p) r[p] = Kd::FN(a[p], c);    \
     put_sm(dof, save, r);                                                    \
     return true;                                                                  \
@@ -1066,7 +1141,7 @@ template <class V, int P> struct FwdExec {
 #undef ECH_FB
 #define ECH_FU(OP)                                                                               \
   case D_FU_BASE + (OP - OP_NEG):                                                                \
-    C::ld(sm + ao, a);                                                                           \
+    C::ld(sp(ao), a);                                                                            \
     _Pragma("unroll") for (int p = 0; p < P; ++p) r[p] = dm::eval_forward<V>(OP, a[p], a[p], aux); \
     put_sm(dof, save, r);                                                                        \
     return true;
@@ -1117,10 +1192,23 @@ template <class V, int P> struct RevExec {
 #pragma unroll
       for (int p = 0; p < P; ++p) v[p] = Kd::c(0);
     } else {
+#ifdef ECH_DEVICE_BOUNDS
+      C::ld(bounded(const_cast<unsigned char*>(tj), off, (uint64_t)kp.traj_slots * kp.tile * sizeof(V), sm, kp.err),
+            v);
+#else
       C::ld(tj + off, v);
+#endif
     }
   }
+#ifdef ECH_DEVICE_BOUNDS
+  __device__ __forceinline__ unsigned char* loc(bool glob, uint32_t off) const {
+    const uint64_t row = (uint64_t)kp.tile * sizeof(V);
+    return glob ? bounded(gs, off, (uint64_t)kp.far_slots * row, sm, kp.err)
+                : bounded(sm, off, (uint64_t)kp.smem_regs * row, sm, kp.err);
+  }
+#else
   __device__ __forceinline__ unsigned char* loc(bool glob, uint32_t off) const { return (glob ? gs : sm) + off; }
+#endif
 
   template <bool FAST>
   __device__ __forceinline__ void accumulate(unsigned char* ptr, bool init, const V (&adj)[P], const V (&d)[P]) const {
@@ -1386,16 +1474,16 @@ template <class V, int P> struct RevExec {
   __device__ __forceinline__ void body(uint32_t opc, uint32_t flags, uint32_t ro, uint32_t ao, uint32_t bo,
                                        uint32_t vao, uint32_t vbo, uint32_t vro, int32_t aux, double imm) const {
     V adj[P], va[P], vb[P], vr[P], da[P], db[P];
-    C::ld(FAST ? sm + ro : loc(flags & RF_R_GLOB, ro), adj);
+    C::ld(FAST ? loc(false, ro) : loc(flags & RF_R_GLOB, ro), adj);
     value(vao, (flags & RF_VA_IMM) != 0, imm, va);
     value(vbo, (flags & RF_VB_IMM) != 0, imm, vb);
     value(vro, false, 0.0, vr);
 #pragma unroll
     for (int p = 0; p < P; ++p) dm::reverse_partials<V>(opc, va[p], vb[p], vr[p], aux, da[p], db[p]);
     if (flags & RF_HAS_A)
-      accumulate<FAST>(FAST ? sm + ao : loc(flags & RF_A_GLOB, ao), (flags & RF_A_INIT) != 0, adj, da);
+      accumulate<FAST>(FAST ? loc(false, ao) : loc(flags & RF_A_GLOB, ao), (flags & RF_A_INIT) != 0, adj, da);
     if (flags & RF_HAS_B)
-      accumulate<FAST>(FAST ? sm + bo : loc(flags & RF_B_GLOB, bo), (flags & RF_B_INIT) != 0, adj, db);
+      accumulate<FAST>(FAST ? loc(false, bo) : loc(flags & RF_B_GLOB, bo), (flags & RF_B_INIT) != 0, adj, db);
   }
 
   __device__ __forceinline__ bool operator()(const unsigned char* raw, Stream<48>& st) const {
@@ -1440,7 +1528,8 @@ template <class V, int P> struct RevExec {
           C::ld(loc(flags & RF_R_GLOB, ro), g);
         }
 #pragma unroll
-        for (int p = 0; p < P; ++p) GradOut<V>::store(kp, unit0 + p, (uint32_t)aux, g[p], valid[p]);
+        for (int p = 0; p < P; ++p)
+          GradOut<V>::store(kp, unit0 + p, (uint32_t)aux, g[p], valid[p] && index_ok((uint32_t)aux, kp.ni, kp.err));
         return true;
       }
 #define ECH_RF(OP) \

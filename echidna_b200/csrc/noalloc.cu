@@ -105,6 +105,7 @@ extern "C" ECH_API ech_status ech_gradient_batch_device_noalloc(ech_ctx* ctx, co
   kp.rev = reinterpret_cast<const DRIns*>(d_rev);
   kp.n_rev = (uint32_t)pg.rev.size();
   kp.far_slots = p.far_slots;
+  kp.traj_slots = p.traj_slots;
   kp.smem_regs = std::max<uint32_t>(p.smem_regs, 1);
   kp.tile = hs.tile;
   kp.n_units = B;
