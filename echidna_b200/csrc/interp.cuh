@@ -673,10 +673,35 @@ template <class V, int P> struct FwdExec {
   // term order.
   static constexpr int kWords = (int)(sizeof(V) * P / 4);
   static constexpr int kLcGroup = kWords <= 8 ? 4 : (kWords <= 16 ? 2 : 1);
+  // One term of a linear-combination chain: acc + Mul(c, x) (or Mul(x, c)).
+  // Dual values: the product's eps is c eps + 0 re; the zero products commute
+  // with every addition and add up exactly, so they collect in a tracker (one
+  // fused step each, started at -0) added once at the end of the chain.
+  __device__ __forceinline__ void lc_term(V& a, const V& c, const V& x, bool cx,
+                                          typename dm::VT<V>::S& dz) const {
+    if constexpr (IsDual<V>::v) {
+      a.re = a.re + c.re * x.re;
+      a.eps = a.eps + c.re * x.eps;
+      dz = fma_zero(x.re, dz);
+    } else {
+      a = Kd::add(a, cx ? Kd::mul(c, x) : Kd::mul(x, c));
+    }
+  }
+  __device__ __forceinline__ void lc_finish(V (&acc)[P], const typename dm::VT<V>::S (&dz)[P]) const {
+    if constexpr (IsDual<V>::v) {
+#pragma unroll
+      for (int p = 0; p < P; ++p) acc[p].eps = acc[p].eps + dz[p];
+    }
+  }
+
   __device__ __forceinline__ bool chain_lc(Stream<32>& st, uint32_t ma, uint32_t ao, double imm, uint32_t n,
                                            V (&acc)[P]) const {
     if constexpr (JetOrder<V>::K > 0) return chain_lc_jet(st, ma, ao, imm, n, acc);
+    using S = typename dm::VT<V>::S;
     ld(ma, ao, imm, acc);
+    S dz[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) dz[p] = -S(0);
     uint32_t q = 0;
     if constexpr (kLcGroup > 1) {
 #pragma unroll 1
@@ -700,8 +725,7 @@ template <class V, int P> struct FwdExec {
 #pragma unroll
         for (int j = 0; j < 2 * kLcGroup; ++j) {
 #pragma unroll
-          for (int p = 0; p < P; ++p)
-            acc[p] = Kd::add(acc[p], cx[j] ? Kd::mul(cs[j], xs[j][p]) : Kd::mul(xs[j][p], cs[j]));
+          for (int p = 0; p < P; ++p) lc_term(acc[p], cs[j], xs[j][p], cx[j], dz[p]);
         }
       }
     }
@@ -722,15 +746,15 @@ template <class V, int P> struct FwdExec {
         const bool b_cx = (xw.z >> 24) != 0;
 #pragma unroll
         for (int p = 0; p < P; ++p) {
-          const V ta = a_cx ? Kd::mul(ca, xa[p]) : Kd::mul(xa[p], ca);
-          const V tb = b_cx ? Kd::mul(cb, xb[p]) : Kd::mul(xb[p], cb);
-          acc[p] = Kd::add(Kd::add(acc[p], ta), tb);
+          lc_term(acc[p], ca, xa[p], a_cx, dz[p]);
+          lc_term(acc[p], cb, xb[p], b_cx, dz[p]);
         }
       } else {
 #pragma unroll
-        for (int p = 0; p < P; ++p) acc[p] = Kd::add(acc[p], a_cx ? Kd::mul(ca, xa[p]) : Kd::mul(xa[p], ca));
+        for (int p = 0; p < P; ++p) lc_term(acc[p], ca, xa[p], a_cx, dz[p]);
       }
     }
+    lc_finish(acc, dz);
     return true;
   }
 
@@ -952,7 +976,12 @@ template <class V, int P> struct FwdExec {
         if ((uint32_t)jj + 1 < m) ld((w.z >> 8) & 0xFFu, w.y, imm.y, acc[jj + 1]);
       }
     }
-    T z[P][KJ];
+    // Dual: the eps part of c x is c eps + 0 re; the zero products commute with
+    // every addition and add up exactly, so one tracker per point, started at
+    // -0 (the identity of +), collects them for the whole group: dz = fma(re, 0, dz).
+    T z[P][KJ], dz[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) dz[p] = -T(0);
     if constexpr (JetOrder<V>::K > 0) {
 #pragma unroll
       for (int p = 0; p < P; ++p)
@@ -980,10 +1009,9 @@ template <class V, int P> struct FwdExec {
         bool direct = false;
         if constexpr (JetOrder<V>::K > 0) direct = lc_jet_operand(mode, xo[t], x);
         else ldv(mode, xo[t], x);
-        T zr[P];
         if constexpr (IsDual<V>::v) {
 #pragma unroll
-          for (int p = 0; p < P; ++p) zr[p] = x[p].re * T(0);
+          for (int p = 0; p < P; ++p) dz[p] = fma_zero(x[p].re, dz[p]);
         }
 #pragma unroll
         for (int jj = 0; jj < MX; jj += PER) {
@@ -1023,7 +1051,7 @@ template <class V, int P> struct FwdExec {
                     for (int k = 0; k < KJ; ++k) a.c[k] = a.c[k] + c * x[p].c[k];
                   } else if constexpr (IsDual<V>::v) {
                     a.re = a.re + c * x[p].re;
-                    a.eps = a.eps + (c * x[p].eps + zr[p]);
+                    a.eps = a.eps + c * x[p].eps;
                   } else {
                     a = a + c * x[p];
                   }
@@ -1069,6 +1097,9 @@ template <class V, int P> struct FwdExec {
                 }
               }
             }
+          } else if constexpr (IsDual<V>::v) {
+#pragma unroll
+            for (int p = 0; p < P; ++p) acc[j][p].eps = acc[j][p].eps + dz[p];
           }
           put((mdw >> (8 * h)) & 0xFFu, h == 0 ? w0.x : w0.y, h == 0 ? w0.z : w0.w, acc[j]);
         }
@@ -1411,10 +1442,21 @@ template <class V, int P> struct RevExec {
   static constexpr int kGather = kWords <= 4 ? 4 : (kWords <= 8 ? 2 : 1);
   // c * t into cur unless t is zero (the zero-adjoint skip); gather constants
   // are never zero (the encoder leaves zero contributions out)
-  __device__ __forceinline__ void gather_update(V (&cur)[P], const V (&t)[P], const V& c) const {
+  // (Dual values: c t's eps is c eps + 0 re; the zero products go to the
+  // target's tracker dz, added once before the store, as in lc_term.)
+  __device__ __forceinline__ void gather_update(V (&cur)[P], const V (&t)[P], const V& c,
+                                                typename dm::VT<V>::S (&dz)[P]) const {
 #pragma unroll
-    for (int p = 0; p < P; ++p)
-      if (!Kd::all_zero(t[p])) cur[p] = Kd::add(cur[p], Kd::mul(c, t[p]));
+    for (int p = 0; p < P; ++p) {
+      if (Kd::all_zero(t[p])) continue;
+      if constexpr (IsDual<V>::v) {
+        cur[p].re = cur[p].re + c.re * t[p].re;
+        cur[p].eps = cur[p].eps + c.re * t[p].eps;
+        dz[p] = fma_zero(t[p].re, dz[p]);
+      } else {
+        cur[p] = Kd::add(cur[p], Kd::mul(c, t[p]));
+      }
+    }
   }
   __device__ __forceinline__ bool gather(Stream<48>& st, uint32_t ntargets) const {
 #pragma unroll 1
@@ -1426,6 +1468,9 @@ template <class V, int P> struct RevExec {
       unsigned char* px = loc(hf & CF_X_GLOB, h.y);
       V cur[P];
       lc_load(px, (hf & CF_X_INIT) != 0, cur);
+      typename dm::VT<V>::S dz[P];
+#pragma unroll
+      for (int p = 0; p < P; ++p) dz[p] = -typename dm::VT<V>::S(0);
       uint32_t q = 0;
       if constexpr (kGather > 1) {
 #pragma unroll 1
@@ -1444,7 +1489,7 @@ template <class V, int P> struct RevExec {
             cs[2 * k + 1] = lc_const<V>(cw.z, cw.w);
           }
 #pragma unroll
-          for (int j = 0; j < 2 * kGather; ++j) gather_update(cur, ts[j], cs[j]);
+          for (int j = 0; j < 2 * kGather; ++j) gather_update(cur, ts[j], cs[j], dz);
         }
       }
 #pragma unroll 1
@@ -1455,12 +1500,16 @@ template <class V, int P> struct RevExec {
         const uint4 aw = *reinterpret_cast<const uint4*>(r2 + 16);
         V t0[P];
         C::ld(loc(aw.z & CF_X_GLOB, aw.x), t0);
-        gather_update(cur, t0, lc_const<V>(cw.x, cw.y));
+        gather_update(cur, t0, lc_const<V>(cw.x, cw.y), dz);
         if (q + 1 < nc) {
           V t1[P];
           C::ld(loc((aw.z >> 16) & CF_X_GLOB, aw.y), t1);
-          gather_update(cur, t1, lc_const<V>(cw.z, cw.w));
+          gather_update(cur, t1, lc_const<V>(cw.z, cw.w), dz);
         }
+      }
+      if constexpr (IsDual<V>::v) {
+#pragma unroll
+        for (int p = 0; p < P; ++p) cur[p].eps = cur[p].eps + dz[p];
       }
       C::st(px, cur);
     }
