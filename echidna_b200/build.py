@@ -4,7 +4,11 @@ Every CUDA translation unit is compiled for sm_100a only
 (``-gencode arch=compute_100a,code=sm_100a``) with ``-fmad=false`` so that
 ``a*b+c`` rounds like the reference's CPU sweeps, then linked with the host
 lowering (plan.cpp) into one library that exports the C ABI of
-``include/echidna_b200.h``.  Compilation is incremental on file timestamps.
+``include/echidna_b200.h``.  The sweep-kernel units are compiled twice, without
+and with the dense-group executor (``-DECH_DN=0/1``); the host launches the
+second only for programs that hold dense groups, since its register demand
+lowers the occupancy of every other program.  Compilation is incremental on
+file timestamps.
 
 ``build(variant="bounds")`` builds ``libechidna_b200_bounds.so`` with
 ``-DECH_DEVICE_BOUNDS``: the same engine with every slot access and every
@@ -35,9 +39,11 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC
            "--expt-relaxed-constexpr", "-I", CSRC, "-I", os.path.join(ROOT, "include")]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-ffp-contract=off", "-I", CSRC]
 
-CU_SOURCES = ["abi.cu", "k_plain.cu", "k_dual.cu", "k_jet.cu", "k_jet1.cu", "k_jet2.cu", "k_jet3.cu", "k_jet4.cu", "k_jet5.cu", "k_jet6.cu",
-              "k_jet7.cu", "k_jet8.cu", "k_jet9.cu",
-              "stde.cu", "noalloc.cu", "k_multi.cu", "mlp.cu"]
+CU_SOURCES = ["abi.cu", "launch.cu", "stde.cu", "noalloc.cu", "mlp.cu"]
+# Sweep-kernel units, compiled twice: without (ECH_DN=0) and with (ECH_DN=1)
+# the dense-group executor.  Listed longest compile first.
+DN_SOURCES = ["k_jet3.cu", "k_jet2.cu", "k_dual.cu", "k_jet4.cu", "k_jet5.cu", "k_plain.cu", "k_multi.cu",
+              "k_jet1.cu", "k_jet6.cu", "k_jet7.cu", "k_jet8.cu", "k_jet9.cu"]
 CXX_SOURCES = ["plan.cpp", "sparsity.cpp"]
 
 
@@ -79,6 +85,13 @@ def build(verbose: bool = False, jobs: int | None = None, variant: str = "") -> 
     build_dir, lib, extra = VARIANTS[variant]
     os.makedirs(build_dir, exist_ok=True)
     cmds, objs = [], []
+    for dn in ("1", "0"):
+        for s in DN_SOURCES:
+            src = os.path.join(CSRC, s)
+            obj = os.path.join(build_dir, f"{s}.dn{dn}.o")
+            objs.append(obj)
+            if _newer(src, obj, _deps(src)):
+                cmds.append([NVCC, *ARCH, *NVFLAGS, *extra, f"-DECH_DN={dn}", "-c", src, "-o", obj])
     for s in CU_SOURCES:
         src = os.path.join(CSRC, s)
         obj = os.path.join(build_dir, s + ".o")

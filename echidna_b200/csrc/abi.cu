@@ -107,6 +107,7 @@ struct ech_ctx {
   uint32_t* d_err = nullptr;
   // launch overrides (0 = automatic)
   uint32_t ov_threads = 0, ov_ppt = 0, ov_cap = 0;
+  uint32_t ov_dense = 0;  // 1: the dense-group kernel build for every program (ech_ctx_set_dense_kernel)
   // ECH_FP32_* options of the FP32 batch STDE calls (0: reference rounding, FP64 reduction)
   uint32_t fp32_mode = 0;
 };
@@ -115,6 +116,11 @@ struct ech_ctx {
 // an SM (which sets the shared-register cap).
 struct Shape {
   uint32_t threads = 128, P = 1, ctas = 2;
+  // 1: run the kernel build with the dense-group executor even for programs
+  // without dense groups.  Both builds compute bit-identical results; the
+  // tuner keeps the faster (the build without the executor needs fewer
+  // registers, which pays where occupancy binds, not in one-warp launches).
+  uint32_t dense_kernel = 0;
 };
 
 struct ech_tape {
@@ -182,6 +188,12 @@ extern "C" ECH_API ech_status ech_ctx_set_launch(ech_ctx* ctx, uint32_t threads,
   ctx->ov_threads = threads;
   ctx->ov_ppt = ppt;
   ctx->ov_cap = cap;
+  return ECH_OK;
+}
+
+extern "C" ECH_API ech_status ech_ctx_set_dense_kernel(ech_ctx* ctx, int always) {
+  if (!ctx) return fail(ECH_ERR_INVALID_ARG, "ctx is null");
+  ctx->ov_dense = always ? 1u : 0u;
   return ECH_OK;
 }
 
@@ -301,6 +313,7 @@ struct LaunchCfg {
   size_t smem = 0;
   size_t smem_full = 0;  // the shape's whole per-CTA share of shared memory
   size_t vbytes = 0;
+  bool dense_kernel = false;  // Shape::dense_kernel
 };
 
 static Kind kind_of(int k) {
@@ -326,6 +339,7 @@ static LaunchCfg cfg_for(ech_ctx* ctx, const ech_tape* t, int kind, int K, Shape
   c.threads = (int)sh.threads;
   c.tile = sh.threads * sh.P;
   c.vbytes = value_bytes(c.req);
+  c.dense_kernel = sh.dense_kernel != 0;
   // per-SM shared memory split between `ctas` CTAs, each paying the
   // per-block reservation and the kernel's static barriers
   const size_t per_sm = ctx->smem_per_sm ? ctx->smem_per_sm : 233472;
@@ -346,6 +360,7 @@ static LaunchCfg choose_cfg(ech_ctx* ctx, const ech_tape* t, int kind, int K) {
   sh.threads = ctx->ov_threads ? ctx->ov_threads : 128;
   sh.P = ctx->ov_ppt ? ctx->ov_ppt : 1;
   sh.ctas = ctx->ov_cap ? 1 : 2;
+  sh.dense_kernel = ctx->ov_dense;
   return cfg_for(ctx, t, kind, K, sh);
 }
 
@@ -419,6 +434,7 @@ static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_
                           io.compensated == 0, &dp);
   if (s != ECH_OK) return s;
   const Plan& p = dp->host;
+  c.req.dense = !p.dense.empty() || c.dense_kernel;
   const uint32_t regs = std::max<uint32_t>(p.smem_regs, 1);
   c.smem = kRingBytes + (size_t)regs * c.tile * c.vbytes;
   const uint32_t dir_bits = bits_bytes ? (uint32_t)c.smem : 0u;
@@ -499,15 +515,13 @@ static ech_status tune(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n_un
   cudaEvent_t e0, e1;
   CU(cudaEventCreate(&e0));
   CU(cudaEventCreate(&e1));
-  float best_ms = -1.0f;
   ech_status first_err = ECH_OK;
   std::string first_msg;
-  const bool small_batch = n_units < (uint64_t)2 * 128 * ctx->sm_count;
-  for (const Shape& sh : kShapes) {
-    if (sh.threads * sh.P < 128 && !small_batch) continue;
+  // one warm launch (plan build + upload), then one timed; < 0 when the shape fails
+  auto time_shape = [&](const Shape& sh, bool warm) -> float {
     const LaunchCfg c = cfg_for(ctx, t, kind, K, sh);
-    if (c.cap < 1 || kRingBytes + (size_t)c.tile * c.vbytes > ctx->smem_optin) continue;
-    ech_status s = launch_cfg(ctx, t, kind, K, n_units, io, st, c);  // warm: plan build + upload
+    if (c.cap < 1 || kRingBytes + (size_t)c.tile * c.vbytes > ctx->smem_optin) return -1.0f;
+    ech_status s = warm ? launch_cfg(ctx, t, kind, K, n_units, io, st, c) : ECH_OK;
     if (s == ECH_OK) {
       cudaEventRecord(e0, st);
       s = launch_cfg(ctx, t, kind, K, n_units, io, st, c);
@@ -515,14 +529,37 @@ static ech_status tune(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n_un
     }
     if (s != ECH_OK) {
       if (first_err == ECH_OK) { first_err = s; first_msg = g_last_error; }
-      continue;
+      return -1.0f;
     }
-    if (cudaEventSynchronize(e1) != cudaSuccess) break;
+    if (cudaEventSynchronize(e1) != cudaSuccess) return -2.0f;
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, e0, e1);
+    return ms;
+  };
+  float best_ms = -1.0f;
+  const bool small_batch = n_units < (uint64_t)2 * 128 * ctx->sm_count;
+  for (const Shape& sh : kShapes) {
+    if (sh.threads * sh.P < 128 && !small_batch) continue;
+    const float ms = time_shape(sh, true);
+    if (ms == -2.0f) break;
+    if (ms < 0.0f) continue;
     if (best_ms < 0.0f || ms < best_ms) {
       best_ms = ms;
       *best = sh;
+    }
+  }
+  if (best_ms >= 0.0f) {
+    // the best shape on the other kernel build: two timings of each, interleaved
+    Shape alt = *best;
+    alt.dense_kernel = 1;
+    float a_ms = time_shape(alt, true);
+    if (a_ms >= 0.0f) {
+      const float b2 = time_shape(*best, false);
+      const float a2 = time_shape(alt, false);
+      float b_ms = best_ms;
+      if (b2 >= 0.0f) b_ms = std::min(b_ms, b2);
+      if (a2 >= 0.0f) a_ms = std::min(a_ms, a2);
+      if (a_ms < b_ms) *best = alt;
     }
   }
   cudaEventDestroy(e0);
@@ -533,7 +570,7 @@ static ech_status tune(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n_un
 
 static ech_status enqueue(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n_units, const SweepIO& io,
                           cudaStream_t st) {
-  const bool overridden = ctx->ov_threads || ctx->ov_ppt || ctx->ov_cap;
+  const bool overridden = ctx->ov_threads || ctx->ov_ppt || ctx->ov_cap || ctx->ov_dense;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   if (!overridden && ctx->autotune && n_units >= kTuneMinUnits && cudaStreamIsCapturing(st, &cap) == cudaSuccess &&
       cap == cudaStreamCaptureStatusNone) {
@@ -606,7 +643,7 @@ static void host_copy(void* dst, const void* src, size_t bytes) {
 static ech_status run_pipelined(ech_ctx* ctx, ech_tape* t, int kind, uint64_t n_units, const SweepIO& io,
                                 const size_t io_unit_bytes[5], const std::vector<PipeArray>& arrays, bool* done) {
   *done = false;
-  const bool overridden = ctx->ov_threads || ctx->ov_ppt || ctx->ov_cap;
+  const bool overridden = ctx->ov_threads || ctx->ov_ppt || ctx->ov_cap || ctx->ov_dense;
   if (overridden || !ctx->autotune || n_units < kPipeMinUnits) return ECH_OK;
   Shape sh;
   {
@@ -2030,7 +2067,7 @@ ECH_API ech_status ech_tape_launch_shape(ech_ctx* ctx, const ech_tape* tc, int k
   c = tuned ? cfg_for(ctx, t, kind, (int)order, sh) : choose_cfg(ctx, t, kind, (int)order);
   Plan p = build_plan(t->host, kind_of(kind), c.cap, dense_group_max((uint32_t)c.vbytes, (uint32_t)c.req.P));
   uint64_t v[8] = {(uint64_t)c.threads, (uint64_t)c.req.P, tuned ? sh.ctas : 0, c.cap, p.smem_regs, p.far_slots,
-                   p.traj_slots, tuned};
+                   p.traj_slots, tuned | (tuned && sh.dense_kernel ? 2u : 0u)};
   memcpy(shape, v, sizeof v);
   return ECH_OK;
 }
@@ -2088,6 +2125,7 @@ static ech_status multi_prepare(ech_multi* m, Shape sh) {
     DevPlan* dp = nullptr;
     CHECK(get_plan(t, 2, 0, c.cap, c.tile, (uint32_t)c.vbytes, (uint32_t)c.req.P, true, &dp));
     const Plan& p = dp->host;
+    if (!p.dense.empty() || c.dense_kernel) c.req.dense = true;
     regs = std::max<uint32_t>(regs, p.smem_regs);
     slots = std::max<uint64_t>(slots, (uint64_t)p.far_slots + p.traj_slots);
     J j{};
@@ -2129,7 +2167,7 @@ static ech_status multi_prepare(ech_multi* m, Shape sh) {
   stride = (stride + 255) & ~(uint64_t)255;
   MultiParams mp{};
   int bps = 0;
-  cudaError_t e = launch_multi_hvp(m->f64, c.req.P, mp, 0, c.threads, c.smem, nullptr, &bps);
+  cudaError_t e = launch_multi_hvp(c.req.dense, m->f64, c.req.P, mp, 0, c.threads, c.smem, nullptr, &bps);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
   if (bps <= 0) return fail(ECH_ERR_OTHER, "tape live set does not fit the shared-memory slot file");
   const uint64_t grid = std::min<uint64_t>(first, (uint64_t)bps * ctx->sm_count);
@@ -2160,7 +2198,8 @@ static ech_status multi_enqueue(ech_multi* m, cudaStream_t st) {
   mp.stride = m->stride;
   CU(cudaMemsetAsync(m->next.p, 0, sizeof(uint32_t), st));
   int bps = 0;
-  cudaError_t e = launch_multi_hvp(m->f64, m->cfg.req.P, mp, m->grid, m->cfg.threads, m->cfg.smem, st, &bps);
+  cudaError_t e = launch_multi_hvp(m->cfg.req.dense, m->f64, m->cfg.req.P, mp, m->grid, m->cfg.threads, m->cfg.smem,
+                                   st, &bps);
   if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
   return ECH_OK;
 }
@@ -2192,7 +2231,8 @@ ECH_API ech_status ech_multi_create(ech_ctx* ctx, int f64, const ech_multi_item*
   std::lock_guard<std::mutex> lk(ctx->mu);
   CU(cudaSetDevice(ctx->device));
   Shape best;
-  if (autotune) {
+  best.dense_kernel = ctx->ov_dense;
+  if (autotune && !ctx->ov_dense) {
     cudaEvent_t e0, e1;
     CU(cudaEventCreate(&e0));
     CU(cudaEventCreate(&e1));
@@ -2210,6 +2250,24 @@ ECH_API ech_status ech_multi_create(ech_ctx* ctx, int f64, const ech_multi_item*
       if (best_ms < 0.0f || ms < best_ms) {
         best_ms = ms;
         best = sh;
+      }
+    }
+    if (best_ms >= 0.0f) {
+      // the best shape on the other kernel build (bit-identical results)
+      Shape alt = best;
+      alt.dense_kernel = 1;
+      if (multi_prepare(m.get(), alt) == ECH_OK && multi_enqueue(m.get(), ctx->stream) == ECH_OK) {
+        float a_ms = -1.0f;
+        for (int r = 0; r < 2; ++r) {
+          cudaEventRecord(e0, ctx->stream);
+          const ech_status s = multi_enqueue(m.get(), ctx->stream);
+          cudaEventRecord(e1, ctx->stream);
+          if (s != ECH_OK || cudaEventSynchronize(e1) != cudaSuccess) break;
+          float ms = 0.0f;
+          cudaEventElapsedTime(&ms, e0, e1);
+          a_ms = a_ms < 0.0f ? ms : std::min(a_ms, ms);
+        }
+        if (a_ms >= 0.0f && a_ms < best_ms) best = alt;
       }
     }
     cudaEventDestroy(e0);
@@ -2233,7 +2291,7 @@ ECH_API ech_status ech_multi_launch(ech_multi* m, void* stream) {
 ECH_API ech_status ech_multi_info(const ech_multi* m, uint64_t* info) {
   if (!m || !info) return fail(ECH_ERR_INVALID_ARG, "null argument");
   uint64_t v[9] = {m->shape.threads, m->shape.P, m->shape.ctas, m->cfg.cap, (uint64_t)m->grid, m->total_tiles,
-                   m->n_jobs, m->stride, m->tuned ? 1u : 0u};
+                   m->n_jobs, m->stride, (m->tuned ? 1u : 0u) | (m->shape.dense_kernel ? 2u : 0u)};
   memcpy(info, v, sizeof v);
   return ECH_OK;
 }
@@ -2282,6 +2340,7 @@ ech_status prepare_gradient_host(ech_ctx* ctx, const ech_tape* tc, int f64, uint
     hp = it->second.get();
   }
   out->req = c.req;
+  out->req.dense = !hp->plan.dense.empty() || ctx->ov_dense;
   out->threads = c.threads;
   out->tile = c.tile;
   out->vbytes = c.vbytes;

@@ -482,7 +482,11 @@ template <class T> struct GradOut<dm::Dual<T>> {
 // ───────────────────────────── forward executor ─────────────────────────────
 // Instructions are decoded from two 16-byte words straight into registers
 // (DIns layout: opc|ma|mb|md, a, b, d | save, aux, imm).
-template <class V, int P> struct FwdExec {
+// DN: the executor carries dense groups (D_DENSE).  Their m running values
+// raise the kernel's register demand for every program, so programs without
+// dense groups run an instantiation without them (DN = false), where D_DENSE is
+// an invalid instruction.
+template <class V, int P, bool DN = true> struct FwdExec {
   using Kd = typename dm::KindOf<V>::K;
   using C = Col<V, P>;
   const KParams& kp;
@@ -943,7 +947,7 @@ template <class V, int P> struct FwdExec {
   //   plain  c x;
   //   Dual   (c re, c eps + 0 re), the zero product shared by the group;
   //   jets   the scaled, normalised form with per-term trackers (chain_lc_jet).
-  static constexpr int kDenseMax = (int)dense_group_max((uint32_t)sizeof(V), (uint32_t)P);
+  static constexpr int kDenseMax = DN ? (int)dense_group_max((uint32_t)sizeof(V), (uint32_t)P) : 1;
   __device__ __forceinline__ bool dense(Stream<32>& st, uint32_t m, uint32_t n) const {
     if constexpr (kDenseMax < 2) {
       if (threadIdx.x == 0) atomicOr(kp.err, (uint32_t)KERR_BADINS);
@@ -1602,7 +1606,7 @@ template <class V, int P> struct RevExec {
 // One tile of `kp.tile` units: the forward program (with trajectory saves when
 // REV), then the reverse program.  `gbase` is the CTA's global scratch region.
 // Returns false when a bounded wait gave up (every thread sees the same value).
-template <class V, int P, bool REV>
+template <class V, int P, bool REV, bool DN>
 __device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned char* sm, unsigned char* gbase,
                                            uint64_t t) {
   const uint32_t tile = kp.tile;
@@ -1612,7 +1616,7 @@ __device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned
                                    : gbase + (size_t)kp.far_slots * tile * sizeof(V) + colb;
   const uint64_t unit0 = t * tile + (uint64_t)threadIdx.x * P;
   uint32_t* bits = kp.dir_bits ? reinterpret_cast<uint32_t*>(rg.buf + kp.dir_bits) + threadIdx.x * P : nullptr;
-  FwdExec<V, P> fx{kp, sm, gs, tj, unit0, bits, {}, {}, {}, {}, {}};
+  FwdExec<V, P, DN> fx{kp, sm, gs, tj, unit0, bits, {}, {}, {}, {}, {}};
 #pragma unroll
   for (int p = 0; p < P; ++p) {
     fx.valid[p] = unit0 + p < kp.n_units;
@@ -1660,7 +1664,8 @@ __device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned
 // REV = false: forward program only (forward values, JVP, Taylor jets).
 // REV = true : forward program with trajectory saves, then the reverse program
 //              (gradient for plain values, HVP for Dual values).
-template <class V, int P, bool REV>
+// DN: with the dense-group executor (programs that hold D_DENSE instructions).
+template <class V, int P, bool REV, bool DN>
 __global__ void __launch_bounds__(256) sweep_kernel(KParams kp) {
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   __shared__ __align__(8) uint64_t full[kStages];
@@ -1674,7 +1679,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(KParams kp) {
   unsigned char* gbase = reinterpret_cast<unsigned char*>(kp.scratch) + blockIdx.x * kp.scratch_stride_bytes;
   const uint64_t ntiles = (kp.n_units + kp.tile - 1) / kp.tile;
   for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x)
-    if (!sweep_tile<V, P, REV>(kp, rg, sm, gbase, t)) return;
+    if (!sweep_tile<V, P, REV, DN>(kp, rg, sm, gbase, t)) return;
 }
 
 // ───────────────────────────── many tapes, one launch ───────────────────────
@@ -1699,7 +1704,7 @@ struct MultiParams {
   uint64_t stride;       // scratch bytes per CTA
 };
 
-template <class V, int P>
+template <class V, int P, bool DN>
 __global__ void __launch_bounds__(256) multi_sweep_kernel(MultiParams mp) {
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   __shared__ __align__(8) uint64_t full[kStages];
@@ -1731,7 +1736,7 @@ __global__ void __launch_bounds__(256) multi_sweep_kernel(MultiParams mp) {
     }
     __syncthreads();
     if (s_tile >= mp.total_tiles) break;
-    if (!sweep_tile<V, P, true>(job, rg, sm, gbase, s_local)) return;
+    if (!sweep_tile<V, P, true, DN>(job, rg, sm, gbase, s_local)) return;
     __syncthreads();  // every thread is done with `job` before thread 0 replaces it
   }
 }

@@ -3,9 +3,11 @@
 #include "k_common.cuh"
 
 namespace ech {
+template <bool DN>
 cudaError_t launch_jet6(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
                         int* bps) {
-  return r.f64 ? launch_p1<dm::Jet<double, 6>>(r, kp, grid, block, smem, st, bps)
-               : launch_p1<dm::Jet<float, 6>>(r, kp, grid, block, smem, st, bps);
+  return r.f64 ? launch_p1<dm::Jet<double, 6>, DN>(r, kp, grid, block, smem, st, bps)
+               : launch_p1<dm::Jet<float, 6>, DN>(r, kp, grid, block, smem, st, bps);
 }
+ECH_INSTANTIATE_DN(launch_jet6, const LaunchReq&, const KParams&, int, int, size_t, cudaStream_t, int*)
 }  // namespace ech

@@ -17,30 +17,31 @@ struct LaunchReq {
   int K = 0;      // jet order (Jet kind)
   int P = 1;      // points per thread
   bool rev = false;
+  bool dense = false;  // the program holds dense groups: the kernel with the dense-group executor
 };
 
 size_t value_bytes(const LaunchReq& r);
-// Each returns cudaErrorInvalidValue for an unsupported combination.
+// Each returns cudaErrorInvalidValue for an unsupported combination.  DN: the
+// kernel with the dense-group executor (r.dense).
+template <bool DN>
 cudaError_t launch_plain(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
                          int* blocks_per_sm);
+template <bool DN>
 cudaError_t launch_dual(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
                         int* blocks_per_sm);
 cudaError_t launch_jet(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
                        int* blocks_per_sm);
 
 // Launch (grid > 0) or query occupancy (grid == 0, result in *blocks_per_sm).
-inline cudaError_t launch_sweep(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem,
-                                cudaStream_t st, int* blocks_per_sm) {
-  switch (r.vk) {
-    case VKind::Plain: return launch_plain(r, kp, grid, block, smem, st, blocks_per_sm);
-    case VKind::Dual: return launch_dual(r, kp, grid, block, smem, st, blocks_per_sm);
-    case VKind::Jet: return launch_jet(r, kp, grid, block, smem, st, blocks_per_sm);
-  }
-  return cudaErrorInvalidValue;
-}
+cudaError_t launch_sweep(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
+                         int* blocks_per_sm);
 
-// Many-tape persistent gradient + per-point HVP launch (grid == 0: occupancy query).
-cudaError_t launch_multi_hvp(bool f64, int P, const MultiParams& mp, int grid, int block, size_t smem,
+// Many-tape persistent gradient + per-point HVP launch (grid == 0: occupancy
+// query); dense: some job's program holds dense groups.
+template <bool DN>
+cudaError_t launch_multi_hvp_dn(bool f64, int P, const MultiParams& mp, int grid, int block, size_t smem,
+                                cudaStream_t st, int* blocks_per_sm);
+cudaError_t launch_multi_hvp(bool dense, bool f64, int P, const MultiParams& mp, int grid, int block, size_t smem,
                              cudaStream_t st, int* blocks_per_sm);
 
 // STDE per-point reduction of scale*c_k samples (Welford in direction order);

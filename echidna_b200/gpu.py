@@ -226,6 +226,11 @@ class CudaContext:
     def set_launch(self, threads: int = 0, points_per_thread: int = 0, smem_reg_cap: int = 0):
         _check(_lib.load().ech_ctx_set_launch(self._h, threads, points_per_thread, smem_reg_cap))
 
+    def set_dense_kernel(self, always: bool = True):
+        """Run every sweep on the kernel build with the dense-group executor, on the fixed
+        launch shape (``ech_ctx_set_dense_kernel``); ``False`` restores the automatic choice."""
+        _check(_lib.load().ech_ctx_set_dense_kernel(self._h, 1 if always else 0))
+
     FP32_COMPENSATED_JETS, FP32_COMPENSATED_MEANS, FP32_PLAIN_MEANS = 1, 2, 4
 
     def set_fp32_mode(self, flags: int = 0):
@@ -243,7 +248,10 @@ class CudaContext:
         _check(_lib.load().ech_tape_launch_shape(self._h, tape._h, kinds[kind], order, n_units, buf))
         keys = ["threads", "points_per_thread", "ctas_per_sm", "smem_reg_cap", "smem_regs", "far_slots",
                 "traj_slots", "tuned"]
-        return dict(zip(keys, [int(v) for v in buf]))
+        d = dict(zip(keys, [int(v) for v in buf]))
+        d["dense_kernel"] = (d["tuned"] >> 1) & 1   # the tuner chose the dense-group kernel build
+        d["tuned"] &= 1
+        return d
 
     def plan_stats(self, tape: _TapeHandle, kind: str, order: int = 0) -> dict:
         kinds = {"forward": 0, "gradient": 1, "hvp": 2, "tangent": 3, "taylor": 4, "taylor_direct": 5}
@@ -462,7 +470,10 @@ class MultiTapeHvp:
         _check(_lib.load().ech_multi_info(self._h, buf))
         keys = ["threads", "points_per_thread", "ctas_per_sm", "smem_reg_cap", "grid", "tiles", "jobs",
                 "scratch_bytes_per_cta", "tuned"]
-        return dict(zip(keys, [int(v) for v in buf]))
+        d = dict(zip(keys, [int(v) for v in buf]))
+        d["dense_kernel"] = (d["tuned"] >> 1) & 1
+        d["tuned"] &= 1
+        return d
 
     def close(self):
         if getattr(self, "_h", None) and getattr(self._ctx, "_h", None):

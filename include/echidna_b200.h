@@ -290,7 +290,8 @@ ECH_API ech_status ech_multi_create(ech_ctx* ctx, int f64, const ech_multi_item*
                                     int autotune, ech_multi** out);
 ECH_API ech_status ech_multi_launch(ech_multi* multi, void* stream);
 /* info[9]: threads, points per thread, CTAs per SM, shared-register cap, grid,
- * tiles, jobs, scratch bytes per CTA, tuned (1/0). */
+ * tiles, jobs, scratch bytes per CTA, and a word: bit 0 tuned, bit 1 the kernel
+ * build with the dense-group executor (as in ech_tape_launch_shape). */
 ECH_API ech_status ech_multi_info(const ech_multi* multi, uint64_t* info);
 ECH_API void ech_multi_destroy(ech_multi* multi);
 
@@ -459,6 +460,13 @@ ECH_API ech_status ech_plan_dump(const uint32_t* opcodes, const uint32_t* arg0, 
  * points per thread and the shared-register cap. */
 ECH_API ech_status ech_ctx_set_launch(ech_ctx* ctx, uint32_t threads, uint32_t points_per_thread,
                                       uint32_t smem_reg_cap);
+/* always != 0: every sweep runs the kernel build with the dense-group
+ * executor, on the fixed launch shape (an override, like ech_ctx_set_launch).
+ * The engine has two builds of each sweep kernel: one carries the dense-group
+ * executor, which programs with dense groups need, and one leaves it out, which
+ * needs fewer registers; both compute the same results.  By default the
+ * autotuner picks per shape. */
+ECH_API ech_status ech_ctx_set_dense_kernel(ech_ctx* ctx, int always);
 /* Launch-shape autotuning (default on).  Without overrides, the first sweep of
  * a (tape, kind, order, batch-size octave) with at least 512 units times a
  * fixed set of shapes (threads per CTA, points per thread, CTAs per SM) on the
@@ -468,7 +476,10 @@ ECH_API ech_status ech_ctx_set_launch(ech_ctx* ctx, uint32_t threads, uint32_t p
 ECH_API ech_status ech_ctx_set_autotune(ech_ctx* ctx, int enable);
 /* The shape a sweep of `n_units` units uses.  shape[8]: threads, points per
  * thread, CTAs per SM (0 = fixed shape), shared-register cap, shared registers
- * used, global slots, trajectory slots, tuned (1/0). */
+ * used, global slots, trajectory slots, and a word whose bit 0 says the shape is
+ * tuned and bit 1 that the tuner chose the kernel build with the dense-group
+ * executor for a program without dense groups (both builds compute the same
+ * results). */
 ECH_API ech_status ech_tape_launch_shape(ech_ctx* ctx, const ech_tape* tape, int kind, uint32_t order,
                                         uint64_t n_units, uint64_t* shape);
 
