@@ -82,6 +82,9 @@ struct DevPlan {
   DIns* d_fwd = nullptr;
   DRIns* d_rev = nullptr;
   uint32_t n_fwd = 0, n_rev = 0;  // records of the device programs (chain terms inline)
+  uint32_t gather_tiles = 0;      // gather tiles in the reverse program
+  // the program needs the kernel build with the dense-group executor
+  bool needs_dense() const { return !host.dense.empty() || gather_tiles > 0; }
   ~DevPlan() {
     if (d_fwd) cudaFree(d_fwd);
     if (d_rev) cudaFree(d_rev);
@@ -389,6 +392,7 @@ static ech_status get_plan(ech_tape* t, int kind, int K, uint32_t cap, uint32_t 
     CU(cudaMemcpy(dp->d_rev, prog.rev.data(), prog.rev.size() * sizeof(DRIns), cudaMemcpyHostToDevice));
   dp->n_fwd = (uint32_t)prog.fwd.size();
   dp->n_rev = (uint32_t)prog.rev.size();
+  dp->gather_tiles = prog.gather_tiles;
   *out = dp.get();
   t->plans[key] = std::move(dp);
   return ECH_OK;
@@ -434,7 +438,7 @@ static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_
                           io.compensated == 0, &dp);
   if (s != ECH_OK) return s;
   const Plan& p = dp->host;
-  c.req.dense = !p.dense.empty() || c.dense_kernel;
+  c.req.dense = dp->needs_dense() || c.dense_kernel;
   const uint32_t regs = std::max<uint32_t>(p.smem_regs, 1);
   c.smem = kRingBytes + (size_t)regs * c.tile * c.vbytes;
   const uint32_t dir_bits = bits_bytes ? (uint32_t)c.smem : 0u;
@@ -2125,7 +2129,7 @@ static ech_status multi_prepare(ech_multi* m, Shape sh) {
     DevPlan* dp = nullptr;
     CHECK(get_plan(t, 2, 0, c.cap, c.tile, (uint32_t)c.vbytes, (uint32_t)c.req.P, true, &dp));
     const Plan& p = dp->host;
-    if (!p.dense.empty() || c.dense_kernel) c.req.dense = true;
+    if (dp->needs_dense() || c.dense_kernel) c.req.dense = true;
     regs = std::max<uint32_t>(regs, p.smem_regs);
     slots = std::max<uint64_t>(slots, (uint64_t)p.far_slots + p.traj_slots);
     J j{};
@@ -2340,7 +2344,7 @@ ech_status prepare_gradient_host(ech_ctx* ctx, const ech_tape* tc, int f64, uint
     hp = it->second.get();
   }
   out->req = c.req;
-  out->req.dense = !hp->plan.dense.empty() || ctx->ov_dense;
+  out->req.dense = !hp->plan.dense.empty() || hp->prog.gather_tiles > 0 || ctx->ov_dense;
   out->threads = c.threads;
   out->tile = c.tile;
   out->vbytes = c.vbytes;

@@ -108,7 +108,9 @@ enum DOp : uint8_t {
   D_DENSE = 86,     // forward: XI_DENSE; followed by its DDenseInit, term and DDenseFin records
   D_NORM = 84,      // reverse: XI_NORM
   D_GATHER = 85,    // reverse: XI_GATHER; per target a DRTerm header (ax, flags, ay = contributions)
-                    // followed by DRPair records (ax = the chain adjoint's offset, c)
+                    // followed by DRPair records (ax = the chain adjoint's offset, c); or, for
+                    // targets that read the same chain adjoints, a gather tile (DRTerm kind 1,
+                    // see DGatherTargets)
   D_FU_BASE = 96,   // forward unary fast form: 96 + (op - OP_NEG), a and dst smem
   D_RF_BASE = 128,  // reverse fast form: 128 + op, every adjoint location in smem
 };
@@ -181,6 +183,33 @@ struct alignas(16) DRPair {
   uint64_t pad2[2];
 };
 static_assert(sizeof(DRPair) == sizeof(DRIns), "reverse term records are instruction-sized");
+
+// A gather tile in a D_GATHER stream: T targets (DRTerm header: kind 1, op = T,
+// ay = n sources) whose contributions read the same n chain adjoints in the
+// same order (the reverse of a dense layer), all with nonzero constants.  Then
+// one DGatherTargets record and, per block of 12 sources, one DGatherSrc record
+// followed by one record of constants per source (T values, f32 or f64).  Each
+// target still adds its contributions in source order.
+struct alignas(16) DGatherTargets {
+  uint32_t tx[12];            // target adjoint byte offsets | GT_INIT | GT_GLOB
+};
+static_assert(sizeof(DGatherTargets) == sizeof(DRIns), "reverse records are instruction-sized");
+struct alignas(16) DGatherSrc {
+  uint32_t ax[12];            // chain adjoint byte offsets | GT_GLOB
+};
+static_assert(sizeof(DGatherSrc) == sizeof(DRIns), "reverse records are instruction-sized");
+constexpr uint32_t GT_GLOB = 1u << 31;   // the slot is a global (far) slot
+constexpr uint32_t GT_INIT = 1u << 30;   // the target's first contribution (starts from +0)
+constexpr uint32_t GT_OFF = GT_INIT - 1; // byte offset bits
+
+// Largest gather tile: its running targets stay in registers, as a dense
+// group's outputs do; at most one record of constants per source (12 f32, 6 f64).
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+constexpr uint32_t gather_tile_max(uint32_t dense_max, bool f64) {
+  return dense_max < (f64 ? 6u : 12u) ? dense_max : (f64 ? 6u : 12u);
+}
 
 // A dense group (D_DENSE: aux = m outputs, a = n terms) in the forward stream:
 //   ceil(m/2) DDenseInit   the outputs' acc0

@@ -1208,7 +1208,8 @@ template <class V, int P, bool DN = true> struct FwdExec {
 
 // ───────────────────────────── reverse executor ─────────────────────────────
 // DRIns layout: opc|pad|flags, r, a, b | va, vb, vr, aux | imm, pad.
-template <class V, int P> struct RevExec {
+// DN: the executor carries gather tiles (built with the dense-group executor).
+template <class V, int P, bool DN = true> struct RevExec {
   using Kd = typename dm::KindOf<V>::K;
   using C = Col<V, P>;
   const KParams& kp;
@@ -1462,12 +1463,108 @@ template <class V, int P> struct RevExec {
       }
     }
   }
+  // A gather tile (DGatherTargets): T targets whose contributions read the
+  // same chain adjoints in the same order, every constant nonzero.  Each source
+  // is loaded and zero-tested once for the tile and added to every target, in
+  // source order per target, as gather_update does.  Dual values: every target
+  // receives the same zero products (one per source that is not skipped), so
+  // one tracker per point serves the whole tile.  Records are read into
+  // registers before the next pull.
+  static constexpr int kGT =
+      DN ? (int)gather_tile_max(dense_group_max((uint32_t)sizeof(V), (uint32_t)P), sizeof(typename dm::VT<V>::S) == 8)
+         : 1;
+  __device__ __forceinline__ bool gather_tile(Stream<48>& st, uint32_t T, uint32_t ns) const {
+    if constexpr (kGT < 2) {
+      if (threadIdx.x == 0) atomicOr(kp.err, (uint32_t)KERR_BADINS);
+      ring_drain(*st.rg);
+      return false;
+    } else {
+      using S = typename dm::VT<V>::S;
+      if (T < 2 || T > (uint32_t)kGT) {
+        if (threadIdx.x == 0) atomicOr(kp.err, (uint32_t)KERR_BADINS);
+        ring_drain(*st.rg);
+        return false;
+      }
+      const unsigned char* trec = st.next();
+      if (trec == nullptr) return false;
+      uint32_t tx[kGT];
+#pragma unroll
+      for (int k = 0; k < kGT; ++k) tx[k] = reinterpret_cast<const uint32_t*>(trec)[k];
+      V cur[kGT][P];
+#pragma unroll
+      for (int k = 0; k < kGT; ++k)
+        if ((uint32_t)k < T) lc_load(loc((tx[k] & GT_GLOB) != 0, tx[k] & GT_OFF), (tx[k] & GT_INIT) != 0, cur[k]);
+      S dz[P];
+#pragma unroll
+      for (int p = 0; p < P; ++p) dz[p] = -S(0);
+#pragma unroll 1
+      for (uint32_t s0 = 0; s0 < ns; s0 += 12) {
+        const unsigned char* srec = st.next();
+        if (srec == nullptr) return false;
+        uint32_t ax[12];
+#pragma unroll
+        for (int j = 0; j < 12; ++j) ax[j] = reinterpret_cast<const uint32_t*>(srec)[j];
+#pragma unroll
+        for (int j = 0; j < 12; ++j) {
+          if (s0 + j >= ns) break;
+          V t[P];
+          C::ld(loc((ax[j] & GT_GLOB) != 0, ax[j] & GT_OFF), t);
+          const unsigned char* crec = st.next();
+          if (crec == nullptr) return false;
+          S cs[kGT];
+#pragma unroll
+          for (int k = 0; k < kGT; ++k) cs[k] = reinterpret_cast<const S*>(crec)[k];
+#pragma unroll
+          for (int p = 0; p < P; ++p) {
+            if (Kd::all_zero(t[p])) continue;  // the zero-adjoint skip
+            if constexpr (IsDual<V>::v) {
+              dz[p] = fma_zero(t[p].re, dz[p]);
+#pragma unroll
+              for (int k = 0; k < kGT; ++k) {
+                if ((uint32_t)k < T) {
+                  cur[k][p].re = cur[k][p].re + cs[k] * t[p].re;
+                  cur[k][p].eps = cur[k][p].eps + cs[k] * t[p].eps;
+                }
+              }
+            } else {
+#pragma unroll
+              for (int k = 0; k < kGT; ++k)
+                if ((uint32_t)k < T) cur[k][p] = Kd::add(cur[k][p], Kd::mul(dm::VT<V>::cst_s(cs[k]), t[p]));
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kGT; ++k) {
+        if ((uint32_t)k < T) {
+          if constexpr (IsDual<V>::v) {
+#pragma unroll
+            for (int p = 0; p < P; ++p) cur[k][p].eps = cur[k][p].eps + dz[p];
+          }
+          C::st(loc((tx[k] & GT_GLOB) != 0, tx[k] & GT_OFF), cur[k]);
+        }
+      }
+      return true;
+    }
+  }
+
   __device__ __forceinline__ bool gather(Stream<48>& st, uint32_t ntargets) const {
 #pragma unroll 1
     for (uint32_t g = 0; g < ntargets; ++g) {
       const unsigned char* rec = st.next();
       if (rec == nullptr) return false;
       const uint4 h = *reinterpret_cast<const uint4*>(rec);
+      if ((h.x & 0xFFu) == 1u) {  // a gather tile of (h.x >> 8) & 0xFF targets, h.z sources
+        const uint32_t T = (h.x >> 8) & 0xFFu;
+        if (T > ntargets - g) {
+          if (threadIdx.x == 0) atomicOr(kp.err, (uint32_t)KERR_BADINS);
+          ring_drain(*st.rg);
+          return false;
+        }
+        if (!gather_tile(st, T, h.z)) return false;
+        g += T - 1;
+        continue;
+      }
       const uint32_t hf = h.x >> 16, nc = h.z;
       unsigned char* px = loc(hf & CF_X_GLOB, h.y);
       V cur[P];
@@ -1653,7 +1750,7 @@ __device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned
   }
   if (!run_program<32>(rg, reinterpret_cast<const unsigned char*>(kp.fwd), kp.n_fwd, kp.err, fx)) return false;
   if (REV) {
-    RevExec<V, P> rx{kp, sm, gs, tj, unit0, {}};
+    RevExec<V, P, DN> rx{kp, sm, gs, tj, unit0, {}};
 #pragma unroll
     for (int p = 0; p < P; ++p) rx.valid[p] = fx.valid[p];
     if (!run_program<48>(rg, reinterpret_cast<const unsigned char*>(kp.rev), kp.n_rev, kp.err, rx)) return false;

@@ -261,6 +261,7 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap, uint32_t dense_
   const bool emit_outputs = (kind != Kind::Hvp);
   const uint32_t seed = t.outs.empty() ? t.out_index : t.outs[0];
   Plan pl;
+  pl.dense_max = dense_max < 1 ? 1 : dense_max;
 
   auto is_const = [&](uint32_t s) { return t.op[s] == OP_CONST; };
   auto has_b = [&](uint32_t i) { return is_binary(t.op[i]); };
@@ -1304,7 +1305,87 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, bool f32, DevPro
       d.opc = D_GATHER;
       d.r = d.a = d.b = d.va = d.vb = d.vr = kNone;
       out.rev.push_back(d);
+      // gather tiles: consecutive targets whose contributions read the same
+      // chain adjoints in the same order, every constant nonzero in the value
+      // type (then no contribution is left out, and the targets share each
+      // source's load, zero test and zero product)
+      const uint32_t tmax = gather_tile_max(p.dense_max, !f32);
+      std::vector<uint32_t> hpos;  // header index of each target
       for (uint32_t h = 0, q = in.va; h < (uint32_t)in.aux; ++h) {
+        hpos.push_back(q);
+        q += 1 + p.gathers[q].n;
+      }
+      auto zero_const = [&](double c) {
+        const double cv = lc_c(c);
+        if (!f32) return cv == 0.0;
+        float f;
+        std::memcpy(&f, &cv, sizeof f);
+        return f == 0.0f;
+      };
+      auto tileable = [&](uint32_t q) {
+        const GRec& hd = p.gathers[q];
+        if (hd.n == 0 || off(hd.idx) > GT_OFF) return false;
+        for (uint32_t c = 1; c <= hd.n; ++c)
+          if (zero_const(p.gathers[q + c].c) || off(p.gathers[q + c].idx) > GT_OFF) return false;
+        return true;
+      };
+      auto same_sources = [&](uint32_t qa, uint32_t qb) {
+        const GRec& a = p.gathers[qa];
+        const GRec& b = p.gathers[qb];
+        if (a.n != b.n) return false;
+        for (uint32_t c = 1; c <= a.n; ++c) {
+          const GRec& ga = p.gathers[qa + c];
+          const GRec& gb = p.gathers[qb + c];
+          if (ga.idx != gb.idx || ga.mode != gb.mode) return false;
+        }
+        return true;
+      };
+      for (uint32_t h = 0; h < (uint32_t)in.aux;) {
+        uint32_t T = 1;
+        if (tmax >= 2 && tileable(hpos[h]))
+          while (h + T < (uint32_t)in.aux && T < tmax && tileable(hpos[h + T]) && same_sources(hpos[h], hpos[h + T]))
+            ++T;
+        if (T >= 2) {
+          const uint32_t ns = p.gathers[hpos[h]].n;
+          DRTerm head{};
+          head.kind = 1;
+          head.op = (uint8_t)T;
+          head.ay = ns;
+          out.rev.push_back(as_record<DRIns>(head));
+          DGatherTargets tg{};
+          for (uint32_t k = 0; k < T; ++k) {
+            const GRec& hd = p.gathers[hpos[h + k]];
+            tg.tx[k] = off(hd.idx) | ((hd.flags & CF_X_INIT) ? GT_INIT : 0u) | (hd.mode == M_GLOB ? GT_GLOB : 0u);
+          }
+          out.rev.push_back(as_record<DRIns>(tg));
+          for (uint32_t s0 = 0; s0 < ns; s0 += 12) {
+            DGatherSrc sr{};
+            for (uint32_t j = 0; j < 12 && s0 + j < ns; ++j) {
+              const GRec& g = p.gathers[hpos[h] + 1 + s0 + j];
+              sr.ax[j] = off(g.idx) | (g.mode == M_GLOB ? GT_GLOB : 0u);
+            }
+            out.rev.push_back(as_record<DRIns>(sr));
+            for (uint32_t j = s0; j < s0 + 12 && j < ns; ++j) {
+              unsigned char rec[sizeof(DRIns)] = {};
+              for (uint32_t k = 0; k < T; ++k) {
+                const double c = p.gathers[hpos[h + k] + 1 + j].c;
+                if (f32) {
+                  const float fc = (float)c;
+                  std::memcpy(rec + 4 * k, &fc, 4);
+                } else {
+                  std::memcpy(rec + 8 * k, &c, 8);
+                }
+              }
+              DRIns r;
+              std::memcpy(&r, rec, sizeof r);
+              out.rev.push_back(r);
+            }
+          }
+          out.gather_tiles += 1;
+          h += T;
+          continue;
+        }
+        const uint32_t q = hpos[h];
         const GRec& hd = p.gathers[q];
         // a contribution whose constant is zero (after rounding to the value
         // type) never changes the target: it is left out, so the kernel skips
@@ -1332,7 +1413,7 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, bool f32, DevPro
           }
           out.rev.push_back(as_record<DRIns>(pr));
         }
-        q += 1 + hd.n;
+        ++h;
       }
       continue;
     }

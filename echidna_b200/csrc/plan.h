@@ -91,6 +91,7 @@ struct Plan {
   uint32_t smem_regs = 0;      // shared registers used
   uint32_t far_slots = 0;      // global registers (max of both sweeps)
   uint32_t traj_slots = 0;     // trajectory slots
+  uint32_t dense_max = 1;      // the dense group limit the plan was built for (also bounds gather tiles)
   PlanStats stats;
 };
 
@@ -107,6 +108,7 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap, uint32_t dense_
 struct DevProgram {
   std::vector<DIns> fwd;
   std::vector<DRIns> rev;
+  uint32_t gather_tiles = 0;   // gather tiles in rev (the kernel build with the dense-group executor runs them)
 };
 // `f32`: the program runs on f32 values (their linear-combination constants are stored rounded).
 bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, bool f32, DevProgram& out, std::string& err);
