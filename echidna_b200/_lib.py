@@ -99,6 +99,7 @@ _SIGS = {
     "ech_mlp_gradients": ([_P, _P, _P, _I, _P, _P, _P, _P, _P, _P, _P], _I),
     "ech_ctx_set_fp32_mode": ([_P, _U32], _I),
     "ech_ctx_set_dense_kernel": ([_P, _I], _I),
+    "ech_tape_program_stats": ([_P, _P, _I, _U32, _U64, _P], _I),
     "ech_mlp_get_weights": ([_P, _P, _P, _P, _P, _P, _P], _I),
     "ech_mlp_destroy": ([_P], None),
     "ech_multi_create": ([_P, _I, _P, _U32, _I, _P], _I),

@@ -2055,6 +2055,30 @@ ECH_API ech_status ech_tape_plan_stats(ech_ctx* ctx, const ech_tape* tc, int kin
   return ECH_OK;
 }
 
+ECH_API ech_status ech_tape_program_stats(ech_ctx* ctx, const ech_tape* tc, int kind, uint32_t order,
+                                         uint64_t n_units, uint64_t* stats) {
+  if (!ctx || !tc || !stats) return fail(ECH_ERR_INVALID_ARG, "null argument");
+  if (kind < 0 || kind > 5) return fail(ECH_ERR_INVALID_ARG, "kind must be 0..5");
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  const int skind = kind == 5 ? 4 : kind;  // input-direct jets use the jets' shapes
+  Shape sh;
+  bool tuned = false;
+  {
+    std::lock_guard<std::mutex> lk(t->mu);
+    auto it = t->shapes.find(std::make_tuple(skind, (int)order, size_bucket(n_units)));
+    if (it != t->shapes.end()) { sh = it->second; tuned = true; }
+  }
+  const LaunchCfg c = tuned ? cfg_for(ctx, t, skind, (int)order, sh) : choose_cfg(ctx, t, skind, (int)order);
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  DevPlan* dp = nullptr;
+  CHECK(get_plan(t, kind, (int)order, c.cap, c.tile, (uint32_t)c.vbytes, (uint32_t)c.req.P, true, &dp));
+  uint64_t v[5] = {dp->n_fwd, dp->n_rev, (uint64_t)dp->host.dense.size(), dp->gather_tiles,
+                   (dp->needs_dense() || c.dense_kernel) ? 1u : 0u};
+  memcpy(stats, v, sizeof v);
+  return ECH_OK;
+}
+
 ECH_API ech_status ech_tape_launch_shape(ech_ctx* ctx, const ech_tape* tc, int kind, uint32_t order,
                                         uint64_t n_units, uint64_t* shape) {
   if (!ctx || !tc || !shape) return fail(ECH_ERR_INVALID_ARG, "null argument");

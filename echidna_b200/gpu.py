@@ -253,6 +253,14 @@ class CudaContext:
         d["tuned"] &= 1
         return d
 
+    def program_stats(self, tape: _TapeHandle, kind: str, n_units: int, order: int = 0) -> dict:
+        """The encoded device program a sweep of ``n_units`` runs (``ech_tape_program_stats``)."""
+        kinds = {"forward": 0, "gradient": 1, "hvp": 2, "tangent": 3, "taylor": 4, "taylor_direct": 5}
+        buf = (ctypes.c_uint64 * 5)()
+        _check(_lib.load().ech_tape_program_stats(self._h, tape._h, kinds[kind], order, n_units, buf))
+        keys = ["fwd_records", "rev_records", "dense_groups", "gather_tiles", "dense_kernel"]
+        return dict(zip(keys, [int(v) for v in buf]))
+
     def plan_stats(self, tape: _TapeHandle, kind: str, order: int = 0) -> dict:
         kinds = {"forward": 0, "gradient": 1, "hvp": 2, "tangent": 3, "taylor": 4, "taylor_direct": 5}
         buf = (ctypes.c_uint64 * 12)()

@@ -482,6 +482,12 @@ ECH_API ech_status ech_ctx_set_autotune(ech_ctx* ctx, int enable);
  * results). */
 ECH_API ech_status ech_tape_launch_shape(ech_ctx* ctx, const ech_tape* tape, int kind, uint32_t order,
                                         uint64_t n_units, uint64_t* shape);
+/* The device program a sweep of `n_units` units runs with that shape (kind 0..4
+ * as above, 5 = input-direct jets; built and uploaded if needed).  stats[5]:
+ * forward records, reverse records, dense groups, reverse gather tiles, and 1
+ * when the sweep runs the kernel build with the dense-group executor. */
+ECH_API ech_status ech_tape_program_stats(ech_ctx* ctx, const ech_tape* tape, int kind, uint32_t order,
+                                         uint64_t n_units, uint64_t* stats);
 
 #ifdef __cplusplus
 }
