@@ -630,59 +630,78 @@ class UnevenWorkload:
 class LearnedWorkload:
     """C5: sparse STDE trace of f = sum a_i softplus(x_i x_{i+1}) + sum a_i cos x_i (n = 1,024,
     a_i log-uniform in [1e-3, 1e3]) with the learned proposal vs uniform sampling.  Setup
-    labels training points with exact FP64 diagonals from the tape's jets and trains the
-    1024-256-256-1024 BF16 MLP on the GPU; the timed step is the learned estimator (MLP +
-    256 sampled jets per point, FP32 jets, FP64 Welford) over 1,024 held-out points.
-    ``detail`` gives the samples and wall time each proposal needs for 1 % relative error."""
+    draws the configured 1,048,576 training points on the device, labels them with exact FP64
+    diagonals (one per-point HVP per color of the Hessian's tridiagonal pattern: two HVPs per
+    point) and trains the 1024-256-256-1024 BF16 MLP on the GPU; the held-out points' diagonals
+    come from order-3 jets along every e_j and are compared with the colored HVPs.  The timed
+    step is the learned estimator (MLP + 256 sampled jets per point, FP32 jets, FP64 Welford)
+    over 1,024 held-out points.  ``detail`` gives the samples and wall time each proposal
+    needs for 1 % relative error."""
     name = "learned"
     n = 1024
     batch = 1024          # held-out points per timed step
     S = 256               # samples per point in the timed step
     launches_per_step = 10  # MLP: 3 conversions, 3 GEMMs, softmax; sampler, jet sweep, reduction
-    n_train = 16384
+    n_train = 1 << 20
     n_eval = 1024
+    train_steps = 4000
+    train_batch = 1024
 
     def __init__(self, rank, world):
         from echidna_b200 import configs
         self.seed = configs.SEEDS["softplus_chain"]
+        self.rank = rank
         self.tape = configs.softplus_chain(self.n)
         rng = np.random.default_rng([self.seed, rank])
-        self.Xtr = rng.normal(size=(self.n_train, self.n))
         self.Xev = rng.normal(size=(self.n_eval, self.n))
 
     def describe(self):
         return {"workload": "learned STDE proposal: softplus-chain n=1024, MLP 1024-256-256-1024 (BF16 tcgen05, "
                             "FP32 accumulation) trained on exact FP64 diagonals; learned vs uniform sparse STDE",
                 "eval_points": self.batch, "samples_per_point_in_step": self.S,
-                "training_points": self.n_train}, "f32"
+                "training_points": self.n_train, "training_steps": self.train_steps,
+                "training_batch": self.train_batch}, "f32"
 
     def setup(self, ctx, lib, torch, sp):
         from echidna_b200 import learned
         from echidna_b200.gpu import GpuTapeData
+        from echidna_b200.sparse import detect_sparsity
         self.ctx, self.lib, self.sp, self.torch = ctx, lib, sp, torch
         self.g64 = ctx.upload_tape_f64(self.tape)
         self.g32 = ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(self.tape))
+        coloring = learned.diagonal_coloring(detect_sparsity(self.tape))
+        self.num_colors = coloring[1]
         # labels and training run on the default stream, before the timed stream is used
         with torch.cuda.stream(torch.cuda.default_stream()):
+            g = torch.Generator(device="cuda").manual_seed(self.seed + self.rank)
+            xtr = torch.randn((self.n_train, self.n), dtype=torch.float64, device="cuda", generator=g)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            xtr = torch.tensor(self.Xtr, device="cuda")
-            d = learned.exact_diagonals(ctx, self.g64, xtr)
+            d = learned.colored_diagonals(ctx, self.g64, xtr, coloring)
             torch.cuda.synchronize()
             self.t_labels = time.perf_counter() - t0
             q = learned.target_distribution(d)
+            del d
+            xf = xtr.float()
+            del xtr
             t0 = time.perf_counter()
             self.mlp = learned.ProposalMLP(ctx, self.n, 256, self.n, seed=self.seed)
-            g = torch.Generator(device="cuda").manual_seed(self.seed)
-            xf = xtr.float()
             self.losses = []
-            for _ in range(1500):
-                rows = torch.randint(0, self.n_train, (512,), device="cuda", generator=g)
+            for _ in range(self.train_steps):
+                rows = torch.randint(0, self.n_train, (self.train_batch,), device="cuda", generator=g)
                 self.losses.append(self.mlp.train_step(xf[rows].contiguous(), q[rows].contiguous(), lr=1e-3))
             torch.cuda.synchronize()
             self.t_train = time.perf_counter() - t0
+            del xf, q
             xev = torch.tensor(self.Xev, device="cuda")
-            self.d_eval = learned.exact_diagonals(ctx, self.g64, xev).cpu().numpy()
+            t0 = time.perf_counter()
+            d_ev = learned.exact_diagonals(ctx, self.g64, xev)
+            torch.cuda.synchronize()
+            self.t_eval_jets = time.perf_counter() - t0
+            d_col = learned.colored_diagonals(ctx, self.g64, xev, coloring)
+            scale = d_ev.abs().amax(dim=1, keepdim=True)
+            self.label_diff = float(((d_col - d_ev).abs() / scale).max())
+            self.d_eval = d_ev.cpu().numpy()
             self.xev32 = xev.float().contiguous()
             self.p_eval = self.mlp.probs(self.xev32).cpu().numpy()
             torch.cuda.synchronize()
@@ -744,8 +763,10 @@ class LearnedWorkload:
                 "mlp_forward_ms_per_1024_points": t_mlp, "uniform_step_ms": t_unif,
                 "check_32_points_at_median_samples": {"samples": S_chk,
                                                       "median_relative_error": float(np.median(rel))},
-                "labels_s": self.t_labels, "training_s": self.t_train, "loss_first_last": [self.losses[0],
-                                                                                          self.losses[-1]]}
+                "labels": {"points": self.n_train, "hvps_per_point": self.num_colors, "seconds": self.t_labels,
+                           "eval_1024_points_by_jets_s": self.t_eval_jets,
+                           "max_rel_diff_colored_hvp_vs_jets": self.label_diff},
+                "training_s": self.t_train, "loss_first_last": [self.losses[0], self.losses[-1]]}
 
     def e2e_step(self):
         torch = self.torch

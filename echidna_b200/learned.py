@@ -172,6 +172,69 @@ def exact_diagonals(ctx, tape64, X64, chunk: int = 4096):
     return torch.cat(parts)
 
 
+def diagonal_coloring(pattern):
+    """Colors the coordinates so that no two of one color interact: H_jk = 0 for
+    every j != k of the same color.  Then, with v_c the indicator vector of color
+    c, (H v_c)_j = H_jj for every j of color c, and one HVP per color yields the
+    exact diagonal.  Greedy in index order over the structural pattern of
+    ``sparse.detect_sparsity`` (a distance-1 coloring of the Hessian's graph; the
+    reference's distance-2 ``greedy_coloring``, ``src/sparse.rs:57-98``, is also
+    valid here but may use more colors).  Returns (colors [n] uint32, count)."""
+    n = int(pattern.dim)
+    r = np.asarray(pattern.rows, np.int64)
+    c = np.asarray(pattern.cols, np.int64)
+    off = r != c
+    nbrs = [[] for _ in range(n)]
+    for a, b in zip(r[off].tolist(), c[off].tolist()):
+        nbrs[a].append(b)
+        nbrs[b].append(a)
+    colors = np.full(n, -1, np.int64)
+    for j in range(n):
+        used = {int(colors[k]) for k in nbrs[j] if colors[k] >= 0}
+        col = 0
+        while col in used:
+            col += 1
+        colors[j] = col
+    return colors.astype(np.uint32), int(colors.max() + 1) if n else 0
+
+
+def colored_diagonals(ctx, tape64, X64, coloring, chunk: int = 65536, stream=None):
+    """Exact FP64 Hessian diagonals of the rows of the device tensor X64 [N, n]
+    from one per-point HVP (forward-over-reverse, ``ech_hvp_batch_device``) per
+    color of ``coloring`` (``diagonal_coloring``): every diagonal entry is read
+    from the HVP of its own color, whose other coordinates do not interact with
+    it.  A tridiagonal Hessian takes two HVPs per point instead of n jets.
+    Returns a device tensor [N, n]; work runs on torch's current stream."""
+    import torch
+    colors, nc = coloring
+    N, n = int(X64.shape[0]), int(X64.shape[1])
+    out = torch.empty_like(X64)
+    if N == 0 or nc == 0:
+        return out.zero_()
+    dev = X64.device
+    col_t = torch.as_tensor(np.asarray(colors, np.int64), device=dev)
+    seeds = torch.zeros((nc, n), dtype=torch.float64, device=dev)
+    seeds[col_t, torch.arange(n, device=dev)] = 1.0
+    masks = [col_t == k for k in range(nc)]
+    st = _stream(stream)
+    lib = _lib.load()
+    b_max = min(chunk, N)
+    dirs = torch.empty((nc, b_max, n), dtype=torch.float64, device=dev)
+    for k in range(nc):
+        dirs[k].copy_(seeds[k].expand(b_max, n))
+    grads = torch.empty((b_max, n), dtype=torch.float64, device=dev)
+    hv = torch.empty((b_max, n), dtype=torch.float64, device=dev)
+    for i in range(0, N, b_max):
+        b = min(b_max, N - i)
+        xs = X64[i:i + b].contiguous()
+        for k in range(nc):
+            _check(lib.ech_hvp_batch_device(ctx._h, tape64._h, 1, xs.data_ptr(), 1, dirs[k].data_ptr(), b,
+                                            grads.data_ptr(), hv.data_ptr(), ctypes.c_void_p(st)))
+            _settle(ctx, st)
+            out[i:i + b, masks[k]] = hv[:b, masks[k]]
+    return out
+
+
 def train_proposal(ctx, tape64, X64, hidden: int = 256, steps: int = 400, batch: int = 256, lr: float = 1e-3,
                    seed: int = 0):
     """Trains the proposal on exact diagonals of the training points X64 [N, n]

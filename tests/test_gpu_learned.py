@@ -5,8 +5,9 @@ import pytest
 
 from echidna_b200 import configs
 from echidna_b200.gpu import GpuTapeData
-from echidna_b200.learned import (as_records, exact_diagonals, samples_to_tolerance, sparse_trace,
-                                  train_proposal)
+from echidna_b200.learned import (as_records, colored_diagonals, diagonal_coloring, exact_diagonals,
+                                  samples_to_tolerance, sparse_trace, train_proposal)
+from echidna_b200.sparse import detect_sparsity
 from oracle.oracle import OracleTape
 
 pytestmark = pytest.mark.gpu
@@ -22,6 +23,27 @@ def test_hessian_diagonal_batch_matches_oracle(ctx):
     for b in range(6):
         ref = np.diag(o.hessian(X[b])[2])
         assert np.allclose(got[b], ref, rtol=1e-10, atol=1e-10 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("n", [2, 3, 64, 1024])
+def test_colored_diagonals_match_jets_and_oracle(ctx, n):
+    # the training labels: two HVPs per point (the softplus chain's Hessian is tridiagonal)
+    # against the n order-3 jets per point and, for small n, the oracle's dense Hessian
+    tape = configs.softplus_chain(n)
+    gt = ctx.upload_tape_f64(tape)
+    coloring = diagonal_coloring(detect_sparsity(tape))
+    assert coloring[1] == (1 if n == 1 else 2)
+    B = 300 if n <= 64 else 40
+    X = torch.tensor(np.random.default_rng(5).normal(size=(B, n)), device="cuda")
+    got = colored_diagonals(ctx, gt, X, coloring, chunk=128).cpu().numpy()
+    jets = exact_diagonals(ctx, gt, X).cpu().numpy()
+    scale = np.abs(jets).max(axis=1, keepdims=True)
+    assert np.all(np.abs(got - jets) <= 1e-12 * scale)
+    if n <= 64:
+        o = OracleTape(tape)
+        for b in range(0, B, 37):
+            ref = np.diag(o.hessian(X[b].cpu().numpy())[2])
+            assert np.allclose(got[b], ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
 
 
 @pytest.mark.parametrize("learned", [False, True])

@@ -116,6 +116,21 @@ def test_patterns_and_colors_match_oracle_restatement(engine_lib, name):
         assert cc.tolist() == occ and cn == ocn
 
 
+def test_diagonal_coloring_separates_interacting_coordinates(engine_lib):
+    from echidna_b200.learned import diagonal_coloring
+    # tridiagonal: two colors; diagonal only: one; a dense 3x3 lower triangle: three
+    assert diagonal_coloring(_pat(5, [0, 1, 1, 2, 2, 3, 3, 4, 4], [0, 0, 1, 1, 2, 2, 3, 3, 4]))[1] == 2
+    assert diagonal_coloring(_pat(4, [0, 1, 2, 3], [0, 1, 2, 3]))[1] == 1
+    assert diagonal_coloring(_pat(3, [0, 1, 1, 2, 2, 2], [0, 0, 1, 0, 1, 2]))[1] == 3
+    assert diagonal_coloring(_pat(0, [], []))[1] == 0
+    # the learned-proposal tape (softplus of x_i x_{i+1}): a valid coloring with two colors
+    p = detect_sparsity(configs.softplus_chain(257))
+    colors, n = diagonal_coloring(p)
+    assert n == 2
+    off = p.rows != p.cols
+    assert np.all(colors[p.rows[off]] != colors[p.cols[off]])
+
+
 def test_many_colors_fall_back_past_64(engine_lib):
     # a dense 70 x 70 Hessian needs 70 colors: exercises the >= 64 color branch
     n = 70
