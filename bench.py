@@ -738,6 +738,7 @@ class LearnedWorkload:
                 e1.synchronize()
                 ts.append(e0.elapsed_time(e1))
             return float(np.mean(ts))
+        gemm = self._gemm_rates(torch, stream, timed)
         t_learn = timed(lambda: self._learned(self.S))
         t_unif = timed(lambda: self._uniform(self.S))
         t_mlp = timed(lambda: self.mlp.probs(self.xev32, out=self.probs, stream=self.sp))
@@ -766,7 +767,42 @@ class LearnedWorkload:
                 "labels": {"points": self.n_train, "hvps_per_point": self.num_colors, "seconds": self.t_labels,
                            "eval_1024_points_by_jets_s": self.t_eval_jets,
                            "max_rel_diff_colored_hvp_vs_jets": self.label_diff},
-                "training_s": self.t_train, "loss_first_last": [self.losses[0], self.losses[-1]]}
+                "training_s": self.t_train, "loss_first_last": [self.losses[0], self.losses[-1]],
+                "gemm_bf16_tcgen05": gemm}
+
+    def _gemm_rates(self, torch, stream, timed):
+        """TFLOP/s of the proposal's tensor-core GEMM (``ech_gemm_bf16``) at the MLP's
+        first-layer shape (batch 1,024) and at 8192^3, against the measured cuBLAS peak."""
+        import ctypes
+        from echidna_b200 import _lib as _lib_mod
+        lib = _lib_mod.load()
+        pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        peak, src = 1590.0, "fallback"
+        if os.path.exists(pk):
+            with open(pk) as f:
+                peak, src = float(json.load(f).get("bf16_tflops", 1590.0)), "measured (cuBLAS bf16, burst)"
+        out = {"peak_bf16_tflops": peak, "peak_source": src}
+        for (M, N, K) in [(1024, 256, 1024), (8192, 8192, 8192)]:
+            g = torch.Generator(device="cuda").manual_seed(M + N + K)
+            A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+            B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+            C = torch.empty(M, N, device="cuda", dtype=torch.float32)
+            st = ctypes.c_void_p(stream.cuda_stream)
+
+            def run():
+                r = lib.ech_gemm_bf16(self.ctx._h, A.data_ptr(), B.data_ptr(), C.data_ptr(), None, M, N, K, K, K,
+                                      N, st)
+                if r != 0:
+                    raise RuntimeError(_lib_mod.last_error())
+            ms = timed(run)
+            ref = (A[:64].float() @ B.float().T)
+            err = float((C[:64] - ref).abs().max() / ref.abs().max().clamp_min(1.0))
+            tf = 2.0 * M * N * K / (ms * 1e-3) / 1e12
+            out[f"{M}x{N}x{K}"] = {"ms": ms, "tflops": tf,
+                                   "frac_of_peak": tf / peak,
+                                   "max_rel_err_vs_fp32_first_64_rows": err}
+            del A, B, C
+        return out
 
     def e2e_step(self):
         torch = self.torch

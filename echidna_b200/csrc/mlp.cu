@@ -8,6 +8,8 @@
 // Training target: per point a probability vector q over the n_out
 // coordinates (for sparse STDE, q_j = |H_jj| / sum_k |H_kk| from exact tape
 // jets); loss = mean over points of -sum_j q_j log p_j.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -136,15 +138,58 @@ __global__ void adam_kernel(float* w, const float* g, float* m, float* v, bf16* 
 
 unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// 2-D map of a row-major bf16 matrix [rows][K] (row stride ld elements): boxes of
+// 8 K-elements x box_rows rows, no swizzle, zero fill past the edges.
+cudaError_t make_operand_map(CUtensorMap* map, const bf16* base, int rows, int K, int ld, int box_rows) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return cudaErrorNotSupported;
+  const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(bf16)};
+  const cuuint32_t box[2] = {8u, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1u, 1u};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16*>(base), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+template <int BN>
+cudaError_t gemm_tiles(const bf16* A, const bf16* B, float* C, const float* bias, int M, int N, int K, int lda,
+                       int ldb, int ldc, uint32_t* err, cudaStream_t st) {
+  using TL = ech::umma::Tile<BN>;
+  CUtensorMap ta, tb;
+  cudaError_t e = make_operand_map(&ta, A, M, K, lda, ech::umma::kBM);
+  if (e == cudaSuccess) e = make_operand_map(&tb, B, N, K, ldb, BN);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ech::umma::gemm_bf16_tn<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TL::kSmemBytes);
+  if (e != cudaSuccess) return e;
+  dim3 grid((N + BN - 1) / BN, (M + ech::umma::kBM - 1) / ech::umma::kBM);
+  ech::umma::gemm_bf16_tn<BN><<<grid, ech::umma::kThreads, TL::kSmemBytes, st>>>(ta, tb, C, bias, M, N, K, ldc, err);
+  return cudaGetLastError();
+}
+
+// 128 x 128 tiles, or 128 x 64 when the 128-wide grid would cover less than
+// half of the 148 SMs.
 cudaError_t gemm(const bf16* A, const bf16* B, float* C, const float* bias, int M, int N, int K, int lda, int ldb,
                  int ldc, uint32_t* err, cudaStream_t st) {
-  cudaError_t e = cudaFuncSetAttribute(ech::umma::gemm_bf16_tn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)ech::umma::kSmemBytes);
-  if (e != cudaSuccess) return e;
-  dim3 grid((N + ech::umma::kBN - 1) / ech::umma::kBN, (M + ech::umma::kBM - 1) / ech::umma::kBM);
-  ech::umma::gemm_bf16_tn<<<grid, ech::umma::kThreads, ech::umma::kSmemBytes, st>>>(A, B, C, bias, M, N, K, lda, ldb,
-                                                                                    ldc, err);
-  return cudaGetLastError();
+  const long tiles128 = (long)((M + 127) / 128) * ((N + 127) / 128);
+  if (tiles128 < 74) return gemm_tiles<64>(A, B, C, bias, M, N, K, lda, ldb, ldc, err, st);
+  return gemm_tiles<128>(A, B, C, bias, M, N, K, lda, ldb, ldc, err, st);
 }
 
 cudaError_t transpose(const bf16* in, bf16* out, int R, int C, cudaStream_t st) {

@@ -1,19 +1,26 @@
-// BF16 GEMM on the sm_100a tensor cores (tcgen05.mma, accumulator in TMEM).
+// BF16 GEMM on the sm_100a tensor cores (tcgen05.mma, accumulator in TMEM),
+// operands moved by TMA (cp.async.bulk.tensor).
 //
 //   C[M x N] (fp32) = A[M x K] (bf16, row-major) * B[N x K]^T (bf16, row-major)  (+ bias[N])
 //
-// One CTA of 128 threads computes a 128 x 128 tile of C.  K advances in blocks
-// of 64: every thread copies its share of the A and B blocks into shared memory
-// in the canonical K-major, no-swizzle layout (8-row x 16-byte core matrices;
-// K-adjacent core matrices 128 B apart, 8-row groups 1024 B apart), thread 0
-// issues four tcgen05.mma (K = 16 each) and commits them to an mbarrier; the
-// next block is copied into the other buffer meanwhile.  The epilogue reads the
-// accumulator back with tcgen05.ld (warp w owns TMEM lanes / rows 32w..32w+31).
+// One CTA of 128 threads computes a 128 x BN tile of C (BN = 128, or 64 when
+// 128-wide tiles would leave most SMs idle).  K advances in blocks of 64
+// through a 4-stage shared-memory ring.  Thread 0 is the producer and the MMA
+// issuer: per block it issues eight 2-D TMA copies per operand, each a box of
+// 8 K-elements (16 B) x 128 (or BN) rows, which lands as the canonical K-major,
+// no-swizzle layout (8-row x 16-byte core matrices; 8-row groups 128 B apart,
+// K-adjacent core matrices one box apart), waits for the block's transaction
+// bytes on the stage's mbarrier, issues four tcgen05.mma (K = 16 each) and
+// commits them to the stage's "empty" mbarrier, after which the stage is
+// refilled.  Rows past M / N are zero-filled by the TMA unit.  The epilogue
+// reads the accumulator with tcgen05.ld (warp w owns TMEM lanes / rows
+// 32w..32w+31).
 //
 // Every wait is bounded (%globaltimer, 2 s): on a timeout the CTA records
-// KERR_TIMEOUT, waits (bounded) for its own outstanding MMAs, releases its TMEM
-// columns and returns.  No load uses cluster multicast.
+// KERR_TIMEOUT, waits (bounded) for its own outstanding copies and MMAs,
+// releases its TMEM columns and returns.  No load uses cluster multicast.
 #pragma once
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
 
@@ -22,11 +29,17 @@
 namespace ech {
 namespace umma {
 
-constexpr int kBM = 128, kBN = 128, kBK = 64;
+constexpr int kBM = 128, kBK = 64;
 constexpr int kThreads = 128;
-constexpr uint32_t kTileBytes = kBM * kBK * 2;           // 16 KiB per operand block
-constexpr uint32_t kSmemBytes = 4 * kTileBytes + 1024;   // A, B double-buffered + alignment slack
-constexpr uint32_t kTmemCols = 128;
+constexpr int kStages = 4;
+constexpr uint32_t kBoxBytesA = kBM * 16;                // one 8-element K slice of 128 rows
+constexpr uint32_t kTileBytesA = kBM * kBK * 2;          // 16 KiB per A block
+template <int BN> struct Tile {
+  static constexpr uint32_t kBoxBytesB = BN * 16;
+  static constexpr uint32_t kTileBytesB = BN * kBK * 2;
+  static constexpr uint32_t kStageBytes = kTileBytesA + kTileBytesB;
+  static constexpr uint32_t kSmemBytes = kStages * kStageBytes + 1024;  // + alignment slack
+};
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -78,45 +91,53 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
-// Copies rows [r0, r0+128) x k-block [k0, k0+64) of a row-major bf16 matrix
-// with `ld` elements per row into the canonical layout at `dst`.  Rows past
-// `rows` are zero-filled.  Each thread moves 16-byte chunks.
-__device__ __forceinline__ void load_block(unsigned char* dst, const __nv_bfloat16* src, int rows, int ld, int r0,
-                                           int k0) {
-  // 128 rows x 8 chunks of 16 B = 1024 chunks; 8 per thread
-#pragma unroll
-  for (int i = 0; i < (kBM * kBK / 8) / kThreads; ++i) {
-    const int c = threadIdx.x + i * kThreads;
-    const int r = c >> 3, kc = c & 7;
-    uint4 v = make_uint4(0, 0, 0, 0);
-    const int gr = r0 + r;
-    if (gr < rows) v = *reinterpret_cast<const uint4*>(src + (size_t)gr * ld + k0 + kc * 8);
-    const uint32_t off = (uint32_t)(r >> 3) * 1024u + (uint32_t)kc * 128u + (uint32_t)(r & 7) * 16u;
-    *reinterpret_cast<uint4*>(dst + off) = v;
-  }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
 }
 
-// M rows of A / C, N rows of B / columns of C, K a multiple of 64; lda, ldb in
-// elements (multiples of 8); C row stride ldc (floats).
-__global__ void __launch_bounds__(kThreads) gemm_bf16_tn(const __nv_bfloat16* __restrict__ A,
-                                                        const __nv_bfloat16* __restrict__ B,
+// One 2-D TMA copy (no multicast): the box at (x = K element, y = row) of the
+// tensor map into shared memory, completing `bytes` on `bar`.  x is a multiple
+// of 8 elements (16 bytes), as TMA requires.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// M rows of A / C, N rows of B / columns of C, K a multiple of 64; the tensor
+// maps describe A [M][K] and B [N][K] (bf16, inner dimension K, boxes 8 x 128
+// and 8 x BN, no swizzle); C row stride ldc (floats).
+template <int BN>
+__global__ void __launch_bounds__(kThreads) gemm_bf16_tn(const __grid_constant__ CUtensorMap tma_a,
+                                                        const __grid_constant__ CUtensorMap tma_b,
                                                         float* __restrict__ C, const float* __restrict__ bias, int M,
-                                                        int N, int K, int lda, int ldb, int ldc, uint32_t* err) {
+                                                        int N, int K, int ldc, uint32_t* err) {
+  using TL = Tile<BN>;
   extern __shared__ unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t done[2];
+  __shared__ __align__(8) uint64_t full[kStages], empty[kStages], fin;
   __shared__ uint32_t tmem_base;
+  __shared__ int failed;
   unsigned char* sm = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+  const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN;
   const int warp = threadIdx.x >> 5;
+  const int nk = K / kBK;
 
   if (threadIdx.x == 0) {
-    mbar_init(&done[0], 1);
-    mbar_init(&done[1], 1);
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(&fin, 1);
+    failed = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tma_a)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tma_b)) : "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_base)),
-                 "r"(kTmemCols)
+                 "r"((uint32_t)BN)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -125,27 +146,33 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tn(const __nv_bfloat16* __
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
 
-  const uint32_t idesc = make_idesc(kBM, kBN);
-  const int nk = K / kBK;
-  uint32_t issued0 = 0, issued1 = 0;  // commits per buffer (parity of the latest = (count - 1) & 1)
-  bool ok = true;
-  for (int kb = 0; kb < nk && ok; ++kb) {
-    const int buf = kb & 1;
-    // the buffer's previous MMAs (block kb - 2) must be done before it is overwritten
-    if (kb >= 2) ok = mbar_wait(&done[buf], (uint32_t)((kb / 2 - 1) & 1));
-    if (__syncthreads_or(!ok)) { ok = false; break; }
-    unsigned char* sa = sm + buf * kTileBytes;
-    unsigned char* sb = sm + (2 + buf) * kTileBytes;
-    load_block(sa, A, M, lda, m0, kb * kBK);
-    load_block(sb, B, N, ldb, n0, kb * kBK);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (threadIdx.x == 0) {
+  if (threadIdx.x == 0) {
+    const uint32_t idesc = make_idesc(kBM, BN);
+    auto stage_a = [&](int s) { return sm + (size_t)s * TL::kStageBytes; };
+    auto stage_b = [&](int s) { return sm + (size_t)s * TL::kStageBytes + kTileBytesA; };
+    auto issue = [&](int kb) {  // block kb into stage kb % kStages
+      const int s = kb % kStages;
+      mbar_expect_tx(&full[s], TL::kStageBytes);
+#pragma unroll
+      for (int kc = 0; kc < kBK / 8; ++kc) {
+        tma_load_2d(stage_a(s) + kc * kBoxBytesA, &tma_a, kb * kBK + kc * 8, m0, &full[s]);
+        tma_load_2d(stage_b(s) + kc * TL::kBoxBytesB, &tma_b, kb * kBK + kc * 8, n0, &full[s]);
+      }
+    };
+    int loaded = 0, consumed = 0;  // blocks whose copies were issued / whose bytes arrived
+    bool ok = true;
+    for (; loaded < nk && loaded < kStages; ++loaded) issue(loaded);
+    for (int kb = 0; kb < nk && ok; ++kb) {
+      const int s = kb % kStages;
+      ok = mbar_wait(&full[s], (uint32_t)((kb / kStages) & 1));
+      if (!ok) break;
+      consumed = kb + 1;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
       for (int ks = 0; ks < kBK / 16; ++ks) {
-        const uint64_t da = make_desc(smem_addr(sa) + ks * 256u, 128u, 1024u);
-        const uint64_t db = make_desc(smem_addr(sb) + ks * 256u, 128u, 1024u);
+        // K = 16 spans two K-adjacent core matrices: two boxes
+        const uint64_t da = make_desc(smem_addr(stage_a(s)) + ks * 2u * kBoxBytesA, kBoxBytesA, 128u);
+        const uint64_t db = make_desc(smem_addr(stage_b(s)) + ks * 2u * TL::kBoxBytesB, TL::kBoxBytesB, 128u);
         const uint32_t acc = (kb > 0 || ks > 0) ? 1u : 0u;
         asm volatile(
             "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
@@ -154,23 +181,33 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tn(const __nv_bfloat16* __
             : "memory");
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       smem_addr(&done[buf]))
+                       smem_addr(&empty[s]))
                    : "memory");
+      // refill the stage block kb - 1 used, once its MMAs are done (block kb's run meanwhile)
+      if (kb >= 1 && loaded < nk) {
+        const int sp = (kb - 1) % kStages;
+        ok = mbar_wait(&empty[sp], (uint32_t)(((kb - 1) / kStages) & 1));
+        if (!ok) break;
+        issue(loaded++);
+      }
     }
-    if (buf) issued1 += 1;
-    else issued0 += 1;
+    if (!ok) {
+      failed = 1;
+      // the copies still in flight land before the CTA's shared memory is given up
+      for (int kb = consumed; kb < loaded; ++kb) (void)mbar_wait(&full[kb % kStages], (uint32_t)((kb / kStages) & 1));
+    }
+    // arrives once every MMA this thread issued has completed
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(&fin))
+                 : "memory");
   }
-  // wait for the last block's MMAs (a commit covers every earlier MMA of the thread)
-  if (ok && nk > 0) {
-    const int last = (nk - 1) & 1;
-    ok = mbar_wait(&done[last], ((last ? issued1 : issued0) - 1) & 1);
-  }
-  ok = !__syncthreads_or(!ok);
+  __syncthreads();
+  bool ok = mbar_wait(&fin, 0u);
+  ok = !__syncthreads_or(!ok || failed);
   if (ok) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const int row = m0 + warp * 32 + (threadIdx.x & 31);
 #pragma unroll 1
-    for (int c0 = 0; c0 < kBN; c0 += 16) {
+    for (int c0 = 0; c0 < BN; c0 += 16) {
       uint32_t r[16];
       const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
       asm volatile(
@@ -187,16 +224,13 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tn(const __nv_bfloat16* __
         }
       }
     }
-  } else {
-    if (threadIdx.x == 0) atomicOr(err, (uint32_t)KERR_TIMEOUT);
-    // let whatever this CTA issued finish (bounded) before the columns are released
-    if (issued0) (void)mbar_wait(&done[0], (issued0 - 1) & 1);
-    if (issued1) (void)mbar_wait(&done[1], (issued1 - 1) & 1);
+  } else if (threadIdx.x == 0) {
+    atomicOr(err, (uint32_t)KERR_TIMEOUT);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN) : "memory");
 }
 
 }  // namespace umma
