@@ -351,6 +351,8 @@ template <class T, int K_> struct JetOrder<dm::Jet<T, K_>> { static constexpr in
 // x * 0 + z with one rounding: z unchanged (+0 stays +0) when x is finite, NaN otherwise.
 __device__ __forceinline__ float fma_zero(float x, float z) { return __fmaf_rn(x, 0.0f, z); }
 __device__ __forceinline__ double fma_zero(double x, double z) { return __fma_rn(x, 0.0, z); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
 
 // s + x with Neumaier's compensation (Neumaier, 1974): the rounding error of
 // the addition accumulates in c.
@@ -954,16 +956,28 @@ template <class V, int P, bool DN = true> struct FwdExec {
       ring_drain(*st.rg);
       return false;
     } else {
-      // (launches with compensated chains run plans without dense groups)
-      return dense_impl(st, m, n);
+      // (launches with compensated chains run plans without dense groups; the
+      // lowering forms only full groups, m == kDenseMax)
+      if constexpr (JetOrder<V>::K > 1) {
+        // device Rademacher signs and basis directions: every direction
+        // component is +-1 or 0
+        if (kp.dir_mode >= 2 && kp.dir_mode <= 4) return dense_impl<true, true>(st, m, n);
+      }
+      return dense_impl<true, false>(st, m, n);
     }
   }
+  // FULL: the group has kDenseMax outputs, so no output needs a bound (the
+  // per-output bounds of the general form cost registers and instructions in
+  // every group).  UNITV: the direction components of input-direct operands
+  // are +-1 or 0, so c * v is exact and c1 + c * v rounds like one fused
+  // multiply-add.
+  template <bool FULL, bool UNITV>
   __device__ __forceinline__ bool dense_impl(Stream<32>& st, uint32_t m, uint32_t n) const {
     using T = typename dm::VT<V>::S;
     constexpr int MX = kDenseMax > 1 ? kDenseMax : 2;
     constexpr int KJ = JetOrder<V>::K > 0 ? JetOrder<V>::K : 1;
     constexpr int PER = sizeof(T) == 4 ? 8 : 4;  // constants per record
-    if (m < 1 || m > (uint32_t)kDenseMax) {
+    if (m < 1 || m > (uint32_t)kDenseMax || (FULL && m != (uint32_t)kDenseMax)) {
       if (threadIdx.x == 0) atomicOr(kp.err, (uint32_t)KERR_BADINS);
       ring_drain(*st.rg);
       return false;
@@ -971,13 +985,13 @@ template <class V, int P, bool DN = true> struct FwdExec {
     V acc[MX][P];
 #pragma unroll
     for (int jj = 0; jj < MX; jj += 2) {
-      if ((uint32_t)jj < m) {
+      if (FULL || (uint32_t)jj < m) {
         const unsigned char* rec = st.next();
         if (rec == nullptr) return false;
         const double2 imm = *reinterpret_cast<const double2*>(rec);
         const uint4 w = *reinterpret_cast<const uint4*>(rec + 16);
         ld(w.z & 0xFFu, w.x, imm.x, acc[jj]);
-        if ((uint32_t)jj + 1 < m) ld((w.z >> 8) & 0xFFu, w.y, imm.y, acc[jj + 1]);
+        if (FULL || (uint32_t)jj + 1 < m) ld((w.z >> 8) & 0xFFu, w.y, imm.y, acc[jj + 1]);
       }
     }
     // Dual: the eps part of c x is c eps + 0 re; the zero products commute with
@@ -1019,7 +1033,7 @@ template <class V, int P, bool DN = true> struct FwdExec {
         }
 #pragma unroll
         for (int jj = 0; jj < MX; jj += PER) {
-          if ((uint32_t)jj < m) {
+          if (FULL || (uint32_t)jj < m) {
             const unsigned char* crec = st.next();
             if (crec == nullptr) return false;
             T cs[PER];
@@ -1031,12 +1045,15 @@ template <class V, int P, bool DN = true> struct FwdExec {
               if (direct) {
 #pragma unroll
                 for (int j = 0; j < PER; ++j) {
-                  if (jj + j < MX && (uint32_t)(jj + j) < m) {
+                  if (jj + j < MX && (FULL || (uint32_t)(jj + j) < m)) {
 #pragma unroll
                     for (int p = 0; p < P; ++p) {
                       V& a = acc[jj + j < MX ? jj + j : 0][p];
                       a.c[0] = a.c[0] + cs[j] * x[p].c[0];
-                      if constexpr (KJ > 1) a.c[1] = a.c[1] + cs[j] * x[p].c[1];
+                      if constexpr (KJ > 1) {
+                        if constexpr (UNITV) a.c[1] = fma_rn(cs[j], x[p].c[1], a.c[1]);
+                        else a.c[1] = a.c[1] + cs[j] * x[p].c[1];
+                      }
                     }
                   }
                 }
@@ -1045,7 +1062,7 @@ template <class V, int P, bool DN = true> struct FwdExec {
             }
 #pragma unroll
             for (int j = 0; j < PER; ++j) {
-              if (jj + j < MX && (uint32_t)(jj + j) < m) {
+              if (jj + j < MX && (FULL || (uint32_t)(jj + j) < m)) {
                 const T c = cs[j];
 #pragma unroll
                 for (int p = 0; p < P; ++p) {
@@ -1080,7 +1097,7 @@ template <class V, int P, bool DN = true> struct FwdExec {
     }
 #pragma unroll
     for (int jj = 0; jj < MX; jj += 2) {
-      if ((uint32_t)jj < m) {
+      if (FULL || (uint32_t)jj < m) {
         const unsigned char* rec = st.next();
         if (rec == nullptr) return false;
         const uint4 w0 = *reinterpret_cast<const uint4*>(rec);
@@ -1088,7 +1105,7 @@ template <class V, int P, bool DN = true> struct FwdExec {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int j = jj + h;
-          if (j >= MX || (uint32_t)j >= m) continue;
+          if (j >= MX || (!FULL && (uint32_t)j >= m)) continue;
           if constexpr (JetOrder<V>::K > 0) {
 #pragma unroll
             for (int p = 0; p < P; ++p) {

@@ -503,7 +503,9 @@ Plan build_plan(const HostTape& t, Kind kind, uint32_t smem_cap, uint32_t dense_
         if (ch.acc0 >= 0 && (uint64_t)ch.acc0 >= lead.first) break;
         ++m;
       }
-      if (m >= 2) {
+      // only full groups: the kernels' dense executor is specialised for
+      // exactly dense_max outputs; shorter runs stay chains
+      if (m == dense_max) {
         for (uint32_t k = 0; k < m; ++k) group_of[c + k] = (int32_t)groups.size();
         groups.push_back({c, m});
       }
