@@ -39,7 +39,7 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC
            "--expt-relaxed-constexpr", "-I", CSRC, "-I", os.path.join(ROOT, "include")]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-ffp-contract=off", "-I", CSRC]
 
-CU_SOURCES = ["abi.cu", "launch.cu", "stde.cu", "noalloc.cu", "mlp.cu"]
+CU_SOURCES = ["k_jet3sp.cu", "abi.cu", "launch.cu", "stde.cu", "noalloc.cu", "mlp.cu"]
 # Sweep-kernel units, compiled twice: without (ECH_DN=0) and with (ECH_DN=1)
 # the dense-group executor.  Listed longest compile first.
 DN_SOURCES = ["k_jet3.cu", "k_jet2.cu", "k_dual.cu", "k_jet4.cu", "k_jet5.cu", "k_plain.cu", "k_multi.cu",
@@ -85,6 +85,12 @@ def build(verbose: bool = False, jobs: int | None = None, variant: str = "") -> 
     build_dir, lib, extra = VARIANTS[variant]
     os.makedirs(build_dir, exist_ok=True)
     cmds, objs = [], []
+    for s in CU_SOURCES:
+        src = os.path.join(CSRC, s)
+        obj = os.path.join(build_dir, s + ".o")
+        objs.append(obj)
+        if _newer(src, obj, _deps(src)):
+            cmds.append([NVCC, *ARCH, *NVFLAGS, *extra, "-c", src, "-o", obj])
     for dn in ("1", "0"):
         for s in DN_SOURCES:
             src = os.path.join(CSRC, s)
@@ -92,12 +98,6 @@ def build(verbose: bool = False, jobs: int | None = None, variant: str = "") -> 
             objs.append(obj)
             if _newer(src, obj, _deps(src)):
                 cmds.append([NVCC, *ARCH, *NVFLAGS, *extra, f"-DECH_DN={dn}", "-c", src, "-o", obj])
-    for s in CU_SOURCES:
-        src = os.path.join(CSRC, s)
-        obj = os.path.join(build_dir, s + ".o")
-        objs.append(obj)
-        if _newer(src, obj, _deps(src)):
-            cmds.append([NVCC, *ARCH, *NVFLAGS, *extra, "-c", src, "-o", obj])
     for s in CXX_SOURCES:
         src = os.path.join(CSRC, s)
         obj = os.path.join(build_dir, s + ".o")

@@ -488,7 +488,11 @@ template <class T> struct GradOut<dm::Dual<T>> {
 // raise the kernel's register demand for every program, so programs without
 // dense groups run an instantiation without them (DN = false), where D_DENSE is
 // an invalid instruction.
-template <class V, int P, bool DN = true> struct FwdExec {
+// SP (shared point): the P units of a thread are directions of one point
+// (point-direction launches with S % P == 0), so coefficient 0 of every jet
+// is the same for all P units; the dense executor keeps one coefficient-0
+// accumulator per output for them.
+template <class V, int P, bool DN = true, bool SP = false> struct FwdExec {
   using Kd = typename dm::KindOf<V>::K;
   using C = Col<V, P>;
   const KParams& kp;
@@ -1012,6 +1016,14 @@ template <class V, int P, bool DN = true> struct FwdExec {
 #pragma unroll
           for (int k = 0; k < KJ; ++k) acc[j][p].c[k] = acc[j][p].c[k] + T(0);
     }
+    // shared point: one coefficient-0 accumulator per output serves all P units
+    constexpr bool kSP = SP && JetOrder<V>::K > 1 && P > 1;
+    constexpr int K0 = kSP ? 1 : 0;  // first coefficient accumulated per unit
+    T a0[kSP ? MX : 1];
+    if constexpr (kSP) {
+#pragma unroll
+      for (int j = 0; j < MX; ++j) a0[j] = acc[j][0].c[0];
+    }
 #pragma unroll 1
     for (uint32_t q0 = 0; q0 < n; q0 += 4) {
       const unsigned char* orec = st.next();
@@ -1046,10 +1058,14 @@ template <class V, int P, bool DN = true> struct FwdExec {
 #pragma unroll
                 for (int j = 0; j < PER; ++j) {
                   if (jj + j < MX && (FULL || (uint32_t)(jj + j) < m)) {
+                    if constexpr (kSP) {
+                      T& s0 = a0[jj + j < MX ? jj + j : 0];
+                      s0 = s0 + cs[j] * x[0].c[0];
+                    }
 #pragma unroll
                     for (int p = 0; p < P; ++p) {
                       V& a = acc[jj + j < MX ? jj + j : 0][p];
-                      a.c[0] = a.c[0] + cs[j] * x[p].c[0];
+                      if constexpr (!kSP) a.c[0] = a.c[0] + cs[j] * x[p].c[0];
                       if constexpr (KJ > 1) {
                         if constexpr (UNITV) a.c[1] = fma_rn(cs[j], x[p].c[1], a.c[1]);
                         else a.c[1] = a.c[1] + cs[j] * x[p].c[1];
@@ -1064,12 +1080,16 @@ template <class V, int P, bool DN = true> struct FwdExec {
             for (int j = 0; j < PER; ++j) {
               if (jj + j < MX && (FULL || (uint32_t)(jj + j) < m)) {
                 const T c = cs[j];
+                if constexpr (kSP) {
+                  T& s0 = a0[jj + j < MX ? jj + j : 0];
+                  s0 = s0 + c * x[0].c[0];
+                }
 #pragma unroll
                 for (int p = 0; p < P; ++p) {
                   V& a = acc[jj + j < MX ? jj + j : 0][p];
                   if constexpr (JetOrder<V>::K > 0) {
 #pragma unroll
-                    for (int k = 0; k < KJ; ++k) a.c[k] = a.c[k] + c * x[p].c[k];
+                    for (int k = K0; k < KJ; ++k) a.c[k] = a.c[k] + c * x[p].c[k];
                   } else if constexpr (IsDual<V>::v) {
                     a.re = a.re + c * x[p].re;
                     a.eps = a.eps + c * x[p].eps;
@@ -1084,16 +1104,24 @@ template <class V, int P, bool DN = true> struct FwdExec {
         if constexpr (JetOrder<V>::K > 1) {
 #pragma unroll
           for (int p = 0; p < P; ++p) {
+            // (shared point: coefficient 0 is unit 0's for every unit)
             if (direct) {
-              z[p][0] = fma_zero(x[p].c[0], z[p][0]);
+              z[p][0] = fma_zero(x[kSP ? 0 : p].c[0], z[p][0]);
               if constexpr (KJ > 2) z[p][1] = fma_zero(x[p].c[1], z[p][1]);
             } else {
+              z[p][0] = fma_zero(x[kSP ? 0 : p].c[0], z[p][0]);
 #pragma unroll
-              for (int k = 0; k + 1 < KJ; ++k) z[p][k] = fma_zero(x[p].c[k], z[p][k]);
+              for (int k = 1; k + 1 < KJ; ++k) z[p][k] = fma_zero(x[p].c[k], z[p][k]);
             }
           }
         }
       }
+    }
+    if constexpr (kSP) {
+#pragma unroll
+      for (int j = 0; j < MX; ++j)
+#pragma unroll
+        for (int p = 0; p < P; ++p) acc[j][p].c[0] = a0[j];
     }
 #pragma unroll
     for (int jj = 0; jj < MX; jj += 2) {
@@ -1480,8 +1508,9 @@ template <class V, int P, bool DN = true> struct RevExec {
       }
     }
   }
-  // A gather tile (DGatherTargets): T targets whose contributions read the
-  // same chain adjoints in the same order, every constant nonzero.  Each source
+  // A gather tile (DGatherTargets): kGT targets (the lowering forms only full
+  // tiles, so no target needs a bound) whose contributions read the same chain
+  // adjoints in the same order, every constant nonzero.  Each source
   // is loaded and zero-tested once for the tile and added to every target, in
   // source order per target, as gather_update does.  Dual values: every target
   // receives the same zero products (one per source that is not skipped), so
@@ -1497,7 +1526,7 @@ template <class V, int P, bool DN = true> struct RevExec {
       return false;
     } else {
       using S = typename dm::VT<V>::S;
-      if (T < 2 || T > (uint32_t)kGT) {
+      if (T != (uint32_t)kGT) {  // the lowering forms only full tiles
         if (threadIdx.x == 0) atomicOr(kp.err, (uint32_t)KERR_BADINS);
         ring_drain(*st.rg);
         return false;
@@ -1510,7 +1539,7 @@ template <class V, int P, bool DN = true> struct RevExec {
       V cur[kGT][P];
 #pragma unroll
       for (int k = 0; k < kGT; ++k)
-        if ((uint32_t)k < T) lc_load(loc((tx[k] & GT_GLOB) != 0, tx[k] & GT_OFF), (tx[k] & GT_INIT) != 0, cur[k]);
+        lc_load(loc((tx[k] & GT_GLOB) != 0, tx[k] & GT_OFF), (tx[k] & GT_INIT) != 0, cur[k]);
       S dz[P];
 #pragma unroll
       for (int p = 0; p < P; ++p) dz[p] = -S(0);
@@ -1538,28 +1567,24 @@ template <class V, int P, bool DN = true> struct RevExec {
               dz[p] = fma_zero(t[p].re, dz[p]);
 #pragma unroll
               for (int k = 0; k < kGT; ++k) {
-                if ((uint32_t)k < T) {
-                  cur[k][p].re = cur[k][p].re + cs[k] * t[p].re;
-                  cur[k][p].eps = cur[k][p].eps + cs[k] * t[p].eps;
-                }
+                cur[k][p].re = cur[k][p].re + cs[k] * t[p].re;
+                cur[k][p].eps = cur[k][p].eps + cs[k] * t[p].eps;
               }
             } else {
 #pragma unroll
               for (int k = 0; k < kGT; ++k)
-                if ((uint32_t)k < T) cur[k][p] = Kd::add(cur[k][p], Kd::mul(dm::VT<V>::cst_s(cs[k]), t[p]));
+                cur[k][p] = Kd::add(cur[k][p], Kd::mul(dm::VT<V>::cst_s(cs[k]), t[p]));
             }
           }
         }
       }
 #pragma unroll
       for (int k = 0; k < kGT; ++k) {
-        if ((uint32_t)k < T) {
-          if constexpr (IsDual<V>::v) {
+        if constexpr (IsDual<V>::v) {
 #pragma unroll
-            for (int p = 0; p < P; ++p) cur[k][p].eps = cur[k][p].eps + dz[p];
-          }
-          C::st(loc((tx[k] & GT_GLOB) != 0, tx[k] & GT_OFF), cur[k]);
+          for (int p = 0; p < P; ++p) cur[k][p].eps = cur[k][p].eps + dz[p];
         }
+        C::st(loc((tx[k] & GT_GLOB) != 0, tx[k] & GT_OFF), cur[k]);
       }
       return true;
     }
@@ -1720,7 +1745,7 @@ template <class V, int P, bool DN = true> struct RevExec {
 // One tile of `kp.tile` units: the forward program (with trajectory saves when
 // REV), then the reverse program.  `gbase` is the CTA's global scratch region.
 // Returns false when a bounded wait gave up (every thread sees the same value).
-template <class V, int P, bool REV, bool DN>
+template <class V, int P, bool REV, bool DN, bool SP = false>
 __device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned char* sm, unsigned char* gbase,
                                            uint64_t t) {
   const uint32_t tile = kp.tile;
@@ -1730,7 +1755,7 @@ __device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned
                                    : gbase + (size_t)kp.far_slots * tile * sizeof(V) + colb;
   const uint64_t unit0 = t * tile + (uint64_t)threadIdx.x * P;
   uint32_t* bits = kp.dir_bits ? reinterpret_cast<uint32_t*>(rg.buf + kp.dir_bits) + threadIdx.x * P : nullptr;
-  FwdExec<V, P, DN> fx{kp, sm, gs, tj, unit0, bits, {}, {}, {}, {}, {}};
+  FwdExec<V, P, DN, SP> fx{kp, sm, gs, tj, unit0, bits, {}, {}, {}, {}, {}};
 #pragma unroll
   for (int p = 0; p < P; ++p) {
     fx.valid[p] = unit0 + p < kp.n_units;
@@ -1779,7 +1804,8 @@ __device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned
 // REV = true : forward program with trajectory saves, then the reverse program
 //              (gradient for plain values, HVP for Dual values).
 // DN: with the dense-group executor (programs that hold D_DENSE instructions).
-template <class V, int P, bool REV, bool DN>
+// SP: the P units of a thread are directions of one point (FwdExec).
+template <class V, int P, bool REV, bool DN, bool SP = false>
 __global__ void __launch_bounds__(256) sweep_kernel(KParams kp) {
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   __shared__ __align__(8) uint64_t full[kStages];
@@ -1793,7 +1819,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(KParams kp) {
   unsigned char* gbase = reinterpret_cast<unsigned char*>(kp.scratch) + blockIdx.x * kp.scratch_stride_bytes;
   const uint64_t ntiles = (kp.n_units + kp.tile - 1) / kp.tile;
   for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x)
-    if (!sweep_tile<V, P, REV, DN>(kp, rg, sm, gbase, t)) return;
+    if (!sweep_tile<V, P, REV, DN, SP>(kp, rg, sm, gbase, t)) return;
 }
 
 // ───────────────────────────── many tapes, one launch ───────────────────────

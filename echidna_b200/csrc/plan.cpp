@@ -1347,7 +1347,8 @@ bool encode_plan(const Plan& p, uint32_t tile, uint32_t vbytes, bool f32, DevPro
         if (tmax >= 2 && tileable(hpos[h]))
           while (h + T < (uint32_t)in.aux && T < tmax && tileable(hpos[h + T]) && same_sources(hpos[h], hpos[h + T]))
             ++T;
-        if (T >= 2) {
+        // only full tiles (the kernel's tile executor has no per-target bounds)
+        if (T >= 2 && T == tmax) {
           const uint32_t ns = p.gathers[hpos[h]].n;
           DRTerm head{};
           head.kind = 1;

@@ -149,3 +149,47 @@ def test_hessian_diagonal_basis_directions_bit_exact(ctx, f64):
     for b in range(B):
         c = o.taylor(np.tile(X[b], (n, 1)), E, 3)
         assert _bits_equal(d[b], (dt(2) * c[2]).astype(dt)), b
+
+
+@pytest.mark.parametrize("f64", [True, False])
+@pytest.mark.parametrize("mode", ["shared", "rademacher", "basis"])
+@pytest.mark.parametrize("S", [16, 15])
+def test_two_units_per_thread_share_the_point(ctx, f64, mode, S):
+    # two units per thread with S even: both are directions of one point, and
+    # the dense groups accumulate coefficient 0 once for the pair (S odd runs
+    # the per-unit form).  Results equal one unit per thread bit for bit.
+    torch = pytest.importorskip("torch")
+    from echidna_b200.learned import hessian_diagonals
+    n, m, B, seed = 40, 24, 150, 0x5EED
+    tape = _layer_tape(n, m, 11, True)
+    dt = np.float64 if f64 else np.float32
+    rng = np.random.default_rng(12)
+    X = rng.normal(size=(B, n)).astype(dt)
+    X[3, 4] = np.inf
+    X[7, 0] = np.nan
+    D = rng.normal(size=(S, n)).astype(dt)
+    gt = ctx.upload_tape_f64(tape) if f64 else ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(tape))
+
+    def run(ppt):
+        ctx.set_launch(128, ppt, 0)
+        try:
+            if mode == "shared":
+                return _stats(laplacian_batch(ctx, gt, X, S, D, DIR_SHARED))
+            if mode == "rademacher":
+                return _stats(laplacian_batch(ctx, gt, X, S, None, DIR_RADEMACHER, seed=seed))
+            d = hessian_diagonals(ctx, gt, torch.tensor(X, device="cuda")).cpu().numpy()
+            return d, None
+        finally:
+            ctx.set_launch(0, 0, 0)
+            ctx.set_autotune(True)
+
+    a, na = run(2)
+    b, nb = run(1)
+    assert _bits_equal(a, b), (mode, S)
+    if na is not None:
+        assert np.array_equal(na, nb)
+    if mode == "shared":
+        # and the per-unit slot path (no input-direct terms)
+        c, nc = _stats(laplacian_batch(ctx, gt, X, S, np.ascontiguousarray(np.broadcast_to(D, (B, S, n))),
+                                       DIR_PER_POINT))
+        assert _bits_equal(a, c)
