@@ -439,9 +439,6 @@ static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_
   if (s != ECH_OK) return s;
   const Plan& p = dp->host;
   c.req.dense = dp->needs_dense() || c.dense_kernel;
-  // a thread's P units are directions of one point: units u = point * S + s
-  // and every thread starts at a multiple of P
-  c.req.shared_point = direct && K == 3 && c.req.P > 1 && io.S % (uint32_t)c.req.P == 0;
   const uint32_t regs = std::max<uint32_t>(p.smem_regs, 1);
   c.smem = kRingBytes + (size_t)regs * c.tile * c.vbytes;
   const uint32_t dir_bits = bits_bytes ? (uint32_t)c.smem : 0u;

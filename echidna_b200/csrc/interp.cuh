@@ -488,11 +488,7 @@ template <class T> struct GradOut<dm::Dual<T>> {
 // raise the kernel's register demand for every program, so programs without
 // dense groups run an instantiation without them (DN = false), where D_DENSE is
 // an invalid instruction.
-// SP (shared point): the P units of a thread are directions of one point
-// (point-direction launches with S % P == 0), so coefficient 0 of every jet
-// is the same for all P units; the dense executor keeps one coefficient-0
-// accumulator per output for them.
-template <class V, int P, bool DN = true, bool SP = false> struct FwdExec {
+template <class V, int P, bool DN = true> struct FwdExec {
   using Kd = typename dm::KindOf<V>::K;
   using C = Col<V, P>;
   const KParams& kp;
@@ -1016,14 +1012,6 @@ template <class V, int P, bool DN = true, bool SP = false> struct FwdExec {
 #pragma unroll
           for (int k = 0; k < KJ; ++k) acc[j][p].c[k] = acc[j][p].c[k] + T(0);
     }
-    // shared point: one coefficient-0 accumulator per output serves all P units
-    constexpr bool kSP = SP && JetOrder<V>::K > 1 && P > 1;
-    constexpr int K0 = kSP ? 1 : 0;  // first coefficient accumulated per unit
-    T a0[kSP ? MX : 1];
-    if constexpr (kSP) {
-#pragma unroll
-      for (int j = 0; j < MX; ++j) a0[j] = acc[j][0].c[0];
-    }
 #pragma unroll 1
     for (uint32_t q0 = 0; q0 < n; q0 += 4) {
       const unsigned char* orec = st.next();
@@ -1058,14 +1046,10 @@ template <class V, int P, bool DN = true, bool SP = false> struct FwdExec {
 #pragma unroll
                 for (int j = 0; j < PER; ++j) {
                   if (jj + j < MX && (FULL || (uint32_t)(jj + j) < m)) {
-                    if constexpr (kSP) {
-                      T& s0 = a0[jj + j < MX ? jj + j : 0];
-                      s0 = s0 + cs[j] * x[0].c[0];
-                    }
 #pragma unroll
                     for (int p = 0; p < P; ++p) {
                       V& a = acc[jj + j < MX ? jj + j : 0][p];
-                      if constexpr (!kSP) a.c[0] = a.c[0] + cs[j] * x[p].c[0];
+                      a.c[0] = a.c[0] + cs[j] * x[p].c[0];
                       if constexpr (KJ > 1) {
                         if constexpr (UNITV) a.c[1] = fma_rn(cs[j], x[p].c[1], a.c[1]);
                         else a.c[1] = a.c[1] + cs[j] * x[p].c[1];
@@ -1080,16 +1064,12 @@ template <class V, int P, bool DN = true, bool SP = false> struct FwdExec {
             for (int j = 0; j < PER; ++j) {
               if (jj + j < MX && (FULL || (uint32_t)(jj + j) < m)) {
                 const T c = cs[j];
-                if constexpr (kSP) {
-                  T& s0 = a0[jj + j < MX ? jj + j : 0];
-                  s0 = s0 + c * x[0].c[0];
-                }
 #pragma unroll
                 for (int p = 0; p < P; ++p) {
                   V& a = acc[jj + j < MX ? jj + j : 0][p];
                   if constexpr (JetOrder<V>::K > 0) {
 #pragma unroll
-                    for (int k = K0; k < KJ; ++k) a.c[k] = a.c[k] + c * x[p].c[k];
+                    for (int k = 0; k < KJ; ++k) a.c[k] = a.c[k] + c * x[p].c[k];
                   } else if constexpr (IsDual<V>::v) {
                     a.re = a.re + c * x[p].re;
                     a.eps = a.eps + c * x[p].eps;
@@ -1104,24 +1084,16 @@ template <class V, int P, bool DN = true, bool SP = false> struct FwdExec {
         if constexpr (JetOrder<V>::K > 1) {
 #pragma unroll
           for (int p = 0; p < P; ++p) {
-            // (shared point: coefficient 0 is unit 0's for every unit)
             if (direct) {
-              z[p][0] = fma_zero(x[kSP ? 0 : p].c[0], z[p][0]);
+              z[p][0] = fma_zero(x[p].c[0], z[p][0]);
               if constexpr (KJ > 2) z[p][1] = fma_zero(x[p].c[1], z[p][1]);
             } else {
-              z[p][0] = fma_zero(x[kSP ? 0 : p].c[0], z[p][0]);
 #pragma unroll
-              for (int k = 1; k + 1 < KJ; ++k) z[p][k] = fma_zero(x[p].c[k], z[p][k]);
+              for (int k = 0; k + 1 < KJ; ++k) z[p][k] = fma_zero(x[p].c[k], z[p][k]);
             }
           }
         }
       }
-    }
-    if constexpr (kSP) {
-#pragma unroll
-      for (int j = 0; j < MX; ++j)
-#pragma unroll
-        for (int p = 0; p < P; ++p) acc[j][p].c[0] = a0[j];
     }
 #pragma unroll
     for (int jj = 0; jj < MX; jj += 2) {
@@ -1745,7 +1717,7 @@ template <class V, int P, bool DN = true> struct RevExec {
 // One tile of `kp.tile` units: the forward program (with trajectory saves when
 // REV), then the reverse program.  `gbase` is the CTA's global scratch region.
 // Returns false when a bounded wait gave up (every thread sees the same value).
-template <class V, int P, bool REV, bool DN, bool SP = false>
+template <class V, int P, bool REV, bool DN>
 __device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned char* sm, unsigned char* gbase,
                                            uint64_t t) {
   const uint32_t tile = kp.tile;
@@ -1755,7 +1727,7 @@ __device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned
                                    : gbase + (size_t)kp.far_slots * tile * sizeof(V) + colb;
   const uint64_t unit0 = t * tile + (uint64_t)threadIdx.x * P;
   uint32_t* bits = kp.dir_bits ? reinterpret_cast<uint32_t*>(rg.buf + kp.dir_bits) + threadIdx.x * P : nullptr;
-  FwdExec<V, P, DN, SP> fx{kp, sm, gs, tj, unit0, bits, {}, {}, {}, {}, {}};
+  FwdExec<V, P, DN> fx{kp, sm, gs, tj, unit0, bits, {}, {}, {}, {}, {}};
 #pragma unroll
   for (int p = 0; p < P; ++p) {
     fx.valid[p] = unit0 + p < kp.n_units;
@@ -1804,8 +1776,7 @@ __device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned
 // REV = true : forward program with trajectory saves, then the reverse program
 //              (gradient for plain values, HVP for Dual values).
 // DN: with the dense-group executor (programs that hold D_DENSE instructions).
-// SP: the P units of a thread are directions of one point (FwdExec).
-template <class V, int P, bool REV, bool DN, bool SP = false>
+template <class V, int P, bool REV, bool DN>
 __global__ void __launch_bounds__(256) sweep_kernel(KParams kp) {
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   __shared__ __align__(8) uint64_t full[kStages];
@@ -1819,7 +1790,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(KParams kp) {
   unsigned char* gbase = reinterpret_cast<unsigned char*>(kp.scratch) + blockIdx.x * kp.scratch_stride_bytes;
   const uint64_t ntiles = (kp.n_units + kp.tile - 1) / kp.tile;
   for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x)
-    if (!sweep_tile<V, P, REV, DN, SP>(kp, rg, sm, gbase, t)) return;
+    if (!sweep_tile<V, P, REV, DN>(kp, rg, sm, gbase, t)) return;
 }
 
 // ───────────────────────────── many tapes, one launch ───────────────────────

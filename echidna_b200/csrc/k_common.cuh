@@ -21,9 +21,9 @@
 
 namespace ech {
 
-template <class V, int P, bool REV, bool DN, bool SP = false>
+template <class V, int P, bool REV, bool DN>
 cudaError_t launch_one(const KParams& kp, int grid, int block, size_t smem, cudaStream_t st, int* blocks_per_sm) {
-  auto fn = sweep_kernel<V, P, REV, DN, SP>;
+  auto fn = sweep_kernel<V, P, REV, DN>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   if (grid == 0) {

@@ -18,7 +18,6 @@ struct LaunchReq {
   int P = 1;      // points per thread
   bool rev = false;
   bool dense = false;  // the program holds dense groups: the kernel with the dense-group executor
-  bool shared_point = false;  // order-3 jets, P > 1: a thread's units are directions of one point
 };
 
 size_t value_bytes(const LaunchReq& r);
@@ -32,10 +31,6 @@ cudaError_t launch_dual(const LaunchReq& r, const KParams& kp, int grid, int blo
                         int* blocks_per_sm);
 cudaError_t launch_jet(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
                        int* blocks_per_sm);
-// Order-3 jets with dense groups at 2 units per thread that share one point
-// (r.shared_point): the dense executor accumulates coefficient 0 once.
-cudaError_t launch_jet3_shared_point(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem,
-                                     cudaStream_t st, int* blocks_per_sm);
 
 // Launch (grid > 0) or query occupancy (grid == 0, result in *blocks_per_sm).
 cudaError_t launch_sweep(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,

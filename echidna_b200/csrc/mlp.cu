@@ -183,12 +183,13 @@ cudaError_t gemm_tiles(const bf16* A, const bf16* B, float* C, const float* bias
   return cudaGetLastError();
 }
 
-// 128 x 128 tiles, or 128 x 64 when the 128-wide grid would cover less than
-// half of the 148 SMs.
+// 128 x 256 tiles when they still give each of the 148 SMs one; else 128 x 128,
+// or 128 x 64 when the 128-wide grid would cover less than half of the SMs.
 cudaError_t gemm(const bf16* A, const bf16* B, float* C, const float* bias, int M, int N, int K, int lda, int ldb,
                  int ldc, uint32_t* err, cudaStream_t st) {
-  const long tiles128 = (long)((M + 127) / 128) * ((N + 127) / 128);
-  if (tiles128 < 74) return gemm_tiles<64>(A, B, C, bias, M, N, K, lda, ldb, ldc, err, st);
+  const long rows = (M + 127) / 128;
+  if (rows * ((N + 255) / 256) >= 148) return gemm_tiles<256>(A, B, C, bias, M, N, K, lda, ldb, ldc, err, st);
+  if (rows * ((N + 127) / 128) < 74) return gemm_tiles<64>(A, B, C, bias, M, N, K, lda, ldb, ldc, err, st);
   return gemm_tiles<128>(A, B, C, bias, M, N, K, lda, ldb, ldc, err, st);
 }
 

@@ -3,9 +3,10 @@
 //
 //   C[M x N] (fp32) = A[M x K] (bf16, row-major) * B[N x K]^T (bf16, row-major)  (+ bias[N])
 //
-// One CTA of 128 threads computes a 128 x BN tile of C (BN = 128, or 64 when
-// 128-wide tiles would leave most SMs idle).  K advances in blocks of 64
-// through a 4-stage shared-memory ring.  Thread 0 is the producer and the MMA
+// One CTA of 128 threads computes a 128 x BN tile of C (BN = 256 when such
+// tiles still give every SM one, else 128, or 64 when 128-wide tiles would
+// leave most SMs idle).  K advances in blocks of 64 through a shared-memory
+// ring of about 192 KiB (4 to 6 stages).  Thread 0 is the producer and the MMA
 // issuer: per block it issues eight 2-D TMA copies per operand, each a box of
 // 8 K-elements (16 B) x 128 (or BN) rows, which lands as the canonical K-major,
 // no-swizzle layout (8-row x 16-byte core matrices; 8-row groups 128 B apart,
@@ -31,13 +32,15 @@ namespace umma {
 
 constexpr int kBM = 128, kBK = 64;
 constexpr int kThreads = 128;
-constexpr int kStages = 4;
 constexpr uint32_t kBoxBytesA = kBM * 16;                // one 8-element K slice of 128 rows
 constexpr uint32_t kTileBytesA = kBM * kBK * 2;          // 16 KiB per A block
+// Stages: as many as fit about 192 KiB, so that the copies in flight cover a
+// TMA round trip (6 stages of 32 KiB at BN = 128, 4 of 48 KiB at BN = 256).
 template <int BN> struct Tile {
   static constexpr uint32_t kBoxBytesB = BN * 16;
   static constexpr uint32_t kTileBytesB = BN * kBK * 2;
   static constexpr uint32_t kStageBytes = kTileBytesA + kTileBytesB;
+  static constexpr int kStages = (int)((192u * 1024u) / kStageBytes) > 8 ? 8 : (int)((192u * 1024u) / kStageBytes);
   static constexpr uint32_t kSmemBytes = kStages * kStageBytes + 1024;  // + alignment slack
 };
 
@@ -115,8 +118,9 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tn(const __grid_constant__
                                                         float* __restrict__ C, const float* __restrict__ bias, int M,
                                                         int N, int K, int ldc, uint32_t* err) {
   using TL = Tile<BN>;
+  static_assert(TL::kStages >= 2, "at least two stages");
   extern __shared__ unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t full[kStages], empty[kStages], fin;
+  __shared__ __align__(8) uint64_t full[TL::kStages], empty[TL::kStages], fin;
   __shared__ uint32_t tmem_base;
   __shared__ int failed;
   unsigned char* sm = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -125,7 +129,7 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tn(const __grid_constant__
   const int nk = K / kBK;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < TL::kStages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
@@ -150,8 +154,8 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tn(const __grid_constant__
     const uint32_t idesc = make_idesc(kBM, BN);
     auto stage_a = [&](int s) { return sm + (size_t)s * TL::kStageBytes; };
     auto stage_b = [&](int s) { return sm + (size_t)s * TL::kStageBytes + kTileBytesA; };
-    auto issue = [&](int kb) {  // block kb into stage kb % kStages
-      const int s = kb % kStages;
+    auto issue = [&](int kb) {  // block kb into stage kb % TL::kStages
+      const int s = kb % TL::kStages;
       mbar_expect_tx(&full[s], TL::kStageBytes);
 #pragma unroll
       for (int kc = 0; kc < kBK / 8; ++kc) {
@@ -161,10 +165,10 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tn(const __grid_constant__
     };
     int loaded = 0, consumed = 0;  // blocks whose copies were issued / whose bytes arrived
     bool ok = true;
-    for (; loaded < nk && loaded < kStages; ++loaded) issue(loaded);
+    for (; loaded < nk && loaded < TL::kStages; ++loaded) issue(loaded);
     for (int kb = 0; kb < nk && ok; ++kb) {
-      const int s = kb % kStages;
-      ok = mbar_wait(&full[s], (uint32_t)((kb / kStages) & 1));
+      const int s = kb % TL::kStages;
+      ok = mbar_wait(&full[s], (uint32_t)((kb / TL::kStages) & 1));
       if (!ok) break;
       consumed = kb + 1;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -185,8 +189,8 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tn(const __grid_constant__
                    : "memory");
       // refill the stage block kb - 1 used, once its MMAs are done (block kb's run meanwhile)
       if (kb >= 1 && loaded < nk) {
-        const int sp = (kb - 1) % kStages;
-        ok = mbar_wait(&empty[sp], (uint32_t)(((kb - 1) / kStages) & 1));
+        const int sp = (kb - 1) % TL::kStages;
+        ok = mbar_wait(&empty[sp], (uint32_t)(((kb - 1) / TL::kStages) & 1));
         if (!ok) break;
         issue(loaded++);
       }
@@ -194,7 +198,7 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tn(const __grid_constant__
     if (!ok) {
       failed = 1;
       // the copies still in flight land before the CTA's shared memory is given up
-      for (int kb = consumed; kb < loaded; ++kb) (void)mbar_wait(&full[kb % kStages], (uint32_t)((kb / kStages) & 1));
+      for (int kb = consumed; kb < loaded; ++kb) (void)mbar_wait(&full[kb % TL::kStages], (uint32_t)((kb / TL::kStages) & 1));
     }
     // arrives once every MMA this thread issued has completed
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(&fin))
@@ -206,6 +210,8 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tn(const __grid_constant__
   if (ok) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const int row = m0 + warp * 32 + (threadIdx.x & 31);
+    // 16-byte stores need every row start and the bias 16-byte aligned
+    const bool vec_ok = (ldc % 4) == 0 && ((uintptr_t)C & 15u) == 0 && ((uintptr_t)bias & 15u) == 0;
 #pragma unroll 1
     for (int c0 = 0; c0 < BN; c0 += 16) {
       uint32_t r[16];
@@ -217,10 +223,24 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tn(const __grid_constant__
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (row < M) {
+        float* crow = C + (size_t)row * ldc + n0 + c0;
+        if (vec_ok && n0 + c0 + 16 <= N) {  // four 16-byte stores
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int col = n0 + c0 + j;
-          if (col < N) C[(size_t)row * ldc + col] = __uint_as_float(r[j]) + (bias ? bias[col] : 0.0f);
+          for (int j = 0; j < 16; j += 4) {
+            float4 q = make_float4(__uint_as_float(r[j]), __uint_as_float(r[j + 1]), __uint_as_float(r[j + 2]),
+                                   __uint_as_float(r[j + 3]));
+            if (bias) {
+              const float4 bq = *reinterpret_cast<const float4*>(bias + n0 + c0 + j);
+              q.x = q.x + bq.x; q.y = q.y + bq.y; q.z = q.z + bq.z; q.w = q.w + bq.w;
+            }
+            *reinterpret_cast<float4*>(crow + j) = q;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int col = n0 + c0 + j;
+            if (col < N) crow[j] = __uint_as_float(r[j]) + (bias ? bias[col] : 0.0f);
+          }
         }
       }
     }

@@ -154,10 +154,10 @@ def test_hessian_diagonal_basis_directions_bit_exact(ctx, f64):
 @pytest.mark.parametrize("f64", [True, False])
 @pytest.mark.parametrize("mode", ["shared", "rademacher", "basis"])
 @pytest.mark.parametrize("S", [16, 15])
-def test_two_units_per_thread_share_the_point(ctx, f64, mode, S):
-    # two units per thread with S even: both are directions of one point, and
-    # the dense groups accumulate coefficient 0 once for the pair (S odd runs
-    # the per-unit form).  Results equal one unit per thread bit for bit.
+def test_two_units_per_thread_equal_one(ctx, f64, mode, S):
+    # point-direction launches at two units per thread (both directions of one
+    # point when S is even, of two points across a thread when S is odd) equal
+    # one unit per thread bit for bit, and the per-unit slot path
     torch = pytest.importorskip("torch")
     from echidna_b200.learned import hessian_diagonals
     n, m, B, seed = 40, 24, 150, 0x5EED

@@ -29,7 +29,8 @@ def _gemm(ctx, A, B, bias=None):
 
 
 @pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 256, 1024), (200, 384, 256), (64, 1024, 128),
-                                   (1024, 1280, 256), (1000, 1200, 192), (4096, 4096, 64), (4096, 4096, 1024)])
+                                   (1024, 1280, 256), (1000, 1200, 192), (4096, 4096, 64), (4096, 4096, 1024),
+                                   (2000, 4000, 128), (256, 1030, 64)])
 def test_gemm_bf16_matches_fp32_matmul(ctx, M, N, K):
     g = torch.Generator(device="cuda").manual_seed(M + N + K)
     A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
