@@ -247,6 +247,32 @@ class MlpWorkload:
                 "shape_gradient": self.ctx.launch_shape(self.gt, "gradient", self.batch),
                 "shape_hvp": self.ctx.launch_shape(self.gt, "hvp", self.batch)}
 
+    def accuracy(self, k=256):
+        """The timed launches' gradients and HVPs of the first k points against the
+        FP64 oracle (error = max |GPU - FP64| / max |FP64| per quantity), beside the
+        same-precision oracle's own error.  Run in the CPU-baseline leg, after timing."""
+        from oracle.oracle import OracleTape
+        n = self.n
+        g = self.d_g.view(self.batch, n)[:k].double().cpu().numpy()
+        g2 = self.d_g2.view(self.batch, n)[:k].double().cpu().numpy()
+        h = self.d_h.view(self.batch, n)[:k].double().cpu().numpy()
+        X, V = self.X[:k].astype(np.float64), self.V[:k].astype(np.float64)
+        o64 = OracleTape(self.tape, dtype=np.float64)
+        _, rg = o64.gradient(X)
+        rg2, rh = o64.hvp(X, V)
+
+        def err(a, ref):
+            return float(np.max(np.abs(a - ref)) / max(np.max(np.abs(ref)), 1e-300))
+        out = {"reference": "oracle (FP64 CPU tape) on the first %d points" % k,
+               "gradient_vs_fp64": err(g, rg), "hvp_gradient_vs_fp64": err(g2, rg2), "hvp_vs_fp64": err(h, rh)}
+        if not self.f64:
+            o32 = OracleTape(self.tape, dtype=np.float32)
+            _, sg = o32.gradient(X.astype(np.float32))
+            _, sh = o32.hvp(X.astype(np.float32), V.astype(np.float32))
+            out["fp32_oracle_gradient_vs_fp64"] = err(sg.astype(np.float64), rg)
+            out["fp32_oracle_hvp_vs_fp64"] = err(sh.astype(np.float64), rh)
+        return out
+
     def cpu_reference(self, budget_s, nthreads, dtype=np.float64):
         from oracle.oracle import OracleTape
         o = OracleTape(self.tape, dtype=dtype)
@@ -1042,6 +1068,8 @@ def main():
                                 "cpu_model": _cpu_model()}
         v1, sample1 = wl.cpu_reference(3.0, 1)
         line["cpu_baseline"]["single_thread"] = {"value": v1, "sample": sample1}
+        if hasattr(wl, "accuracy"):
+            line["detail"]["accuracy_256_points"] = wl.accuracy(256)
         if dtype == "f32" and "dtype" in wl.cpu_reference.__code__.co_varnames:
             # the same CPU path in FP32, so the FP32 GPU figure has a same-precision CPU number beside it
             v32, sample32 = wl.cpu_reference(5.0, nth, dtype=np.float32)

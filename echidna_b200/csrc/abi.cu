@@ -14,6 +14,7 @@
 #include <cmath>
 #include <memory>
 #include <atomic>
+#include <condition_variable>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -625,24 +626,90 @@ static bool host_pageable(const void* p) {
 }
 
 // memcpy on a few host threads for large copies (staging of pageable arrays).
-static void host_copy(void* dst, const void* src, size_t bytes) {
-  constexpr size_t kPart = 1u << 20;
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const size_t parts = std::min<size_t>(std::min<size_t>(hw, 8), (bytes + kPart - 1) / kPart);
-  if (parts <= 1) {
-    memcpy(dst, src, bytes);
-    return;
+// Host memcpy of staged chunks, split over a process-wide pool of copy threads
+// (started on first use and kept, so a copy costs no thread creation): the
+// caller copies parts too, and returns when every part is done.  One copy runs
+// at a time; calls from several threads queue on the pool's mutex.
+class CopyPool {
+ public:
+  static CopyPool& get() {
+    static CopyPool pool;
+    return pool;
   }
-  const size_t step = (bytes + parts - 1) / parts;
-  std::vector<std::thread> th;
-  for (size_t i = 1; i < parts; ++i) {
-    const size_t b = i * step;
-    if (b >= bytes) break;
-    th.emplace_back([=] { memcpy((char*)dst + b, (const char*)src + b, std::min(step, bytes - b)); });
+  void copy(void* dst, const void* src, size_t bytes) {
+    constexpr size_t kPart = 1u << 20;
+    const size_t parts = std::min<size_t>(workers_.size() + 1, (bytes + kPart - 1) / kPart);
+    if (parts <= 1) {
+      memcpy(dst, src, bytes);
+      return;
+    }
+    std::lock_guard<std::mutex> one(job_mu_);
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      dst_ = (char*)dst;
+      src_ = (const char*)src;
+      bytes_ = bytes;
+      step_ = (bytes + parts - 1) / parts;
+      parts_ = parts;
+      next_.store(0);
+      left_ = parts;
+      ++generation_;
+    }
+    cv_.notify_all();
+    work();
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [&] { return left_ == 0; });
   }
-  memcpy(dst, src, std::min(step, bytes));
-  for (std::thread& t : th) t.join();
-}
+
+ private:
+  CopyPool() {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned n = std::min(hw, 8u) - 1;
+    for (unsigned i = 0; i < n; ++i) workers_.emplace_back([this] { loop(); });
+  }
+  ~CopyPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (std::thread& t : workers_) t.join();
+  }
+  // copies parts until none is left
+  void work() {
+    for (;;) {
+      const size_t i = next_.fetch_add(1);
+      if (i >= parts_) return;
+      const size_t b = i * step_;
+      if (b < bytes_) memcpy(dst_ + b, src_ + b, std::min(step_, bytes_ - b));
+      std::lock_guard<std::mutex> lk(mu_);
+      if (--left_ == 0) done_cv_.notify_all();
+    }
+  }
+  void loop() {
+    uint64_t seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return stop_ || generation_ != seen; });
+        if (stop_) return;
+        seen = generation_;
+      }
+      work();
+    }
+  }
+  std::vector<std::thread> workers_;
+  std::mutex job_mu_, mu_;
+  std::condition_variable cv_, done_cv_;
+  char* dst_ = nullptr;
+  const char* src_ = nullptr;
+  size_t bytes_ = 0, step_ = 0, parts_ = 0, left_ = 0;
+  std::atomic<size_t> next_{0};
+  uint64_t generation_ = 0;
+  bool stop_ = false;
+};
+
+static void host_copy(void* dst, const void* src, size_t bytes) { CopyPool::get().copy(dst, src, bytes); }
 
 static ech_status run_pipelined(ech_ctx* ctx, ech_tape* t, int kind, uint64_t n_units, const SweepIO& io,
                                 const size_t io_unit_bytes[5], const std::vector<PipeArray>& arrays, bool* done) {

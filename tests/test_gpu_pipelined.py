@@ -1,8 +1,9 @@
 """Host-buffer sweeps of large batches run in chunks on several streams once
 their launch shape is tuned (copies of one chunk overlap the sweeps of the
 others).  The chunked calls must return exactly what the first, whole-batch
-call returned, for ragged batch sizes, and the f64 gradients must match the
-oracle."""
+call returned, for ragged batch sizes (the largest stages chunks of several
+MiB, which the host copies in parts on its copy threads), and the f64 gradients
+must match the oracle."""
 import numpy as np
 import pytest
 
@@ -18,7 +19,7 @@ def _bits(a):
     return a.view(np.uint32 if a.dtype == np.float32 else np.uint64)
 
 
-@pytest.mark.parametrize("B", [16384, 50001])
+@pytest.mark.parametrize("B", [16384, 50001, 200003])
 def test_chunked_gradient_and_hvp_equal_whole_batch(ctx, B):
     tape = configs.mlp(16, 16)
     rng = np.random.default_rng(B)
