@@ -662,10 +662,16 @@ class CopyPool {
   }
 
  private:
+  // min(hardware threads, 8) copiers in all (the caller and the workers), or
+  // ECHIDNA_B200_COPY_THREADS (1..64) when set
   CopyPool() {
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const unsigned n = std::min(hw, 8u) - 1;
-    for (unsigned i = 0; i < n; ++i) workers_.emplace_back([this] { loop(); });
+    unsigned n = std::min(hw, 8u);
+    if (const char* e = std::getenv("ECHIDNA_B200_COPY_THREADS")) {
+      const long v = std::strtol(e, nullptr, 10);
+      if (v >= 1 && v <= 64) n = (unsigned)v;
+    }
+    for (unsigned i = 1; i < n; ++i) workers_.emplace_back([this] { loop(); });
   }
   ~CopyPool() {
     {
