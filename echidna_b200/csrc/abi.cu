@@ -102,12 +102,14 @@ struct ech_ctx {
   bool autotune = true;        // pick launch shapes by timing (per tape, kind, batch size)
   std::mutex mu;
   DevBuf scratch, io_in, io_in2, io_out, io_out2, io_out3, stde_tmp;
-  // host-buffer sweeps of large batches run as chunks, one stream each
-  static constexpr int kPipe = 4;
-  cudaStream_t pipe[kPipe] = {};
+  // host-buffer sweeps of large batches run as pipe_chunks chunks, one stream
+  // each (4, or ECHIDNA_B200_PIPE_CHUNKS in 1..8, read at context creation)
+  static constexpr int kPipeMax = 8;
+  int pipe_chunks = 4;
+  cudaStream_t pipe[kPipeMax] = {};
   cudaEvent_t pipe_ev = nullptr;
-  DevBuf pipe_scratch[kPipe];
-  PinnedBuf pipe_stage[kPipe];   // staging for chunks of pageable host arrays
+  DevBuf pipe_scratch[kPipeMax];
+  PinnedBuf pipe_stage[kPipeMax];   // staging for chunks of pageable host arrays
   uint32_t* d_err = nullptr;
   // launch overrides (0 = automatic)
   uint32_t ov_threads = 0, ov_ppt = 0, ov_cap = 0;
@@ -163,6 +165,10 @@ extern "C" ECH_API ech_status ech_ctx_create(int device, ech_ctx** out) {
   c->smem_optin = prop.sharedMemPerBlockOptin;
   c->smem_per_sm = prop.sharedMemPerMultiprocessor;
   c->smem_reserved = prop.reservedSharedMemPerBlock;
+  if (const char* e = std::getenv("ECHIDNA_B200_PIPE_CHUNKS")) {
+    const long v = std::strtol(e, nullptr, 10);
+    if (v >= 1 && v <= ech_ctx::kPipeMax) c->pipe_chunks = (int)v;
+  }
   CU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   CU(cudaMalloc(&c->d_err, sizeof(uint32_t)));
   CU(cudaMemset(c->d_err, 0, sizeof(uint32_t)));
@@ -600,7 +606,7 @@ static ech_status enqueue(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n
 
 // ── host-buffer sweeps in chunks ──
 // A host-buffer call on a large batch whose launch shape is already tuned runs
-// as ech_ctx::kPipe chunks, each on its own stream: copy its inputs in, sweep,
+// as ctx->pipe_chunks chunks, each on its own stream: copy its inputs in, sweep,
 // copy its outputs out, so the copies of one chunk overlap the sweeps of the
 // others.  Every chunk uses the whole batch's tuned shape (the chunks' kernels
 // run side by side and together fill the GPU like one launch) and its own
@@ -662,11 +668,11 @@ class CopyPool {
   }
 
  private:
-  // min(hardware threads, 8) copiers in all (the caller and the workers), or
+  // min(hardware threads, 16) copiers in all (the caller and the workers), or
   // ECHIDNA_B200_COPY_THREADS (1..64) when set
   CopyPool() {
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    unsigned n = std::min(hw, 8u);
+    unsigned n = std::min(hw, 16u);
     if (const char* e = std::getenv("ECHIDNA_B200_COPY_THREADS")) {
       const long v = std::strtol(e, nullptr, 10);
       if (v >= 1 && v <= 64) n = (unsigned)v;
@@ -731,11 +737,11 @@ static ech_status run_pipelined(ech_ctx* ctx, ech_tape* t, int kind, uint64_t n_
   }
   const LaunchCfg c = cfg_for(ctx, t, kind, 0, sh);
   if (!ctx->pipe_ev) CU(cudaEventCreateWithFlags(&ctx->pipe_ev, cudaEventDisableTiming));
-  for (cudaStream_t& s : ctx->pipe)
-    if (!s) CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  const int nc = ctx->pipe_chunks;
+  for (int k = 0; k < nc; ++k)
+    if (!ctx->pipe[k]) CU(cudaStreamCreateWithFlags(&ctx->pipe[k], cudaStreamNonBlocking));
   // the chunks start after the context stream's earlier work
   CU(cudaEventRecord(ctx->pipe_ev, ctx->stream));
-  const int nc = ech_ctx::kPipe;
   uint64_t per = (n_units + nc - 1) / nc;
   per = (per + c.tile - 1) / c.tile * c.tile;
   // Pageable host arrays (what a caller's ordinary allocations are) go through
@@ -808,7 +814,7 @@ static ech_status run_pipelined(ech_ctx* ctx, ech_tape* t, int kind, uint64_t n_
   }
   // every chunk's copies finish before the host buffers are handed back;
   // staged outputs are copied out chunk by chunk as their streams finish
-  for (int k = 0; k < ech_ctx::kPipe; ++k) {
+  for (int k = 0; k < nc; ++k) {
     cudaError_t e = cudaStreamSynchronize(ctx->pipe[k]);
     if (e != cudaSuccess && first == ECH_OK) first = cuda_fail(e, "chunk sync");
     if (e != cudaSuccess || first != ECH_OK || k >= issued) continue;
