@@ -6,14 +6,15 @@
 // One CTA of 128 threads computes a 128 x BN tile of C (BN = 256 when such
 // tiles still give every SM one, else 128, or 64 when 128-wide tiles would
 // leave most SMs idle).  K advances in blocks of 64 through a shared-memory
-// ring of about 192 KiB (4 to 6 stages).  Thread 0 is the producer and the MMA
-// issuer: per block it issues eight 2-D TMA copies per operand, each a box of
-// 8 K-elements (16 B) x 128 (or BN) rows, which lands as the canonical K-major,
-// no-swizzle layout (8-row x 16-byte core matrices; 8-row groups 128 B apart,
-// K-adjacent core matrices one box apart), waits for the block's transaction
-// bytes on the stage's mbarrier, issues four tcgen05.mma (K = 16 each) and
-// commits them to the stage's "empty" mbarrier, after which the stage is
-// refilled.  Rows past M / N are zero-filled by the TMA unit.  The epilogue
+// ring of about 192 KiB (4 to 8 stages).  Thread 0 is the producer and the MMA
+// issuer: per block it issues one 2-D TMA copy per operand, a box of 64
+// K-elements (one 128-byte line per row) x 128 (or BN) rows with the 128-byte
+// swizzle, which lands as the canonical K-major SWIZZLE_128B layout (rows 128 B
+// apart, 8-row groups 1024 B apart, the 16-byte chunks of row r XOR-permuted by
+// r mod 8), waits for the block's transaction bytes on the stage's mbarrier,
+// issues four tcgen05.mma (K = 16 each: the descriptor's start advances 32 B
+// within the swizzle atom) and commits them to the stage's "empty" mbarrier,
+// after which the stage is refilled.  Rows past M / N are zero-filled by the TMA unit.  The epilogue
 // reads the accumulator with tcgen05.ld (warp w owns TMEM lanes / rows
 // 32w..32w+31).
 //
@@ -32,12 +33,10 @@ namespace umma {
 
 constexpr int kBM = 128, kBK = 64;
 constexpr int kThreads = 128;
-constexpr uint32_t kBoxBytesA = kBM * 16;                // one 8-element K slice of 128 rows
-constexpr uint32_t kTileBytesA = kBM * kBK * 2;          // 16 KiB per A block
+constexpr uint32_t kTileBytesA = kBM * kBK * 2;          // 16 KiB per A block (128 rows x 128 B)
 // Stages: as many as fit about 192 KiB, so that the copies in flight cover a
 // TMA round trip (6 stages of 32 KiB at BN = 128, 4 of 48 KiB at BN = 256).
 template <int BN> struct Tile {
-  static constexpr uint32_t kBoxBytesB = BN * 16;
   static constexpr uint32_t kTileBytesB = BN * kBK * 2;
   static constexpr uint32_t kStageBytes = kTileBytesA + kTileBytesB;
   static constexpr int kStages = (int)((192u * 1024u) / kStageBytes) > 8 ? 8 : (int)((192u * 1024u) / kStageBytes);
@@ -48,14 +47,19 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// Shared-memory matrix descriptor: K-major, no swizzle, version 1 (sm_100).
-__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+// Shared-memory matrix descriptor, version 1 (sm_100), K-major with the
+// 128-byte swizzle (layout type 2, bits 61-63): rows of one 128-byte line, the
+// stride byte offset (SBO) between 8-row groups is 1024 B, the leading byte
+// offset is unused for this layout (16 B).  The tile base is 1024-B aligned
+// (base offset 0); the start may advance within a line to pick a K slice.
+__device__ __forceinline__ uint64_t make_desc_sw128(uint32_t saddr) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-  d |= (uint64_t)1 << 46;  // descriptor version
-  return d;               // base offset 0, relative LBO, layout SWIZZLE_NONE
+  d |= (uint64_t)(16u >> 4) << 16;     // LBO
+  d |= (uint64_t)(1024u >> 4) << 32;   // SBO
+  d |= (uint64_t)1 << 46;              // descriptor version
+  d |= (uint64_t)2 << 61;              // SWIZZLE_128B
+  return d;
 }
 
 // Instruction descriptor, kind::f16: D fp32, A and B bf16, both K-major.
@@ -99,8 +103,8 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 }
 
 // One 2-D TMA copy (no multicast): the box at (x = K element, y = row) of the
-// tensor map into shared memory, completing `bytes` on `bar`.  x is a multiple
-// of 8 elements (16 bytes), as TMA requires.
+// tensor map into shared memory, completing its bytes on `bar`.  x is a
+// multiple of 64 elements (128 bytes; TMA requires 16).
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
@@ -110,8 +114,8 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 }
 
 // M rows of A / C, N rows of B / columns of C, K a multiple of 64; the tensor
-// maps describe A [M][K] and B [N][K] (bf16, inner dimension K, boxes 8 x 128
-// and 8 x BN, no swizzle); C row stride ldc (floats).
+// maps describe A [M][K] and B [N][K] (bf16, inner dimension K, boxes 64 x 128
+// and 64 x BN, 128-byte swizzle); C row stride ldc (floats).
 template <int BN>
 __global__ void __launch_bounds__(kThreads) gemm_bf16_tn(const __grid_constant__ CUtensorMap tma_a,
                                                         const __grid_constant__ CUtensorMap tma_b,
@@ -157,11 +161,8 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tn(const __grid_constant__
     auto issue = [&](int kb) {  // block kb into stage kb % TL::kStages
       const int s = kb % TL::kStages;
       mbar_expect_tx(&full[s], TL::kStageBytes);
-#pragma unroll
-      for (int kc = 0; kc < kBK / 8; ++kc) {
-        tma_load_2d(stage_a(s) + kc * kBoxBytesA, &tma_a, kb * kBK + kc * 8, m0, &full[s]);
-        tma_load_2d(stage_b(s) + kc * TL::kBoxBytesB, &tma_b, kb * kBK + kc * 8, n0, &full[s]);
-      }
+      tma_load_2d(stage_a(s), &tma_a, kb * kBK, m0, &full[s]);
+      tma_load_2d(stage_b(s), &tma_b, kb * kBK, n0, &full[s]);
     };
     int loaded = 0, consumed = 0;  // blocks whose copies were issued / whose bytes arrived
     bool ok = true;
@@ -174,9 +175,9 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tn(const __grid_constant__
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
       for (int ks = 0; ks < kBK / 16; ++ks) {
-        // K = 16 spans two K-adjacent core matrices: two boxes
-        const uint64_t da = make_desc(smem_addr(stage_a(s)) + ks * 2u * kBoxBytesA, kBoxBytesA, 128u);
-        const uint64_t db = make_desc(smem_addr(stage_b(s)) + ks * 2u * TL::kBoxBytesB, TL::kBoxBytesB, 128u);
+        // K slice ks: 16 elements = 32 B into every row's line
+        const uint64_t da = make_desc_sw128(smem_addr(stage_a(s)) + ks * 32u);
+        const uint64_t db = make_desc_sw128(smem_addr(stage_b(s)) + ks * 32u);
         const uint32_t acc = (kb > 0 || ks > 0) ? 1u : 0u;
         asm volatile(
             "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
