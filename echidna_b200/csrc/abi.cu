@@ -560,17 +560,21 @@ static ech_status tune(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_t n_un
     }
   }
   if (best_ms >= 0.0f) {
-    // the best shape on the other kernel build: two timings of each, interleaved
+    // the best shape on the other kernel build: three timings of each, interleaved; the
+    // dense-group build (more registers, more instructions per record for programs
+    // without dense groups) must win by 2 % to be kept
     Shape alt = *best;
     alt.dense_kernel = 1;
     float a_ms = time_shape(alt, true);
     if (a_ms >= 0.0f) {
-      const float b2 = time_shape(*best, false);
-      const float a2 = time_shape(alt, false);
       float b_ms = best_ms;
-      if (b2 >= 0.0f) b_ms = std::min(b_ms, b2);
-      if (a2 >= 0.0f) a_ms = std::min(a_ms, a2);
-      if (a_ms < b_ms) *best = alt;
+      for (int r = 0; r < 2; ++r) {
+        const float b2 = time_shape(*best, false);
+        const float a2 = time_shape(alt, false);
+        if (b2 >= 0.0f) b_ms = std::min(b_ms, b2);
+        if (a2 >= 0.0f) a_ms = std::min(a_ms, a2);
+      }
+      if (a_ms < 0.98f * b_ms) *best = alt;
     }
   }
   cudaEventDestroy(e0);
