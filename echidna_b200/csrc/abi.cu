@@ -111,6 +111,9 @@ struct ech_ctx {
   DevBuf pipe_scratch[kPipeMax];
   PinnedBuf pipe_stage[kPipeMax];   // staging for chunks of pageable host arrays
   uint32_t* d_err = nullptr;
+  // resident CTAs per SM of a sweep kernel: (value kind, f64, order, points per
+  // thread, reverse, dense build, threads, dynamic shared memory) -> blocks
+  std::map<std::tuple<int, int, int, int, int, int, int, size_t>, int> occupancy;
   // launch overrides (0 = automatic)
   uint32_t ov_threads = 0, ov_ppt = 0, ov_cap = 0;
   uint32_t ov_dense = 0;  // 1: the dense-group kernel build for every program (ech_ctx_set_dense_kernel)
@@ -484,9 +487,19 @@ static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_
   kp.seed_items = io.seed_items;
   kp.dir_bits = dir_bits;
   kp.compensated = (uint32_t)io.compensated;
+  // occupancy per kernel and launch shape, queried once per context (callers hold ctx->mu)
+  const auto okey = std::make_tuple((int)c.req.vk, (int)c.req.f64, c.req.K, c.req.P, (int)c.req.rev,
+                                    (int)c.req.dense, (int)c.threads, c.smem);
   int bps = 0;
-  cudaError_t e = launch_sweep(c.req, kp, 0, c.threads, c.smem, st, &bps);
-  if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+  cudaError_t e = cudaSuccess;
+  auto oit = ctx->occupancy.find(okey);
+  if (oit != ctx->occupancy.end()) {
+    bps = oit->second;
+  } else {
+    e = launch_sweep(c.req, kp, 0, c.threads, c.smem, st, &bps);
+    if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+    ctx->occupancy[okey] = bps;
+  }
   if (bps <= 0) return fail(ECH_ERR_OTHER, "tape live set does not fit the shared-memory slot file");
   const uint64_t ntiles = (n_units + c.tile - 1) / c.tile;
   const uint64_t grid = std::min<uint64_t>(ntiles, (uint64_t)bps * ctx->sm_count);

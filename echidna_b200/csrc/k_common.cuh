@@ -5,6 +5,8 @@
 // builds of a unit compile in parallel.  A unit compiled without ECH_DN
 // instantiates both.
 #pragma once
+#include <atomic>
+
 #include "interp.cuh"
 #include "launch.h"
 
@@ -21,11 +23,27 @@
 
 namespace ech {
 
+// The kernel's dynamic shared-memory limit is raised once per device to the
+// largest size asked so far; launches that need no more skip the attribute call
+// (a host round trip that would otherwise precede every launch).
 template <class V, int P, bool REV, bool DN>
 cudaError_t launch_one(const KParams& kp, int grid, int block, size_t smem, cudaStream_t st, int* blocks_per_sm) {
+  constexpr int kDevices = 64;
+  static std::atomic<int> smem_set[kDevices];  // static storage: zero-initialised
   auto fn = sweep_kernel<V, P, REV, DN>;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
+  const bool known = dev >= 0 && dev < kDevices;
+  if (!known || (int)smem > smem_set[dev].load(std::memory_order_acquire)) {
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (known) {
+      int cur = smem_set[dev].load(std::memory_order_relaxed);
+      while ((int)smem > cur && !smem_set[dev].compare_exchange_weak(cur, (int)smem)) {
+      }
+    }
+  }
   if (grid == 0) {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, block, smem);
   }
