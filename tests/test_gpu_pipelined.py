@@ -46,3 +46,42 @@ def test_chunked_f64_gradient_matches_oracle(ctx):
     ov, og = OracleTape(tape).gradient(X)
     assert (_bits(v) == _bits(ov[:, 0])).all()
     assert (_bits(g.reshape(B, 12)) == _bits(og)).all()
+
+
+def test_chunked_calls_from_two_threads(ctx):
+    # two contexts on one device, each called from its own thread with pageable
+    # arrays big enough that both stage their chunks through the shared pool of
+    # copy threads at once: every call returns what a call on its own returns
+    import threading
+
+    from echidna_b200.gpu import CudaContext
+    tape = configs.mlp(16, 16)
+    B = 200003
+    rng = np.random.default_rng(7)
+    X = [rng.normal(size=(B, 16)).astype(np.float32) for _ in range(2)]
+    ctxs = [ctx, CudaContext.new(0)]
+    tapes = [c.upload_tape(GpuTapeData.from_tape_f64_lossy(tape)) for c in ctxs]
+    want = []
+    for c, t, x in zip(ctxs, tapes, X):
+        c.gradient_batch(t, x, B)                  # tunes the shape (whole batch)
+        want.append(c.gradient_batch(t, x, B))     # chunked, alone
+    got = [None, None]
+    errors = []
+
+    def run(i):
+        try:
+            for _ in range(3):
+                got[i] = ctxs[i].gradient_batch(tapes[i], X[i], B)
+        except Exception as e:  # reported below
+            errors.append(e)
+    threads = [threading.Thread(target=run, args=(i,)) for i in range(2)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    assert not errors, errors
+    for i in range(2):
+        for a, b in zip(got[i], want[i]):
+            assert (_bits(a) == _bits(b)).all()
+    tapes.clear()
+    ctxs[1].close()
