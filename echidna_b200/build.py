@@ -39,7 +39,7 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC
            "--expt-relaxed-constexpr", "-I", CSRC, "-I", os.path.join(ROOT, "include")]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-ffp-contract=off", "-I", CSRC]
 
-CU_SOURCES = ["abi.cu", "launch.cu", "stde.cu", "noalloc.cu", "mlp.cu"]
+CU_SOURCES = ["k_jet3ws.cu", "abi.cu", "launch.cu", "stde.cu", "noalloc.cu", "mlp.cu"]
 # Sweep-kernel units, compiled twice: without (ECH_DN=0) and with (ECH_DN=1)
 # the dense-group executor.  Listed longest compile first.
 DN_SOURCES = ["k_jet3.cu", "k_jet2.cu", "k_dual.cu", "k_jet4.cu", "k_jet5.cu", "k_plain.cu", "k_multi.cu",

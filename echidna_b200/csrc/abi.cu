@@ -112,7 +112,8 @@ struct ech_ctx {
   PinnedBuf pipe_stage[kPipeMax];   // staging for chunks of pageable host arrays
   uint32_t* d_err = nullptr;
   // resident CTAs per SM of a sweep kernel: (value kind, f64, order, points per
-  // thread, reverse, dense build, threads, dynamic shared memory) -> blocks
+  // thread, reverse, dense build | warp-shared point << 1, threads, dynamic
+  // shared memory) -> blocks
   std::map<std::tuple<int, int, int, int, int, int, int, size_t>, int> occupancy;
   // launch overrides (0 = automatic)
   uint32_t ov_threads = 0, ov_ppt = 0, ov_cap = 0;
@@ -449,6 +450,9 @@ static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_
   if (s != ECH_OK) return s;
   const Plan& p = dp->host;
   c.req.dense = dp->needs_dense() || c.dense_kernel;
+  // every warp's 32 units are directions of one point: units u = point * S + s,
+  // one per thread, warps start at multiples of 32
+  c.req.warp_point = direct && K == 3 && c.req.P == 1 && io.S % 32u == 0;
   const uint32_t regs = std::max<uint32_t>(p.smem_regs, 1);
   c.smem = kRingBytes + (size_t)regs * c.tile * c.vbytes;
   const uint32_t dir_bits = bits_bytes ? (uint32_t)c.smem : 0u;
@@ -489,7 +493,7 @@ static ech_status launch_cfg(ech_ctx* ctx, ech_tape* t, int kind, int K, uint64_
   kp.compensated = (uint32_t)io.compensated;
   // occupancy per kernel and launch shape, queried once per context (callers hold ctx->mu)
   const auto okey = std::make_tuple((int)c.req.vk, (int)c.req.f64, c.req.K, c.req.P, (int)c.req.rev,
-                                    (int)c.req.dense, (int)c.threads, c.smem);
+                                    (int)c.req.dense | ((int)c.req.warp_point << 1), (int)c.threads, c.smem);
   int bps = 0;
   cudaError_t e = cudaSuccess;
   auto oit = ctx->occupancy.find(okey);

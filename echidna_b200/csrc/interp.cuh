@@ -488,7 +488,13 @@ template <class T> struct GradOut<dm::Dual<T>> {
 // raise the kernel's register demand for every program, so programs without
 // dense groups run an instantiation without them (DN = false), where D_DENSE is
 // an invalid instruction.
-template <class V, int P, bool DN = true> struct FwdExec {
+// WS (warp-shared point): every warp's 32 units are directions of one point
+// (point-direction launches, one unit per thread, S a multiple of 32), so
+// coefficient 0 of every jet is the same in all lanes; the dense executor then
+// accumulates coefficient 0 of output r in lane r (mod the group size) only and
+// broadcasts the results with shuffles, instead of every lane accumulating it
+// for every output.
+template <class V, int P, bool DN = true, bool WS = false> struct FwdExec {
   using Kd = typename dm::KindOf<V>::K;
   using C = Col<V, P>;
   const KParams& kp;
@@ -1012,6 +1018,16 @@ template <class V, int P, bool DN = true> struct FwdExec {
 #pragma unroll
           for (int k = 0; k < KJ; ++k) acc[j][p].c[k] = acc[j][p].c[k] + T(0);
     }
+    // warp-shared point: this lane accumulates coefficient 0 of output `myrow`
+    // (every lane holds the same starting values, so a select picks it)
+    constexpr bool kWS = WS && JetOrder<V>::K > 1 && P == 1;
+    const int myrow = kWS ? (int)((threadIdx.x & 31u) % (uint32_t)MX) : 0;
+    T c0m = T(0);
+    if constexpr (kWS) {
+#pragma unroll
+      for (int j = 0; j < MX; ++j)
+        if (j == myrow) c0m = acc[j][0].c[0];
+    }
 #pragma unroll 1
     for (uint32_t q0 = 0; q0 < n; q0 += 4) {
       const unsigned char* orec = st.next();
@@ -1031,6 +1047,7 @@ template <class V, int P, bool DN = true> struct FwdExec {
 #pragma unroll
           for (int p = 0; p < P; ++p) dz[p] = fma_zero(x[p].re, dz[p]);
         }
+        T mycs = T(0);  // warp-shared point: this lane's output's constant of the term
 #pragma unroll
         for (int jj = 0; jj < MX; jj += PER) {
           if (FULL || (uint32_t)jj < m) {
@@ -1039,6 +1056,11 @@ template <class V, int P, bool DN = true> struct FwdExec {
             T cs[PER];
 #pragma unroll
             for (int j = 0; j < PER; ++j) cs[j] = reinterpret_cast<const T*>(crec)[j];
+            if constexpr (kWS) {
+              // read before the next pull, which may recycle the record's stage
+              const T mine = reinterpret_cast<const T*>(crec)[myrow % PER];
+              if (myrow / PER == jj / PER) mycs = mine;
+            }
             // an input jet (x_i, v_i, 0, ..) read at its source changes
             // coefficients 0 and 1 only (its zero products add nothing)
             if constexpr (JetOrder<V>::K > 0) {
@@ -1049,7 +1071,7 @@ template <class V, int P, bool DN = true> struct FwdExec {
 #pragma unroll
                     for (int p = 0; p < P; ++p) {
                       V& a = acc[jj + j < MX ? jj + j : 0][p];
-                      a.c[0] = a.c[0] + cs[j] * x[p].c[0];
+                      if constexpr (!kWS) a.c[0] = a.c[0] + cs[j] * x[p].c[0];
                       if constexpr (KJ > 1) {
                         if constexpr (UNITV) a.c[1] = fma_rn(cs[j], x[p].c[1], a.c[1]);
                         else a.c[1] = a.c[1] + cs[j] * x[p].c[1];
@@ -1069,7 +1091,7 @@ template <class V, int P, bool DN = true> struct FwdExec {
                   V& a = acc[jj + j < MX ? jj + j : 0][p];
                   if constexpr (JetOrder<V>::K > 0) {
 #pragma unroll
-                    for (int k = 0; k < KJ; ++k) a.c[k] = a.c[k] + c * x[p].c[k];
+                    for (int k = kWS ? 1 : 0; k < KJ; ++k) a.c[k] = a.c[k] + c * x[p].c[k];
                   } else if constexpr (IsDual<V>::v) {
                     a.re = a.re + c * x[p].re;
                     a.eps = a.eps + c * x[p].eps;
@@ -1081,6 +1103,7 @@ template <class V, int P, bool DN = true> struct FwdExec {
             }
           }
         }
+        if constexpr (kWS) c0m = c0m + mycs * x[0].c[0];
         if constexpr (JetOrder<V>::K > 1) {
 #pragma unroll
           for (int p = 0; p < P; ++p) {
@@ -1094,6 +1117,10 @@ template <class V, int P, bool DN = true> struct FwdExec {
           }
         }
       }
+    }
+    if constexpr (kWS) {
+#pragma unroll
+      for (int j = 0; j < MX; ++j) acc[j][0].c[0] = __shfl_sync(0xffffffffu, c0m, j);
     }
 #pragma unroll
     for (int jj = 0; jj < MX; jj += 2) {
@@ -1717,7 +1744,7 @@ template <class V, int P, bool DN = true> struct RevExec {
 // One tile of `kp.tile` units: the forward program (with trajectory saves when
 // REV), then the reverse program.  `gbase` is the CTA's global scratch region.
 // Returns false when a bounded wait gave up (every thread sees the same value).
-template <class V, int P, bool REV, bool DN>
+template <class V, int P, bool REV, bool DN, bool WS = false>
 __device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned char* sm, unsigned char* gbase,
                                            uint64_t t) {
   const uint32_t tile = kp.tile;
@@ -1727,7 +1754,7 @@ __device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned
                                    : gbase + (size_t)kp.far_slots * tile * sizeof(V) + colb;
   const uint64_t unit0 = t * tile + (uint64_t)threadIdx.x * P;
   uint32_t* bits = kp.dir_bits ? reinterpret_cast<uint32_t*>(rg.buf + kp.dir_bits) + threadIdx.x * P : nullptr;
-  FwdExec<V, P, DN> fx{kp, sm, gs, tj, unit0, bits, {}, {}, {}, {}, {}};
+  FwdExec<V, P, DN, WS> fx{kp, sm, gs, tj, unit0, bits, {}, {}, {}, {}, {}};
 #pragma unroll
   for (int p = 0; p < P; ++p) {
     fx.valid[p] = unit0 + p < kp.n_units;
@@ -1776,7 +1803,8 @@ __device__ __forceinline__ bool sweep_tile(const KParams& kp, Ring& rg, unsigned
 // REV = true : forward program with trajectory saves, then the reverse program
 //              (gradient for plain values, HVP for Dual values).
 // DN: with the dense-group executor (programs that hold D_DENSE instructions).
-template <class V, int P, bool REV, bool DN>
+// WS: every warp's units are directions of one point (FwdExec).
+template <class V, int P, bool REV, bool DN, bool WS = false>
 __global__ void __launch_bounds__(256) sweep_kernel(KParams kp) {
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   __shared__ __align__(8) uint64_t full[kStages];
@@ -1790,7 +1818,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(KParams kp) {
   unsigned char* gbase = reinterpret_cast<unsigned char*>(kp.scratch) + blockIdx.x * kp.scratch_stride_bytes;
   const uint64_t ntiles = (kp.n_units + kp.tile - 1) / kp.tile;
   for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x)
-    if (!sweep_tile<V, P, REV, DN>(kp, rg, sm, gbase, t)) return;
+    if (!sweep_tile<V, P, REV, DN, WS>(kp, rg, sm, gbase, t)) return;
 }
 
 // ───────────────────────────── many tapes, one launch ───────────────────────

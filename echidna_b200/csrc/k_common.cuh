@@ -26,11 +26,11 @@ namespace ech {
 // The kernel's dynamic shared-memory limit is raised once per device to the
 // largest size asked so far; launches that need no more skip the attribute call
 // (a host round trip that would otherwise precede every launch).
-template <class V, int P, bool REV, bool DN>
+template <class V, int P, bool REV, bool DN, bool WS = false>
 cudaError_t launch_one(const KParams& kp, int grid, int block, size_t smem, cudaStream_t st, int* blocks_per_sm) {
   constexpr int kDevices = 64;
   static std::atomic<int> smem_set[kDevices];  // static storage: zero-initialised
-  auto fn = sweep_kernel<V, P, REV, DN>;
+  auto fn = sweep_kernel<V, P, REV, DN, WS>;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;

@@ -35,6 +35,8 @@ static cudaError_t launch_jet_dn(const LaunchReq& r, const KParams& kp, int grid
 
 cudaError_t launch_jet(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
                        int* bps) {
+  if (r.warp_point && r.dense && r.K == 3 && !r.rev && r.P == 1)
+    return launch_jet3_warp_point(r, kp, grid, block, smem, st, bps);
   return r.dense ? launch_jet_dn<true>(r, kp, grid, block, smem, st, bps)
                  : launch_jet_dn<false>(r, kp, grid, block, smem, st, bps);
 }

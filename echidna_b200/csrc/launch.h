@@ -18,6 +18,7 @@ struct LaunchReq {
   int P = 1;      // points per thread
   bool rev = false;
   bool dense = false;  // the program holds dense groups: the kernel with the dense-group executor
+  bool warp_point = false;  // order-3 jets, one unit per thread: each warp's units share a point
 };
 
 size_t value_bytes(const LaunchReq& r);
@@ -31,6 +32,11 @@ cudaError_t launch_dual(const LaunchReq& r, const KParams& kp, int grid, int blo
                         int* blocks_per_sm);
 cudaError_t launch_jet(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,
                        int* blocks_per_sm);
+// Order-3 jets with dense groups, one unit per thread, every warp's units
+// directions of one point (r.warp_point): coefficient 0 of a dense group's
+// outputs is accumulated one output per lane and broadcast.
+cudaError_t launch_jet3_warp_point(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem,
+                                   cudaStream_t st, int* blocks_per_sm);
 
 // Launch (grid > 0) or query occupancy (grid == 0, result in *blocks_per_sm).
 cudaError_t launch_sweep(const LaunchReq& r, const KParams& kp, int grid, int block, size_t smem, cudaStream_t st,

@@ -193,3 +193,49 @@ def test_two_units_per_thread_equal_one(ctx, f64, mode, S):
         c, nc = _stats(laplacian_batch(ctx, gt, X, S, np.ascontiguousarray(np.broadcast_to(D, (B, S, n))),
                                        DIR_PER_POINT))
         assert _bits_equal(a, c)
+
+
+@pytest.mark.parametrize("f64", [True, False])
+@pytest.mark.parametrize("mode", ["shared", "rademacher", "basis"])
+def test_warps_of_one_point_share_coefficient_zero(ctx, f64, mode):
+    # S a multiple of 32 at one unit per thread: every warp's units are directions
+    # of one point, and the dense groups accumulate coefficient 0 one output per
+    # lane, broadcast by shuffles.  Results equal the per-unit slot path (no
+    # input-direct terms) or the oracle bit for bit, with inf and NaN inputs.
+    torch = pytest.importorskip("torch")
+    from echidna_b200.learned import hessian_diagonals
+    n = 64 if mode == "basis" else 40
+    m, B, S, seed = 40, 70, 64, 0x5EED77
+    tape = _layer_tape(n, m, 13, True)
+    dt = np.float64 if f64 else np.float32
+    rng = np.random.default_rng(14)
+    X = rng.normal(size=(B, n)).astype(dt)
+    X[3, 4] = np.inf
+    X[7, 0] = np.nan
+    gt = ctx.upload_tape_f64(tape) if f64 else ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(tape))
+    ctx.set_launch(128, 1, 0)
+    try:
+        if mode == "basis":
+            d = hessian_diagonals(ctx, gt, torch.tensor(X, device="cuda")).cpu().numpy()
+            o = OracleTape(tape, dtype=dt)
+            E = np.eye(n, dtype=dt)
+            for b in (0, 3, 7, 40, 69):
+                c = o.taylor(np.tile(X[b], (n, 1)), E, 3)
+                assert _bits_equal(d[b], (dt(2) * c[2]).astype(dt)), b
+            return
+        if mode == "shared":
+            D = rng.normal(size=(S, n)).astype(dt)
+            a, na = _stats(laplacian_batch(ctx, gt, X, S, D, DIR_SHARED))
+            per_unit = np.ascontiguousarray(np.broadcast_to(D, (B, S, n)))
+        else:
+            a, na = _stats(laplacian_batch(ctx, gt, X, S, None, DIR_RADEMACHER, seed=seed))
+            p = np.arange(B, dtype=np.uint64)[:, None, None]
+            s = np.arange(S, dtype=np.uint64)[None, :, None]
+            i = np.arange(n, dtype=np.uint64)[None, None, :]
+            per_unit = np.ascontiguousarray(np.where(philox_bits(seed, p, s, i) & 1, 1.0, -1.0).astype(dt))
+        b, nb = _stats(laplacian_batch(ctx, gt, X, S, per_unit, DIR_PER_POINT))
+        assert _bits_equal(a, b)
+        assert np.array_equal(na, nb)
+    finally:
+        ctx.set_launch(0, 0, 0)
+        ctx.set_autotune(True)
