@@ -8,7 +8,8 @@ tape uploaded with ``from_tape_f64_lossy`` and evaluated in f32, with the
 reference's own tolerances.  The second group restates CPU tests of the same
 conventions on the bytecode tape in f64 (``tests/atan2_extreme_magnitudes.rs``,
 ``tests/asinh_acosh_large.rs``, ``tests/taylor.rs``,
-``tests/hypot_leading_zero_parity.rs``); Dual-number cases become JVPs of the
+``tests/hypot_leading_zero_parity.rs``, ``tests/opcode_edge_cases.rs`` as one-op
+tapes, ``tests/stde_nonfinite_samples.rs``); Dual-number cases become JVPs of the
 one-op tape (a ``Dual::new(x, 1)`` operand is a seeded input, a
 ``Dual::constant`` operand a tape constant).  The oracle runs every case in the
 precision the case names (its f32 mode rounds the tape constants to f32, as
@@ -139,6 +140,96 @@ CASES = {
                     ((1.0,), 4), lambda r: list(r["jet"]) == [8.0, 12.0, 6.0, 1.0]),
 }
 
+# opcode_edge_cases.rs (TOL = 1e-10): eval_forward and reverse_partials of one op,
+# as the forward value and the gradient of a one-op tape in f64
+_T = 1e-10
+_ok = lambda got, want: abs(got - want) < _T  # noqa: E731
+_UN = lambda f: (lambda v: f(v[0]))  # noqa: E731
+_BI = lambda f: (lambda v: f(v[0], v[1]))  # noqa: E731
+OPCODE_EDGE = {
+    "add_nan": ("opcode_edge_cases.rs:16-19", _BI(lambda a, b: a + b), (NAN, 1.0), "forward", lambda r: math.isnan(r)),
+    "mul_nan": ("opcode_edge_cases.rs:22-25", _BI(lambda a, b: a * b), (1.0, NAN), "forward", lambda r: math.isnan(r)),
+    "div_nan": ("opcode_edge_cases.rs:37-41", _BI(lambda a, b: a / b), (NAN, 1.0), "forward", lambda r: math.isnan(r)),
+    "neg_nan": ("opcode_edge_cases.rs:28-34", _UN(lambda a: -a), (NAN,), "forward", lambda r: math.isnan(r)),
+    "exp_nan": ("opcode_edge_cases.rs:28-34", _UN(lambda a: a.exp()), (NAN,), "forward", lambda r: math.isnan(r)),
+    "sin_nan": ("opcode_edge_cases.rs:28-34", _UN(lambda a: a.sin()), (NAN,), "forward", lambda r: math.isnan(r)),
+    "sqrt_nan": ("opcode_edge_cases.rs:28-34", _UN(lambda a: a.sqrt()), (NAN,), "forward", lambda r: math.isnan(r)),
+    "abs_nan": ("opcode_edge_cases.rs:28-34", _UN(lambda a: a.abs()), (NAN,), "forward", lambda r: math.isnan(r)),
+    "exp_large": ("opcode_edge_cases.rs:47-49", _UN(lambda a: a.exp()), (1000.0,), "forward", lambda r: math.isinf(r)),
+    "ln_zero": ("opcode_edge_cases.rs:52-55", _UN(lambda a: a.ln()), (0.0,), "forward", lambda r: r == -INF),
+    "div_zero": ("opcode_edge_cases.rs:58-61", _BI(lambda a, b: a / b), (1.0, 0.0), "forward", lambda r: math.isinf(r)),
+    "recip_zero": ("opcode_edge_cases.rs:64-67", _UN(lambda a: a.recip()), (0.0,), "forward", lambda r: math.isinf(r)),
+    "sqrt_negative": ("opcode_edge_cases.rs:70-72", _UN(lambda a: a.sqrt()), (-1.0,), "forward",
+                      lambda r: math.isnan(r)),
+    "ln_negative": ("opcode_edge_cases.rs:75-77", _UN(lambda a: a.ln()), (-1.0,), "forward", lambda r: math.isnan(r)),
+    "max_35": ("opcode_edge_cases.rs:84-89", _BI(lambda a, b: a.max(b)), (3.0, 5.0), "forward", lambda r: r == 5.0),
+    "max_53": ("opcode_edge_cases.rs:84-89", _BI(lambda a, b: a.max(b)), (5.0, 3.0), "forward", lambda r: r == 5.0),
+    "min_35": ("opcode_edge_cases.rs:84-89", _BI(lambda a, b: a.min(b)), (3.0, 5.0), "forward", lambda r: r == 3.0),
+    "min_53": ("opcode_edge_cases.rs:84-89", _BI(lambda a, b: a.min(b)), (5.0, 3.0), "forward", lambda r: r == 3.0),
+    "max_equal": ("opcode_edge_cases.rs:92-95", _BI(lambda a, b: a.max(b)), (4.0, 4.0), "forward", lambda r: r == 4.0),
+    "min_equal": ("opcode_edge_cases.rs:92-95", _BI(lambda a, b: a.min(b)), (4.0, 4.0), "forward", lambda r: r == 4.0),
+    "abs_zero": ("opcode_edge_cases.rs:98-101", _UN(lambda a: a.abs()), (0.0,), "forward", lambda r: r == 0.0),
+    "abs_neg_zero": ("opcode_edge_cases.rs:98-101", _UN(lambda a: a.abs()), (-0.0,), "forward", lambda r: r == 0.0),
+    "abs_neg": ("opcode_edge_cases.rs:104-107", _UN(lambda a: a.abs()), (-3.5,), "forward", lambda r: r == 3.5),
+    "powi_0": ("opcode_edge_cases.rs:114-117", _UN(lambda a: a.powi(0)), (5.0,), "forward", lambda r: _ok(r, 1.0)),
+    "powi_3": ("opcode_edge_cases.rs:120-123", _UN(lambda a: a.powi(3)), (2.0,), "forward", lambda r: _ok(r, 8.0)),
+    "powi_-2": ("opcode_edge_cases.rs:126-129", _UN(lambda a: a.powi(-2)), (2.0,), "forward",
+                lambda r: _ok(r, 0.25)),
+    "floor": ("opcode_edge_cases.rs:147-153", _UN(lambda a: a.floor()), (2.7,), "forward", lambda r: r == 2.0),
+    "ceil": ("opcode_edge_cases.rs:147-153", _UN(lambda a: a.ceil()), (2.3,), "forward", lambda r: r == 3.0),
+    "round_half": ("opcode_edge_cases.rs:147-153", _UN(lambda a: a.round()), (2.5,), "forward", lambda r: r == 3.0),
+    "trunc": ("opcode_edge_cases.rs:147-153", _UN(lambda a: a.trunc()), (-2.7,), "forward", lambda r: r == -2.0),
+    "fract": ("opcode_edge_cases.rs:147-153", _UN(lambda a: a.fract()), (2.7,), "forward", lambda r: _ok(r, 0.7)),
+    # reverse_partials -> gradient of the one-op tape
+    "d_add": ("opcode_edge_cases.rs:160-165", _BI(lambda a, b: a + b), (2.0, 3.0), "gradient", (1.0, 1.0)),
+    "d_sub": ("opcode_edge_cases.rs:167-172", _BI(lambda a, b: a - b), (5.0, 3.0), "gradient", (1.0, -1.0)),
+    "d_mul": ("opcode_edge_cases.rs:174-179", _BI(lambda a, b: a * b), (3.0, 4.0), "gradient", (4.0, 3.0)),
+    "d_div": ("opcode_edge_cases.rs:181-186", _BI(lambda a, b: a / b), (6.0, 3.0), "gradient", (1 / 3, -6 / 9)),
+    "d_exp": ("opcode_edge_cases.rs:188-194", _UN(lambda a: a.exp()), (1.5,), "gradient", (math.exp(1.5),)),
+    "d_ln": ("opcode_edge_cases.rs:196-202", _UN(lambda a: a.ln()), (2.0,), "gradient", (0.5,)),
+    "d_sin": ("opcode_edge_cases.rs:204-210", _UN(lambda a: a.sin()), (0.7,), "gradient", (math.cos(0.7),)),
+    "d_cos": ("opcode_edge_cases.rs:212-218", _UN(lambda a: a.cos()), (0.7,), "gradient", (-math.sin(0.7),)),
+    "d_sqrt": ("opcode_edge_cases.rs:220-226", _UN(lambda a: a.sqrt()), (4.0,), "gradient", (0.25,)),
+    "d_neg": ("opcode_edge_cases.rs:228-233", _UN(lambda a: -a), (5.0,), "gradient", (-1.0,)),
+    "d_recip": ("opcode_edge_cases.rs:235-239", _UN(lambda a: a.recip()), (2.0,), "gradient", (-0.25,)),
+    "d_powi": ("opcode_edge_cases.rs:241-247", _UN(lambda a: a.powi(3)), (2.0,), "gradient", (12.0,)),
+    "d_hypot": ("opcode_edge_cases.rs:252-256", _BI(lambda a, b: a.hypot(b)), (3.0, 4.0), "gradient", (0.6, 0.8)),
+    "d_atan2": ("opcode_edge_cases.rs:258-265", _BI(lambda a, b: a.atan2(b)), (1.0, 1.0), "gradient", (0.5, -0.5)),
+    "d_max_first": ("opcode_edge_cases.rs:267-271", _BI(lambda a, b: a.max(b)), (5.0, 3.0), "gradient", (1.0, 0.0)),
+    "d_max_second": ("opcode_edge_cases.rs:273-277", _BI(lambda a, b: a.max(b)), (3.0, 5.0), "gradient", (0.0, 1.0)),
+    "d_min_first": ("opcode_edge_cases.rs:279-283", _BI(lambda a, b: a.min(b)), (3.0, 5.0), "gradient", (1.0, 0.0)),
+    "d_abs_positive": ("opcode_edge_cases.rs:285-288", _UN(lambda a: a.abs()), (3.0,), "gradient", (1.0,)),
+}
+
+
+def _edge_check(name, value, grad):
+    _, _, _, call, want = OPCODE_EDGE[name]
+    if call == "forward":
+        assert want(float(value)), (name, value)
+    else:
+        assert all(abs(float(g) - w) < _T for g, w in zip(grad, want)), (name, list(grad), want)
+
+
+@pytest.mark.parametrize("name", sorted(OPCODE_EDGE))
+def test_oracle_opcode_edge_cases(name):
+    _, fn, x, call, _ = OPCODE_EDGE[name]
+    tape = record(fn, list(x))[0]
+    v, g = OracleTape(tape).gradient(np.asarray([x]))
+    _edge_check(name, v[0, 0], g[0])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(OPCODE_EDGE))
+def test_gpu_opcode_edge_cases(ctx, name):
+    _, fn, x, call, _ = OPCODE_EDGE[name]
+    tape = record(fn, list(x))[0]
+    gt = ctx.upload_tape_f64(tape)
+    xa = np.asarray(x, dtype=np.float64)
+    fwd = ctx.forward_batch_f64(gt, xa, 1)
+    v, g = ctx.gradient_batch_f64(gt, xa, 1)
+    assert np.array_equal(fwd, v, equal_nan=True)
+    _edge_check(name, v[0], g)
+
 
 def _poly(t, coeffs):
     """sum_k c_k t^k on the tape, built so that its jet at t = 0 along 1 is
@@ -266,3 +357,60 @@ def test_gpu_upload_with_empty_output_indices(ctx):
     gt = ctx.upload_tape(data)
     r, _ = ctx.gradient_batch(gt, np.asarray([2.0], np.float32), 1)
     assert r.size == 1 and abs(r[0] - 6.0) < 1e-5
+
+
+# stde_nonfinite_samples.rs: f = exp(x0 x1) at (1, 700).  A direction through x0
+# overflows the second-order coefficient (e^700 * 700^2 / 2), a non-finite sample
+# that the Welford accumulator skips; the zero direction gives the finite sample 0.
+LIVE, DEAD = [1.0, 0.0], [0.0, 0.0]
+NONFINITE = {
+    "skips_nonfinite": ("stde_nonfinite_samples.rs:28-39", [LIVE, DEAD, DEAD], 2, 0.0),
+    "all_nonfinite": ("stde_nonfinite_samples.rs:42-55", [LIVE, LIVE], 0, "nan"),
+}
+
+
+def _exp_prod_tape():
+    return record(lambda v: (v[0] * v[1]).exp(), [1.0, 700.0])[0]
+
+
+def _check_estimate(num_samples, estimate, se, want_n, want_est):
+    assert num_samples == want_n
+    if want_est == "nan":
+        assert math.isnan(estimate)
+    else:
+        assert estimate == want_est and math.isfinite(se)
+
+
+@pytest.mark.parametrize("name", sorted(NONFINITE))
+def test_oracle_laplacian_skips_nonfinite_samples(name):
+    _, dirs, want_n, want_est = NONFINITE[name]
+    r = OracleTape(_exp_prod_tape()).laplacian_stats_batch(np.asarray([[1.0, 700.0]]), np.asarray([dirs]))[0]
+    _check_estimate(int(r[4]), float(r[1]), float(r[3]), want_n, want_est)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(NONFINITE))
+def test_gpu_laplacian_skips_nonfinite_samples(ctx, name):
+    from echidna_b200.stde_gpu import DIR_PER_POINT, laplacian_batch
+    _, dirs, want_n, want_est = NONFINITE[name]
+    gt = ctx.upload_tape_f64(_exp_prod_tape())
+    r = laplacian_batch(ctx, gt, np.asarray([[1.0, 700.0]]), len(dirs), np.asarray([dirs]), DIR_PER_POINT)[0]
+    _check_estimate(int(r["num_samples"]), float(r["estimate"]), float(r["standard_error"]), want_n, want_est)
+
+
+def test_oracle_estimate_weighted_nonfinite_and_zero_weights():
+    o = OracleTape(_exp_prod_tape())
+    x = np.asarray([1.0, 700.0])
+    # stde_nonfinite_samples.rs:58-69: the non-finite sample is skipped
+    r = o.estimate_weighted(x, np.asarray([LIVE, DEAD]), np.asarray([1.0, 1.0]))
+    assert int(r[4]) == 1 and r[1] == 0.0
+    # :72-82: nothing contributes -> NaN
+    r = o.estimate_weighted(x, np.asarray([LIVE]), np.asarray([1.0]))
+    assert int(r[4]) == 0 and math.isnan(r[1])
+    # :85-99: zero weights still count as samples
+    q = OracleTape(record(lambda v: v[0] * v[0] + v[1] * v[1], [1.0, 2.0])[0])
+    r = q.estimate_weighted(np.asarray([1.0, 2.0]), np.asarray([[1.0, 0.0], [0.0, 1.0]]), np.asarray([1.0, 0.0]))
+    assert int(r[4]) == 2 and math.isfinite(r[1])
+    # :103-111: a negative weight is rejected
+    with pytest.raises(ValueError):
+        q.estimate_weighted(np.asarray([1.0, 2.0]), np.asarray([[1.0, 0.0]]), np.asarray([-1.0]))
