@@ -9,9 +9,10 @@ reference's own tolerances.  The second group restates CPU tests of the same
 conventions on the bytecode tape in f64 (``tests/atan2_extreme_magnitudes.rs``,
 ``tests/asinh_acosh_large.rs``, ``tests/taylor.rs``,
 ``tests/hypot_leading_zero_parity.rs``, ``tests/opcode_edge_cases.rs`` as one-op
-tapes, ``tests/stde_nonfinite_samples.rs``); Dual-number cases become JVPs of the
-one-op tape (a ``Dual::new(x, 1)`` operand is a seeded input, a
-``Dual::constant`` operand a tape constant).  The oracle runs every case in the
+tapes, ``tests/stde_nonfinite_samples.rs``, the tape cases of
+``tests/regressions.rs``); Dual-number cases become JVPs of the one-op tape (a
+``Dual::new(x, 1)`` operand is a seeded input, a ``Dual::constant`` operand a
+tape constant).  The oracle runs every case in the
 precision the case names (its f32 mode rounds the tape constants to f32, as
 ``from_tape_f64_lossy`` does).
 """
@@ -138,6 +139,26 @@ CASES = {
                         and abs(r["jet"][2] + math.sin(1.0) / 2.0) < 1e-10),
     "taylor_cube": ("taylor.rs:255-257, 397-405", lambda v: v[0] * v[0] * v[0], (2.0,), "f64", "taylor", (2.0,),
                     ((1.0,), 4), lambda r: list(r["jet"]) == [8.0, 12.0, 6.0, 1.0]),
+    # ── regressions.rs, tape cases (f64) ──
+    "reg_powi0_at_zero": ("regressions.rs:143-156", lambda v: v[0].powi(0), (0.0,), "f64", "gradient", (0.0,), None,
+                          lambda r: r["value"][0] == 1.0 and r["grad"][0] == 0.0),
+    "reg_hypot_origin": ("regressions.rs:191-212", lambda v: v[0].hypot(v[1]), (0.0, 0.0), "f64", "gradient",
+                         (0.0, 0.0), None, lambda r: r["value"][0] == 0.0 and r["grad"] == [0.0, 0.0]),
+    "reg_rem_partials": ("regressions.rs:522-530", lambda v: v[0] % v[1], (7.0, 3.0), "f64", "gradient", (7.0, 3.0),
+                         None, lambda r: r["value"][0] == 1.0 and r["grad"] == [1.0, -2.0]),
+    "reg_max_nan": ("regressions.rs:546-553", lambda v: v[0].max(v[1]), (5.0, NAN), "f64", "gradient", (5.0, NAN),
+                    None, lambda r: r["value"][0] == 5.0 and r["grad"][0] == 1.0),
+    "reg_min_nan": ("regressions.rs:555-562", lambda v: v[0].min(v[1]), (5.0, NAN), "f64", "gradient", (5.0, NAN),
+                    None, lambda r: r["value"][0] == 5.0 and r["grad"][0] == 1.0),
+    "reg_max_nan_replay": ("regressions.rs:564-571", lambda v: v[0].max(v[1]), (3.0, 4.0), "f64", "gradient",
+                           (5.0, NAN), None, lambda r: r["grad"][0] == 1.0),
+    "reg_atan2_origin": ("regressions.rs:603-610", lambda v: v[0].atan2(v[1]), (0.0, 0.0), "f64", "gradient",
+                         (0.0, 0.0), None, lambda r: all(math.isfinite(g) for g in r["grad"])),
+    "reg_powf_zero_exponent": ("regressions.rs:664-674", lambda v: v[0].powf(v[1]), (2.0, 0.0), "f64", "gradient",
+                               (2.0, 0.0), None, lambda r: r["value"][0] == 1.0 and r["grad"][0] == 0.0
+                               and abs(r["grad"][1] - math.log(2.0)) < 1e-12),
+    "reg_powf_zero_base": ("regressions.rs:686-692", lambda v: v[0].powf(v[1]), (0.0, 2.0), "f64", "gradient",
+                           (0.0, 2.0), None, lambda r: r["value"][0] == 0.0 and r["grad"][0] == 0.0),
 }
 
 # opcode_edge_cases.rs (TOL = 1e-10): eval_forward and reverse_partials of one op,
