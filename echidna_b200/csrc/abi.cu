@@ -1463,9 +1463,15 @@ static ech_status do_diag_kth(ech_ctx* ctx, const ech_tape* tc, const T* x, size
   CHECK(stde_checks(t, n, "diagonal_kth_order_stochastic", "diagonal"));
   if (n_idx == 0) return fail(ECH_ERR_OTHER, "sampled_indices must not be empty");
   if (k < 2) return fail(ECH_ERR_OTHER, "k must be >= 2 (use gradient for k=1)");
-  if (k + 1 > 5) {
+  // The reference's factorial-exactness limits (higher_order.rs:13-22), then
+  // the engine's own: jets are instantiated up to order 9, so k <= 8.
+  if (k > 18) return fail(ECH_ERR_OTHER, "k must be <= 18 (k! is exact in f64 only up to 18!; 19! exceeds 2^53)");
+  if (k > 12 && sizeof(T) == 4)
+    return fail(ECH_ERR_OTHER,
+                "k must be <= 12 for f32 (one order of margin: f32 k! exactness first degrades at 14!; use f64)");
+  if (k + 1 > 9) {
     char buf[96];
-    snprintf(buf, sizeof buf, "unsupported Taylor order %u, must be 1..=5", k + 1);
+    snprintf(buf, sizeof buf, "unsupported Taylor order %u, must be 1..=9", k + 1);
     return fail(ECH_ERR_OTHER, buf);
   }
   if (!x || !idx || !out) return fail(ECH_ERR_INVALID_ARG, "null buffer");

@@ -115,7 +115,10 @@ class GpuTapeData:
         """``GpuTapeData::from_tape_f64_lossy`` (``src/gpu/mod.rs:378-384``)."""
         if tape.has_custom_ops:
             raise CustomOpsNotSupported("tape contains custom ops which cannot run on GPU")
-        return cls._build(tape, np.asarray(tape.values, dtype=np.float64).astype(np.float32))
+        # `as f32` in the reference: magnitudes past f32's range become +-inf
+        with np.errstate(over="ignore"):
+            vals = np.asarray(tape.values, dtype=np.float64).astype(np.float32)
+        return cls._build(tape, vals)
 
     def _arrays(self):
         return (np.ascontiguousarray(self.opcodes, dtype=np.uint32), np.ascontiguousarray(self.arg0, dtype=np.uint32),

@@ -89,7 +89,7 @@ def laplacian_batch(backend: CudaContext, tape, xs, num_directions: int, directi
 
 def diagonal_kth_order_stochastic_gpu(backend: CudaContext, tape, x, k: int, sampled_indices) -> EstimatorResult:
     """``stde::diagonal_kth_order_stochastic`` (``src/stde/higher_order.rs:173-227``) on the GPU:
-    ``n * mean_j(k! * c_k)`` over jets along ``e_j`` for the sampled coordinates (k = 2..4)."""
+    ``n * mean_j(k! * c_k)`` over jets along ``e_j`` for the sampled coordinates (k = 2..8)."""
     lib = _lib.load()
     f64 = bool(tape.f64)
     dt = np.float64 if f64 else np.float32

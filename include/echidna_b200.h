@@ -228,9 +228,11 @@ ECH_API ech_status ech_gradient_batch_device_noalloc(ech_ctx* ctx, const ech_tap
 /* Extension: stde::diagonal_kth_order_stochastic (src/stde/higher_order.rs:173-227)
  * on the GPU: one jet of order k+1 along e_j per sampled index j, samples k!*c_k,
  * Welford in the sample type, estimate / variance / SE rescaled by n, n^2, n.
- * k in 2..=4 (jets up to order 5).  Errors use the reference's texts
+ * k in 2..=8 (jets up to order 9).  Errors use the reference's texts
  * ("sampled_indices must not be empty", "k must be >= 2 (use gradient for k=1)",
- * "sampled index {j} out of bounds (n={n})"); scalar-output tapes only. */
+ * "k must be <= 18 ...", "k must be <= 12 for f32 ...", "sampled index {j} out of
+ * bounds (n={n})"), then "unsupported Taylor order {k+1}, must be 1..=9" for
+ * 9 <= k <= 18; scalar-output tapes only. */
 ECH_API ech_status ech_diagonal_kth_order_stochastic_f32(ech_ctx* ctx, const ech_tape* tape, const float* x, size_t n,
                                                          uint32_t k, const uint32_t* sampled_indices,
                                                          size_t n_indices, ech_estimator_result* out);

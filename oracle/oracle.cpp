@@ -1351,6 +1351,9 @@ template <class F, int ORDER> void dks(const orc::Tape<F>& t, const F* x, const 
       case 3: dks<F, 4>(t, x, idx, nidx, out); return 0;                                                            \
       case 4: dks<F, 5>(t, x, idx, nidx, out); return 0;                                                            \
       case 5: dks<F, 6>(t, x, idx, nidx, out); return 0;                                                            \
+      case 6: dks<F, 7>(t, x, idx, nidx, out); return 0;                                                            \
+      case 7: dks<F, 8>(t, x, idx, nidx, out); return 0;                                                            \
+      case 8: dks<F, 9>(t, x, idx, nidx, out); return 0;                                                            \
       default: return -1;                                                                                           \
     }                                                                                                               \
   }

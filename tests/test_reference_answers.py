@@ -6,15 +6,20 @@ The first group restates the reference's CUDA and GPU-fix tests
 ``tests/phase7_gpu_fixes.rs``, ``tests/phase7_gpu_parity.rs``): an f64-recorded
 tape uploaded with ``from_tape_f64_lossy`` and evaluated in f32, with the
 reference's own tolerances.  The second group restates CPU tests of the same
-conventions on the bytecode tape in f64 (``tests/atan2_extreme_magnitudes.rs``,
-``tests/asinh_acosh_large.rs``, ``tests/taylor.rs``,
-``tests/hypot_leading_zero_parity.rs``, ``tests/opcode_edge_cases.rs`` as one-op
-tapes, ``tests/stde_nonfinite_samples.rs``, the tape cases of
-``tests/regressions.rs``); Dual-number cases become JVPs of the one-op tape (a
-``Dual::new(x, 1)`` operand is a seeded input, a ``Dual::constant`` operand a
-tape constant).  The oracle runs every case in the
-precision the case names (its f32 mode rounds the tape constants to f32, as
-``from_tape_f64_lossy`` does).
+conventions on the bytecode tape in f64:
+
+* ``tests/atan2_extreme_magnitudes.rs`` and ``tests/asinh_acosh_large.rs``;
+* ``tests/taylor.rs``: its tape jets and, as jets of one-op tapes, the series
+  of its Taylor-type tests;
+* ``tests/hypot_leading_zero_parity.rs`` (jets built from polynomials);
+* ``tests/opcode_edge_cases.rs`` as forward values and gradients of one-op tapes;
+* ``tests/stde_nonfinite_samples.rs`` (the Welford accumulator);
+* the tape cases of ``tests/regressions.rs``.
+
+Dual-number cases become JVPs of the one-op tape (a ``Dual::new(x, 1)`` operand
+is a seeded input, a ``Dual::constant`` operand a tape constant).  The oracle
+runs every case in the precision the case names (its f32 mode rounds the tape
+constants to f32, as ``from_tape_f64_lossy`` does).
 """
 import math
 
@@ -352,6 +357,51 @@ def test_gpu_reference_answers(ctx, name):
     assert case[-1](res), (name, case[0], res)
 
 
+# taylor.rs:11-157 (epsilon 1e-12): Taylor::<f64, K>::variable(x0) through one op,
+# i.e. the jet of a one-op tape at x0 along 1; polynomial jets built with _poly
+_C1 = lambda: constant(1.0)  # noqa: E731
+TAYLOR_OPS = {
+    "exp_at_0": ("taylor.rs:11-20", lambda t: t.exp(), 0.0, [1.0, 1.0, 0.5, 1 / 6, 1 / 24]),
+    "sin_at_0": ("taylor.rs:23-32", lambda t: t.sin(), 0.0, [0.0, 1.0, 0.0, -1 / 6, 0.0]),
+    "cos_at_0": ("taylor.rs:35-44", lambda t: t.cos(), 0.0, [1.0, 0.0, -0.5, 0.0, 1 / 24]),
+    "ln_1p_at_0": ("taylor.rs:47-57", lambda t: (_C1() + t).ln(), 0.0, [0.0, 1.0, -0.5, 1 / 3, -0.25]),
+    "geometric": ("taylor.rs:60-68", lambda t: _C1() / (_C1() - t), 0.0, [1.0] * 5),
+    "exp_at_1.5": ("taylor.rs:75-83", lambda t: t.exp(), 1.5, [math.exp(1.5), math.exp(1.5)]),
+    "sin_at_0.7": ("taylor.rs:86-92", lambda t: t.sin(), 0.7, [math.sin(0.7), math.cos(0.7)]),
+    "ln_at_2": ("taylor.rs:95-101", lambda t: t.ln(), 2.0, [math.log(2.0), 0.5]),
+    "sqrt_at_4": ("taylor.rs:104-110", lambda t: t.sqrt(), 4.0, [2.0, 0.25]),
+    "atan_at_0.5": ("taylor.rs:113-119", lambda t: t.atan(), 0.5, [math.atan(0.5), 1 / 1.25]),
+    "tanh_at_0.3": ("taylor.rs:122-128", lambda t: t.tanh(), 0.3, [math.tanh(0.3), 1 / math.cosh(0.3) ** 2]),
+    "cauchy_product": ("taylor.rs:135-146", lambda t: _poly(t, [1.0, 1.0]) * _poly(t, [1.0, 1.0]), 0.0,
+                       [1.0, 2.0, 1.0]),
+    "recursive_division": ("taylor.rs:149-157", lambda t: _poly(t, [1.0, 2.0, 1.0]) / _poly(t, [1.0, 1.0]), 0.0,
+                           [1.0, 1.0, 0.0]),
+}
+
+
+def _taylor_op_tape(name):
+    _, fn, x0, _ = TAYLOR_OPS[name]
+    return record(lambda v: fn(v[0]), [x0 + 0.25])[0]
+
+
+@pytest.mark.parametrize("name", sorted(TAYLOR_OPS))
+def test_oracle_taylor_op_rules(name):
+    _, _, x0, want = TAYLOR_OPS[name]
+    c = OracleTape(_taylor_op_tape(name)).taylor(np.asarray([[x0]]), np.asarray([[1.0]]), len(want))
+    got = [float(c[k][0]) for k in range(len(want))]
+    assert all(abs(g - w) < 1e-12 for g, w in zip(got, want)), (name, got, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(TAYLOR_OPS))
+def test_gpu_taylor_op_rules(ctx, name):
+    _, _, x0, want = TAYLOR_OPS[name]
+    gt = ctx.upload_tape_f64(_taylor_op_tape(name))
+    res = ctx.taylor_forward_kth_batch_f64(gt, np.asarray([x0]), np.ones(1), 1, len(want))
+    got = [float(res.coefficients[k][0]) for k in range(len(want))]
+    assert all(abs(g - w) < 1e-12 for g, w in zip(got, want)), (name, got, want)
+
+
 @pytest.mark.parametrize("name", sorted(HYPOT_JETS))
 def test_oracle_hypot_jets_leading_zeros(name):
     _, a, b, want = HYPOT_JETS[name]
@@ -435,3 +485,246 @@ def test_oracle_estimate_weighted_nonfinite_and_zero_weights():
     # :103-111: a negative weight is rejected
     with pytest.raises(ValueError):
         q.estimate_weighted(np.asarray([1.0, 2.0]), np.asarray([[1.0, 0.0]]), np.asarray([-1.0]))
+
+
+# stde_higher_order.rs: diagonal_kth_order(_stochastic) and parabolic diffusion.
+# diagonal_kth_order(tape, x, k)[j] is the stochastic estimate over the single
+# index j divided by n (the estimator rescales the mean by n / |J| * |J|).
+def _exp_1d():
+    return record(lambda v: v[0].exp(), [1.0])[0]
+
+
+def _quartic():
+    return record(lambda v: v[0] * v[0] * v[0] * v[0] + v[1] * v[1] * v[1] * v[1], [2.0, 3.0])[0]
+
+
+def _cubic_mix():
+    return record(lambda v: v[0] * v[0] * v[1] + v[1] * v[1] * v[1], [1.0, 2.0, 3.0])[0]
+
+
+E = math.e
+# name: (source, tape, x, k, sampled indices, estimate, tolerance)
+KTH_ORDER = {
+    **{f"exp_k{k}": ("stde_higher_order.rs:39-51", _exp_1d, [1.0], k, [0], E, 10.0 ** -(12 - k))
+       for k in (2, 3, 4, 5)},
+    # :53-68: d^4/dx^4 (x^4 + y^4) = 24 each; the order-5 derivatives vanish
+    "quartic_k4_x": ("stde_higher_order.rs:53-68", _quartic, [2.0, 3.0], 4, [0], 2 * 24.0, 1e-6),
+    "quartic_k4_y": ("stde_higher_order.rs:53-68", _quartic, [2.0, 3.0], 4, [1], 2 * 24.0, 1e-6),
+    "quartic_k5": ("stde_higher_order.rs:53-68", _quartic, [2.0, 3.0], 5, [0, 1], 0.0, 1e-4),
+    # :83-93 and :95-103: the full sample and the n/|J| scaling both give 48
+    "full_sample": ("stde_higher_order.rs:83-93", _quartic, [2.0, 3.0], 4, [0, 1], 48.0, 1e-4),
+    "scaling": ("stde_higher_order.rs:95-103", _quartic, [2.0, 3.0], 4, [0], 48.0, 1e-4),
+    # :70-81: k = 2 is the Hessian diagonal, (2y, 6y, 0) at (1, 2, 3); summed: 16
+    "cubic_mix_k2": ("stde_higher_order.rs:70-81", _cubic_mix, [1.0, 2.0, 3.0], 2, [0, 1, 2], 16.0, 1e-10),
+}
+
+
+def _kth_check(name, value, estimate):
+    _, mk, x, k, idx, want, tol = KTH_ORDER[name]
+    assert _close(value, float(OracleTape(mk()).forward(np.asarray([x]))[0][0]), 1e-12), name
+    assert abs(estimate - want) <= tol * max(1.0, abs(want)), (name, estimate, want)
+
+
+@pytest.mark.parametrize("name", sorted(KTH_ORDER))
+def test_oracle_diagonal_kth_order(name):
+    _, mk, x, k, idx, _, _ = KTH_ORDER[name]
+    r = OracleTape(mk()).diagonal_kth_order_stochastic(np.asarray(x), k, idx)
+    _kth_check(name, float(r[0]), float(r[1]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(KTH_ORDER))
+def test_gpu_diagonal_kth_order(ctx, name):
+    from echidna_b200.stde_gpu import diagonal_kth_order_stochastic_gpu
+    _, mk, x, k, idx, _, _ = KTH_ORDER[name]
+    r = diagonal_kth_order_stochastic_gpu(ctx, ctx.upload_tape_f64(mk()), x, k, idx)
+    assert r.num_samples == len(idx)
+    _kth_check(name, r.value, r.estimate)
+
+
+@pytest.mark.gpu
+def test_gpu_diagonal_kth_order_limits(ctx):
+    # stde_higher_order.rs:105-118 and higher_order.rs:13-22: the reference's k
+    # range, then the engine's jet limit (order 9) for 9 <= k <= 18
+    from echidna_b200.gpu import GpuError
+    from echidna_b200.stde_gpu import diagonal_kth_order_stochastic_gpu
+    gt = ctx.upload_tape_f64(_exp_1d())
+    with pytest.raises(GpuError, match="k must be >= 2"):
+        diagonal_kth_order_stochastic_gpu(ctx, gt, [1.0], 1, [0])
+    with pytest.raises(GpuError, match="k must be <= 18"):
+        diagonal_kth_order_stochastic_gpu(ctx, gt, [1.0], 19, [0])
+    with pytest.raises(GpuError, match="k must be <= 12 for f32"):
+        f32_tape = ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(_exp_1d()))
+        diagonal_kth_order_stochastic_gpu(ctx, f32_tape, [1.0], 13, [0])
+    with pytest.raises(GpuError, match="unsupported Taylor order 10"):
+        diagonal_kth_order_stochastic_gpu(ctx, gt, [1.0], 9, [0])
+    # the highest order the engine runs: d^8/dx^8 exp(x) = e
+    r = diagonal_kth_order_stochastic_gpu(ctx, gt, [1.0], 8, [0])
+    assert abs(r.estimate - E) <= 1e-3
+
+
+# stde_higher_order.rs:150-181: sigma = I on x^2 + y^2 at (1, 2) gives the value
+# 5 and the diffusion 1/2 tr(H) = 2; the full stochastic sample matches it.
+@pytest.mark.gpu
+def test_gpu_parabolic_diffusion_identity_sigma(ctx):
+    from echidna_b200.stde_gpu import parabolic_diffusion_gpu, parabolic_diffusion_stochastic_gpu
+    gt = ctx.upload_tape_f64(record(lambda v: v[0] * v[0] + v[1] * v[1], [1.0, 2.0])[0])
+    sig = np.eye(2)
+    value, diffusion = parabolic_diffusion_gpu(ctx, gt, [1.0, 2.0], sig)
+    assert abs(value - 5.0) <= 1e-10 and abs(diffusion - 2.0) <= 1e-10
+    r = parabolic_diffusion_stochastic_gpu(ctx, gt, [1.0, 2.0], sig, [0, 1])
+    assert abs(r.estimate - diffusion) <= 1e-10
+
+
+# gpu_stde.rs, section 2 (run by the reference on its CUDA backend too): f32 jets
+# of one-op tapes from taylor_forward_2nd_batch along 1, uploaded with
+# from_tape_f64_lossy.  check_1d (:187-226) compares c0, c1, c2 against the f64 CPU
+# jet with an absolute floor of 1e-2 and relative 1e-4, 1e-4, 1e-3.
+_U1 = {
+    "exp": lambda t: t.exp(), "ln": lambda t: t.ln(), "exp2": lambda t: t.exp2(), "log2": lambda t: t.log2(),
+    "log10": lambda t: t.log10(), "ln_1p": lambda t: t.ln_1p(), "exp_m1": lambda t: t.exp_m1(),
+    "sqrt": lambda t: t.sqrt(), "cbrt": lambda t: t.cbrt(), "sin": lambda t: t.sin(), "cos": lambda t: t.cos(),
+    "tan": lambda t: t.tan(), "sinh": lambda t: t.sinh(), "cosh": lambda t: t.cosh(), "tanh": lambda t: t.tanh(),
+    "asin": lambda t: t.asin(), "acos": lambda t: t.acos(), "atan": lambda t: t.atan(),
+    "asinh": lambda t: t.asinh(), "acosh": lambda t: t.acosh(), "atanh": lambda t: t.atanh(),
+    "abs": lambda t: t.abs(), "powi3": lambda t: t.powi(3), "powf25": lambda t: t.powf(constant(2.5)),
+    "powf3": lambda t: t.powf(constant(3.0)),
+    "arith": lambda t: (t + _C1()) * (constant(2.0) - t) + t.recip(),
+    "div": lambda t: (t * t + _C1()) / (t + _C1()),
+    "signum": lambda t: t.signum(), "round": lambda t: t.round(),
+}
+JET_1D = {f"{op}@{x0}": (op, x0) for op, x0 in [
+    # :363-480
+    ("exp", 1.5), ("ln", 2.0), ("exp2", 1.0), ("log2", 3.0), ("log10", 2.0), ("ln_1p", 0.5), ("exp_m1", 0.3),
+    ("sqrt", 4.0), ("cbrt", 8.0), ("sin", 1.0), ("cos", 1.0), ("tan", 0.5), ("sinh", 1.0), ("cosh", 1.0),
+    ("tanh", 0.5), ("asin", 0.5), ("acos", 0.5), ("atan", 1.0), ("asinh", 1.0), ("acosh", 2.0), ("atanh", 0.5),
+    ("powf25", 2.0), ("powi3", 2.0), ("powi3", -2.0), ("powf3", -2.0), ("arith", 1.5), ("div", 2.0),
+    ("abs", -2.0), ("abs", 2.0),
+    # :482-497, near |x| = 1
+    ("asin", 0.9), ("acos", 0.9), ("atanh", 0.9), ("asin", 0.99), ("acos", 0.99), ("atanh", 0.99)]}
+
+
+def _jet1(op, x0):
+    return record(lambda v: _U1[op](v[0]), [x0])[0]
+
+
+def _f32_jets(run, tape, x, seed):
+    """(c0, c1, c2) of output 0 of one f32 point: ``run`` is "oracle" or a context."""
+    xs, ss = np.asarray([x], np.float32), np.asarray([seed], np.float32)
+    if run == "oracle":
+        c = OracleTape(tape, dtype=np.float32).taylor(xs, ss, 3)
+        return tuple(float(c[k][0]) for k in range(3))
+    r = run.taylor_forward_2nd_batch(run.upload_tape(GpuTapeData.from_tape_f64_lossy(tape)), xs.ravel(),
+                                     ss.ravel(), 1)
+    return float(r.values[0]), float(r.c1s[0]), float(r.c2s[0])
+
+
+def _check_1d(run, name):
+    op, x0 = JET_1D[name]
+    tape = _jet1(op, x0)
+    got = _f32_jets(run, tape, [x0], [1.0])
+    c = OracleTape(tape).taylor(np.asarray([[x0]]), np.asarray([[1.0]]), 3)
+    want = [float(c[k][0]) for k in range(3)]
+    for g, w, rel in zip(got, want, (1e-4, 1e-4, 1e-3)):
+        assert abs(g - w) < max(1e-2, abs(w) * rel), (name, got, want)
+
+
+@pytest.mark.parametrize("name", sorted(JET_1D))
+def test_oracle_f32_jets_match_f64(name):
+    _check_1d("oracle", name)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(JET_1D))
+def test_gpu_f32_jets_match_f64(ctx, name):
+    _check_1d(ctx, name)
+
+
+_NEXT_BELOW_HALF = float(np.frombuffer(np.uint32(0x3EFFFFFF).tobytes(), np.float32)[0])
+# name: (source, op or binary fn, inputs, seed, expected (c0, c1, c2) with None = any;
+# "nan", "+inf", "-inf" classes, or (value, rel) for a relative check of c0 against
+# the f64 truth at the f32-rounded input)
+JET_EDGE = {
+    # :498-535 (check_primal_rel, tolerance 1e-3) and the overflow limit
+    "expm1@1e-6": (":498-500", "exp_m1", [1e-6], [1.0], ("rel", math.expm1), None, None),
+    "expm1@1e-7": (":498-500", "exp_m1", [1e-7], [1.0], ("rel", math.expm1), None, None),
+    "ln1p@1e-6": (":498-500", "ln_1p", [1e-6], [1.0], ("rel", math.log1p), None, None),
+    "ln1p@1e-7": (":498-500", "ln_1p", [1e-7], [1.0], ("rel", math.log1p), None, None),
+    "expm1@87": (":531", "exp_m1", [87.0], [1.0], ("rel", math.expm1), None, None),
+    "expm1@90": (":512-526", "exp_m1", [90.0], [1.0], "+inf", None, None),
+    # :537-564: all-NaN jets strictly outside the real domain
+    **{f"{op}@{x}_nan": (":537-564", op, [x], [1.0], "nan", "nan", "nan") for op, x in [
+        ("ln", -2.0), ("log2", -2.0), ("log10", -2.0), ("ln_1p", -2.0), ("acosh", -2.0), ("atanh", 1.5),
+        ("asin", 1.5), ("acos", 1.5), ("acosh", 0.5)]},
+    # :566-600: the domain boundary keeps its branch-point value
+    "acosh@1": (":573-577", "acosh", [1.0], [1.0], 0.0, None, None),
+    "atanh@1": (":578-582", "atanh", [1.0], [1.0], "+inf", None, None),
+    "atanh@-1": (":585-589", "atanh", [-1.0], [1.0], "-inf", None, None),
+    "ln1p@-1": (":590-594", "ln_1p", [-1.0], [1.0], "-inf", None, None),
+    "ln@0": (":595-599", "ln", [0.0], [1.0], "-inf", None, None),
+    # :603-627: max / min keep the finite operand against NaN
+    "max_nan": (":611-618", lambda v: v[0].max(v[1]), [1.0, NAN], [1.0, 0.0], 1.0, None, None),
+    "min_nan": (":619-626", lambda v: v[0].min(v[1]), [1.0, NAN], [1.0, 0.0], 1.0, None, None),
+    # :629-641: rem by a zero-leading divisor is an all-NaN jet
+    "rem_zero": (":637-641", lambda v: v[0] % v[1], [3.0, 0.0], [1.0, 0.0], "nan", "nan", "nan"),
+    # :643-683: signum(-0) = -1 and round ties away from zero
+    "signum@-0": (":657-659", "signum", [-0.0], [1.0], -1.0, None, None),
+    "round@2.5": (":662-663", "round", [2.5], [1.0], 3.0, None, None),
+    "round@-2.5": (":664-665", "round", [-2.5], [1.0], -3.0, None, None),
+    "round@0.5": (":666-670", "round", [0.5], [1.0], 1.0, None, None),
+    "round@8388609": (":673-678", "round", [8388609.0], [1.0], 8388609.0, None, None),
+    "round@below_half": (":679-682", "round", [_NEXT_BELOW_HALF], [1.0], 0.0, None, None),
+    # :687-715: sqrt at 0 has a uniform +Inf jet
+    "sqrt@0": (":687-715", "sqrt", [0.0], [1.0], 0.0, "+inf", "+inf"),
+}
+
+
+def _edge_tape(fn, x):
+    f = (lambda v: _U1[fn](v[0])) if isinstance(fn, str) else fn
+    return record(f, list(x))[0]
+
+
+def _check_class(got, want, x, label):
+    if want is None:
+        return
+    if isinstance(want, tuple):
+        truth = want[1](float(np.float32(x)))
+        assert abs(got - truth) / max(abs(truth), 2.2e-308) < 1e-3, (label, got, truth)
+    elif want == "nan":
+        assert math.isnan(got), (label, got)
+    elif want in ("+inf", "-inf"):
+        assert math.isinf(got) and (got > 0) == (want == "+inf"), (label, got)
+    else:
+        assert got == want, (label, got, want)
+
+
+def _jet_edge(run, name):
+    _, fn, x, seed, *want = JET_EDGE[name]
+    got = _f32_jets(run, _edge_tape(fn, x), x, seed)
+    for k in range(3):
+        _check_class(got[k], want[k], x[0], (name, k))
+
+
+@pytest.mark.filterwarnings("ignore:overflow encountered in cast")  # the recorded e^90 in f32
+@pytest.mark.parametrize("name", sorted(JET_EDGE))
+def test_oracle_f32_jet_edge_cases(name):
+    _jet_edge("oracle", name)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(JET_EDGE))
+def test_gpu_f32_jet_edge_cases(ctx, name):
+    _jet_edge(ctx, name)
+
+
+# gpu_stde.rs:864-913: x^2 + y^2 at (3, 4) in f32.  The four Rademacher
+# directions give the Laplacian 4 exactly; the Hessian diagonal is (2, 2), value 25.
+@pytest.mark.gpu
+def test_gpu_polynomial_exact_laplacian_and_diagonal(ctx):
+    from echidna_b200.stde_gpu import hessian_diagonal_gpu, laplacian_gpu
+    gt = ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(record(lambda v: v[0] * v[0] + v[1] * v[1],
+                                                                [3.0, 4.0])[0]))
+    dirs = [[1.0, 1.0], [1.0, -1.0], [-1.0, 1.0], [-1.0, -1.0]]
+    assert abs(laplacian_gpu(ctx, gt, [3.0, 4.0], dirs).estimate - 4.0) < 1e-3
+    val, diag = hessian_diagonal_gpu(ctx, gt, [3.0, 4.0])
+    assert abs(val - 25.0) < 1e-3 and abs(diag[0] - 2.0) < 1e-3 and abs(diag[1] - 2.0) < 1e-3
