@@ -728,3 +728,110 @@ def test_gpu_polynomial_exact_laplacian_and_diagonal(ctx):
     assert abs(laplacian_gpu(ctx, gt, [3.0, 4.0], dirs).estimate - 4.0) < 1e-3
     val, diag = hessian_diagonal_gpu(ctx, gt, [3.0, 4.0])
     assert abs(val - 25.0) < 1e-3 and abs(diag[0] - 2.0) < 1e-3 and abs(diag[1] - 2.0) < 1e-3
+
+
+# gpu_stde.rs:1353-2093, the cases the reference runs with its CUDA backend: f32
+# jets from taylor_forward_kth_batch (tape recorded at `rec`, evaluated at `x`).
+# Expectations per coefficient: a number (exact), ("near", v, tol), "nan",
+# "+inf", "inf" (either sign), or "cpu": check_hypot_jet's finiteness plus the
+# check_1d tolerances against the f64 CPU jet.
+_HYP = lambda v: v[0].hypot(v[1])  # noqa: E731
+_CPU3 = ("cpu", "cpu", "cpu")
+CUDA_JETS = {
+    # :1532-1558 (check_hypot_jet)
+    "hypot(3,4)_dx": (":1534-1541", _HYP, [3.0, 4.0], [3.0, 4.0], [1.0, 0.0], _CPU3),
+    "hypot(3,4)_dy": (":1534-1541", _HYP, [3.0, 4.0], [3.0, 4.0], [0.0, 1.0], _CPU3),
+    "hypot(1e20,1e19)_dx": (":1545-1551", _HYP, [1e20, 1e19], [1e20, 1e19], [1.0, 0.0], _CPU3),
+    "hypot(0,0)_dx": (":1555-1558", _HYP, [0.0, 0.0], [0.0, 0.0], [1.0, 0.0], _CPU3),
+    # :1504-1515: a NaN operand makes the whole jet NaN (tape recorded at (1, 1))
+    "hypot(nan,0)": (":1506-1514", _HYP, [1.0, 1.0], [NAN, 0.0], [1.0, 0.0], ("nan", "nan", "nan")),
+    "hypot(0,nan)": (":1506-1514", _HYP, [1.0, 1.0], [0.0, NAN], [1.0, 0.0], ("nan", "nan", "nan")),
+    "hypot(nan,1)": (":1506-1514", _HYP, [1.0, 1.0], [NAN, 1.0], [1.0, 0.0], ("nan", "nan", "nan")),
+    # :1731-1757 and :1784-1801
+    "hypot(inf,1)": (":1733-1757", _HYP, [INF, 1.0], [INF, 1.0], [1.0, 0.0], ("inf", "nan", "nan")),
+    "hypot(1,inf)": (":1733-1757", _HYP, [1.0, INF], [1.0, INF], [1.0, 0.0], ("inf", "nan", "nan")),
+    "hypot_identically_zero": (":1786-1801", _HYP, [0.0, 0.0], [0.0, 0.0], [0.0, 0.0], (0.0, 0.0, 0.0)),
+    # :1853-1877: fract is x - trunc(x)
+    "fract(-2.3)": (":1853-1877", lambda v: v[0].fract(), [-2.3], [-2.3], [1.0],
+                    (("near", -0.3, 1e-5), ("near", 1.0, 1e-6), None)),
+    # :1880-1901: hypot(t^2, 0) = t^2, a depth-two shift
+    "hypot_depth_two": (":1880-1901", lambda v: (v[0] * v[0]).hypot(v[1]), [0.0, 0.0], [0.0, 0.0], [1.0, 0.0],
+                        tuple(("near", e, 1e-6) for e in (0.0, 0.0, 1.0, 0.0, 0.0))),
+    # :1904-1922: x^10 seeded at 0 has valuation 10 > K - 1
+    "powi10_at_0": (":1904-1922", lambda v: v[0].powi(10), [0.0], [0.0], [1.0], (0.0,) * 5),
+    # :1987-2011: x^2.5 at 0 (recorded at 1): zero below the branch order, +Inf above
+    "powf2.5_at_0": (":1987-2011", lambda v: v[0].powf(constant(2.5)), [1.0], [0.0], [1.0],
+                     (0.0, 0.0, 0.0, "+inf", "+inf")),
+}
+
+
+def _f32_kth(run, tape, x, seed, K):
+    xs, ss = np.asarray([x], np.float32), np.asarray([seed], np.float32)
+    if run == "oracle":
+        c = OracleTape(tape, dtype=np.float32).taylor(xs, ss, K)
+        return [float(c[k][0]) for k in range(K)]
+    r = run.taylor_forward_kth_batch(run.upload_tape(GpuTapeData.from_tape_f64_lossy(tape)), xs.ravel(),
+                                     ss.ravel(), 1, K)
+    return [float(r.coefficients[k][0]) for k in range(K)]
+
+
+def _cuda_jet(run, name):
+    _, fn, rec, x, seed, want = CUDA_JETS[name]
+    tape = record(fn, list(rec))[0]
+    got = _f32_kth(run, tape, x, seed, len(want))
+    cpu = None
+    if "cpu" in want:
+        c = OracleTape(tape).taylor(np.asarray([x]), np.asarray([seed]), len(want))
+        cpu = [float(c[k][0]) for k in range(len(want))]
+    for k, (g, w) in enumerate(zip(got, want)):
+        label = (name, k, got)
+        if w == "cpu":
+            rel = 1e-3 if k == 2 else 1e-4
+            assert math.isfinite(g) and abs(g - cpu[k]) < max(1e-2, abs(cpu[k]) * rel), (label, cpu)
+        elif w == "inf":
+            assert math.isinf(g), label
+        elif isinstance(w, tuple):
+            assert abs(g - w[1]) < w[2], label
+        elif w is not None:
+            _check_class(g, w, x[0], label)
+
+
+@pytest.mark.parametrize("name", sorted(CUDA_JETS))
+def test_oracle_f32_cuda_backend_jets(name):
+    _cuda_jet("oracle", name)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(CUDA_JETS))
+def test_gpu_f32_cuda_backend_jets(ctx, name):
+    _cuda_jet(ctx, name)
+
+
+def _sqrt_hypot_tape():
+    return record(lambda v: v[0].hypot(v[1]).sqrt(), [3.0, 4.0])[0]
+
+
+# gpu_stde.rs:2038-2090: sqrt'(0) = Inf reaches hypot's origin node, whose partials
+# are exactly 0: gradient and HVP are 0 there; away from it the replay holds.
+_ZM_X = 0.6 * 0.5 / math.sqrt(5.0)
+
+
+def test_oracle_f32_zero_multiplier_absorbs_inf_adjoint():
+    o = OracleTape(_sqrt_hypot_tape(), dtype=np.float32)
+    _, g = o.gradient(np.asarray([[0.0, 0.0]], np.float32))
+    assert list(g[0]) == [0.0, 0.0]
+    _, g = o.gradient(np.asarray([[3.0, 4.0]], np.float32))
+    assert abs(g[0][0] - _ZM_X) < 1e-5
+    hg, hv = o.hvp(np.asarray([0.0, 0.0], np.float32), np.asarray([[1.0, 0.0]], np.float32))
+    assert list(hg[0]) == [0.0, 0.0] and list(hv[0]) == [0.0, 0.0]
+
+
+@pytest.mark.gpu
+def test_gpu_f32_zero_multiplier_absorbs_inf_adjoint(ctx):
+    gt = ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(_sqrt_hypot_tape()))
+    _, g = ctx.gradient_batch(gt, np.asarray([0.0, 0.0], np.float32), 1)
+    assert list(np.asarray(g, np.float64)) == [0.0, 0.0]
+    _, g = ctx.gradient_batch(gt, np.asarray([3.0, 4.0], np.float32), 1)
+    assert abs(float(g[0]) - _ZM_X) < 1e-5
+    hg, hv = ctx.hvp_batch(gt, np.asarray([0.0, 0.0], np.float32), np.asarray([1.0, 0.0], np.float32), 1)
+    assert list(np.asarray(hg, np.float64)) == [0.0, 0.0] and list(np.asarray(hv, np.float64)) == [0.0, 0.0]
