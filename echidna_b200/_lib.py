@@ -109,6 +109,8 @@ _SIGS = {
     "ech_laplacian_batch_device": ([_P, _P, _I, _P, _U32, _P, _U32, _I, _U64, _P, _P], _I),
     "ech_diagonal_kth_order_stochastic_f32": ([_P, _P, _P, _SZ, _U32, _P, _SZ, _P], _I),
     "ech_diagonal_kth_order_stochastic_f64": ([_P, _P, _P, _SZ, _U32, _P, _SZ, _P], _I),
+    "ech_diagonal_kth_order_f32": ([_P, _P, _P, _SZ, _U32, _P, _P], _I),
+    "ech_diagonal_kth_order_f64": ([_P, _P, _P, _SZ, _U32, _P, _P], _I),
     "ech_stde_sparse_batch_f32": ([_P, _P, _P, _SZ, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, ctypes.c_float, _P, _U32,
                                    _P], _I),
     "ech_stde_sparse_batch_f64": ([_P, _P, _P, _SZ, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, ctypes.c_double, _P, _U32,

@@ -1452,6 +1452,23 @@ ECH_API ech_status ech_laplacian_batch_f64(ech_ctx* ctx, const ech_tape* t, cons
   return do_laplacian_batch<double>(ctx, t, xs, n_xs, B, dirs, n_dirs, S, dir_mode, seed, res);
 }
 
+// The k range of the k-th order diagonals: the reference's checks
+// (higher_order.rs:56 and the factorial-exactness limits at :13-22), then the
+// engine's own: jets are instantiated up to order 9, so k <= 8.
+static ech_status kth_order_range(uint32_t k, bool f32) {
+  if (k < 2) return fail(ECH_ERR_OTHER, "k must be >= 2 (use gradient for k=1)");
+  if (k > 18) return fail(ECH_ERR_OTHER, "k must be <= 18 (k! is exact in f64 only up to 18!; 19! exceeds 2^53)");
+  if (k > 12 && f32)
+    return fail(ECH_ERR_OTHER,
+                "k must be <= 12 for f32 (one order of margin: f32 k! exactness first degrades at 14!; use f64)");
+  if (k + 1 > 9) {
+    char buf[96];
+    snprintf(buf, sizeof buf, "unsupported Taylor order %u, must be 1..=9", k + 1);
+    return fail(ECH_ERR_OTHER, buf);
+  }
+  return ECH_OK;
+}
+
 // diagonal_kth_order_stochastic (src/stde/higher_order.rs:173-227): one jet of
 // order k+1 along e_j per sampled coordinate j, samples k! * c_k, Welford in
 // the sample type, then the n / |J| rescaling of the estimate, variance and SE.
@@ -1462,18 +1479,7 @@ static ech_status do_diag_kth(ech_ctx* ctx, const ech_tape* tc, const T* x, size
   ech_tape* t = const_cast<ech_tape*>(tc);
   CHECK(stde_checks(t, n, "diagonal_kth_order_stochastic", "diagonal"));
   if (n_idx == 0) return fail(ECH_ERR_OTHER, "sampled_indices must not be empty");
-  if (k < 2) return fail(ECH_ERR_OTHER, "k must be >= 2 (use gradient for k=1)");
-  // The reference's factorial-exactness limits (higher_order.rs:13-22), then
-  // the engine's own: jets are instantiated up to order 9, so k <= 8.
-  if (k > 18) return fail(ECH_ERR_OTHER, "k must be <= 18 (k! is exact in f64 only up to 18!; 19! exceeds 2^53)");
-  if (k > 12 && sizeof(T) == 4)
-    return fail(ECH_ERR_OTHER,
-                "k must be <= 12 for f32 (one order of margin: f32 k! exactness first degrades at 14!; use f64)");
-  if (k + 1 > 9) {
-    char buf[96];
-    snprintf(buf, sizeof buf, "unsupported Taylor order %u, must be 1..=9", k + 1);
-    return fail(ECH_ERR_OTHER, buf);
-  }
+  CHECK(kth_order_range(k, sizeof(T) == 4));
   if (!x || !idx || !out) return fail(ECH_ERR_INVALID_ARG, "null buffer");
   for (size_t s = 0; s < n_idx; ++s) {
     if (idx[s] >= n) {
@@ -1517,6 +1523,57 @@ ECH_API ech_status ech_diagonal_kth_order_stochastic_f64(ech_ctx* ctx, const ech
                                                          uint32_t k, const uint32_t* sampled_indices,
                                                          size_t n_indices, ech_estimator_result* out) {
   return do_diag_kth<double>(ctx, t, x, n, k, sampled_indices, n_indices, out);
+}
+
+// diagonal_kth_order (src/stde/higher_order.rs:40-95): diag[j] = k! * c_k of the
+// order-(k+1) jet along e_j, all n coordinates in one launch (basis directions
+// drawn in the kernel); value = c0.  A zero-input tape returns its recorded
+// output value and no diagonal, as the reference does.
+template <class T>
+static ech_status do_diag_kth_exact(ech_ctx* ctx, const ech_tape* tc, const T* x, size_t n, uint32_t k, T* value,
+                                    T* diag) {
+  CHECK(common_checks(ctx, tc, sizeof(T) == 8));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  if (t->host.outs.size() != 1) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "diagonal_kth_order requires a scalar-output tape; got %zu outputs", t->host.outs.size());
+    return fail(ECH_ERR_OTHER, buf);
+  }
+  CHECK(kth_order_range(k, sizeof(T) == 4));
+  if (!value) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  if (n != t->host.ni) return fail(ECH_ERR_INVALID_ARG, "x length must match the tape's num_inputs");
+  if (n == 0) {
+    *value = (T)t->host.vals[t->host.out_index];
+    return ECH_OK;
+  }
+  if (!x || !diag) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  T kfact = T(1);
+  for (uint32_t i = 2; i <= k; ++i) kfact = kfact * (T)i;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CU(cudaSetDevice(ctx->device));
+  CU(ctx->io_in.ensure(n * sizeof(T)));
+  CU(ctx->io_out.ensure(n * sizeof(T)));
+  CU(ctx->io_out2.ensure(n * sizeof(T)));
+  CU(cudaMemcpyAsync(ctx->io_in.p, x, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  CHECK(stde_run<T>(ctx, t, (const T*)ctx->io_in.p, true, 1, (uint32_t)n, nullptr, 3, 0, false, nullptr, 0.0, 0,
+                    nullptr, (T*)ctx->io_out.p, (T*)ctx->io_out2.p, (int)k + 1, (int)k));
+  std::vector<T> c0(n), ck(n);
+  CU(cudaMemcpyAsync(c0.data(), ctx->io_out.p, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaMemcpyAsync(ck.data(), ctx->io_out2.p, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  CHECK(check_err_word(ctx));
+  *value = c0[n - 1];
+  for (size_t j = 0; j < n; ++j) diag[j] = kfact * ck[j];
+  return ECH_OK;
+}
+
+ECH_API ech_status ech_diagonal_kth_order_f32(ech_ctx* ctx, const ech_tape* t, const float* x, size_t n, uint32_t k,
+                                              float* value, float* diag) {
+  return do_diag_kth_exact<float>(ctx, t, x, n, k, value, diag);
+}
+ECH_API ech_status ech_diagonal_kth_order_f64(ech_ctx* ctx, const ech_tape* t, const double* x, size_t n,
+                                              uint32_t k, double* value, double* diag) {
+  return do_diag_kth_exact<double>(ctx, t, x, n, k, value, diag);
 }
 
 // stde_sparse (src/stde/sparse.rs:37-78) over the sampling distribution of a

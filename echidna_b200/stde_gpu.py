@@ -101,6 +101,20 @@ def diagonal_kth_order_stochastic_gpu(backend: CudaContext, tape, x, k: int, sam
     return _result(r, float)
 
 
+def diagonal_kth_order_gpu(backend: CudaContext, tape, x, k: int):
+    """``stde::diagonal_kth_order`` (``src/stde/higher_order.rs:40-95``) on the GPU:
+    ``(f(x), [k! * c_k along e_j for every j])`` in one launch (k = 2..8)."""
+    lib = _lib.load()
+    f64 = bool(tape.f64)
+    dt = np.float64 if f64 else np.float32
+    xx = np.ascontiguousarray(x, dtype=dt).ravel()
+    value = np.zeros(1, dtype=dt)
+    diag = np.zeros(xx.size, dtype=dt)
+    fn = lib.ech_diagonal_kth_order_f64 if f64 else lib.ech_diagonal_kth_order_f32
+    _check(fn(backend._h, tape._h, _lib.ptr(xx), xx.size, int(k), _lib.ptr(value), _lib.ptr(diag)))
+    return float(value[0]), diag
+
+
 # ── operator estimators (src/stde/laplacian.rs:252-344, src/stde/pde.rs) ──
 
 def _fn(tape, name):

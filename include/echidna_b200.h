@@ -240,6 +240,16 @@ ECH_API ech_status ech_diagonal_kth_order_stochastic_f64(ech_ctx* ctx, const ech
                                                          size_t n, uint32_t k, const uint32_t* sampled_indices,
                                                          size_t n_indices, ech_estimator_result* out);
 
+/* stde::diagonal_kth_order (src/stde/higher_order.rs:40-95) on the GPU: diag[n]
+ * = [d^k f / dx_j^k] as k! * c_k of an order-(k+1) jet along every e_j (one
+ * launch), value = f(x).  k range and error texts as for the stochastic form;
+ * a zero-input tape returns its recorded output value and writes no diagonal;
+ * scalar-output tapes only. */
+ECH_API ech_status ech_diagonal_kth_order_f32(ech_ctx* ctx, const ech_tape* tape, const float* x, size_t n,
+                                              uint32_t k, float* value, float* diag);
+ECH_API ech_status ech_diagonal_kth_order_f64(ech_ctx* ctx, const ech_tape* tape, const double* x, size_t n,
+                                              uint32_t k, double* value, double* diag);
+
 /* stde::stde_sparse (src/stde/sparse.rs:37-78) over a SparseSamplingDistribution
  * (src/diffop.rs:896-1045), for `batch` points xs [batch][n] with their own
  * sampled entry indices sampled_indices [batch][n_samples]; batch = 1 is the

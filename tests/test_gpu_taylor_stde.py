@@ -225,3 +225,18 @@ def test_diagonal_kth_order_stochastic_errors(ctx):
         stde_gpu.diagonal_kth_order_stochastic_gpu(ctx, gt, x, 1, [0])
     with pytest.raises(GpuError, match="out of bounds"):
         stde_gpu.diagonal_kth_order_stochastic_gpu(ctx, gt, x, 2, [4])
+
+
+@pytest.mark.parametrize("k", [2, 3, 5, 8])
+def test_diagonal_kth_order_vector_matches_oracle(ctx, k):
+    # stde/higher_order.rs:40-95 on the GPU (one launch over the n basis jets) vs
+    # the oracle's single-index estimates n * k! * c_k
+    tape = configs.random_dag(8, 400, seed=40 + k)
+    x = np.random.default_rng(k).uniform(-0.8, 0.8, size=8)
+    value, diag = stde_gpu.diagonal_kth_order_gpu(ctx, ctx.upload_tape_f64(tape), x, k)
+    o = OracleTape(tape)
+    for j in range(8):
+        r = o.diagonal_kth_order_stochastic(x, k, [j])
+        want = float(r[1]) / 8
+        assert abs(diag[j] - want) <= 1e-10 * max(1.0, abs(want)), (j, diag[j], want)
+        assert abs(value - float(r[0])) <= 1e-12 * max(1.0, abs(float(r[0])))

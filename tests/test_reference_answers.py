@@ -835,3 +835,53 @@ def test_gpu_f32_zero_multiplier_absorbs_inf_adjoint(ctx):
     assert abs(float(g[0]) - _ZM_X) < 1e-5
     hg, hv = ctx.hvp_batch(gt, np.asarray([0.0, 0.0], np.float32), np.asarray([1.0, 0.0], np.float32), 1)
     assert list(np.asarray(hg, np.float64)) == [0.0, 0.0] and list(np.asarray(hv, np.float64)) == [0.0, 0.0]
+
+
+# stde_higher_order.rs:39-81 and :185-263 on the exact vector form
+# (diagonal_kth_order and its const-order twin): (value, [d^k f / dx_j^k]).
+KTH_DIAG = {
+    **{f"exp_k{k}": (_exp_1d, [1.0], k, E, [E], 10.0 ** -(12 - k)) for k in (2, 3, 4, 5)},
+    "quartic_k4": (_quartic, [2.0, 3.0], 4, 97.0, [24.0, 24.0], 1e-6),
+    "quartic_k5": (_quartic, [2.0, 3.0], 5, 97.0, [0.0, 0.0], 1e-4),
+    "cubic_mix_k2": (_cubic_mix, [1.0, 2.0, 3.0], 2, 10.0, [4.0, 12.0, 0.0], 1e-10),
+}
+
+
+@pytest.mark.parametrize("name", sorted(KTH_DIAG))
+def test_oracle_diagonal_kth_order_vector(name):
+    # the oracle's single-index estimate is n * d^k f / dx_j^k
+    mk, x, k, _, want, tol = KTH_DIAG[name]
+    o = OracleTape(mk())
+    got = [float(o.diagonal_kth_order_stochastic(np.asarray(x), k, [j])[1]) / len(x) for j in range(len(x))]
+    assert all(abs(g - w) <= tol * max(1.0, abs(w)) for g, w in zip(got, want)), (name, got, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(KTH_DIAG))
+def test_gpu_diagonal_kth_order_vector(ctx, name):
+    from echidna_b200.stde_gpu import diagonal_kth_order_gpu
+    mk, x, k, value, want, tol = KTH_DIAG[name]
+    v, d = diagonal_kth_order_gpu(ctx, ctx.upload_tape_f64(mk()), x, k)
+    assert abs(v - value) <= 1e-10 * max(1.0, abs(value))
+    assert all(abs(g - w) <= tol * max(1.0, abs(w)) for g, w in zip(d, want)), (name, list(d), want)
+
+
+@pytest.mark.gpu
+def test_gpu_diagonal_kth_order_vector_edges(ctx):
+    from echidna_b200.gpu import GpuError
+    from echidna_b200.stde_gpu import diagonal_kth_order_gpu
+    # higher_order.rs:59-62: a zero-input tape returns its primal and no diagonal
+    gt = ctx.upload_tape_f64(record(lambda v: constant(3.0) * constant(2.0), [])[0])
+    v, d = diagonal_kth_order_gpu(ctx, gt, [], 3)
+    assert v == 6.0 and d.size == 0
+    # the highest order the engine runs, and f32
+    v, d = diagonal_kth_order_gpu(ctx, ctx.upload_tape_f64(_exp_1d()), [1.0], 8)
+    assert abs(d[0] - E) <= 1e-3
+    v, d = diagonal_kth_order_gpu(ctx, ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(_exp_1d())), [1.0], 2)
+    assert abs(d[0] - E) <= 1e-5 * E
+    with pytest.raises(GpuError, match="k must be >= 2"):
+        diagonal_kth_order_gpu(ctx, ctx.upload_tape_f64(_exp_1d()), [1.0], 1)
+    from echidna_b200 import record_multi
+    two = record_multi(lambda v: [v[0] * v[1], v[0] + v[1]], [1.0, 2.0])[0]
+    with pytest.raises(GpuError, match="scalar-output"):
+        diagonal_kth_order_gpu(ctx, ctx.upload_tape_f64(two), [1.0, 2.0], 2)
