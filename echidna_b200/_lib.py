@@ -111,6 +111,8 @@ _SIGS = {
     "ech_diagonal_kth_order_stochastic_f64": ([_P, _P, _P, _SZ, _U32, _P, _SZ, _P], _I),
     "ech_diagonal_kth_order_f32": ([_P, _P, _P, _SZ, _U32, _P, _P], _I),
     "ech_diagonal_kth_order_f64": ([_P, _P, _P, _SZ, _U32, _P, _P], _I),
+    "ech_estimate_f32": ([_P, _P, _P, _SZ, _I, _P, _U32, _P, _P], _I),
+    "ech_estimate_f64": ([_P, _P, _P, _SZ, _I, _P, _U32, _P, _P], _I),
     "ech_stde_sparse_batch_f32": ([_P, _P, _P, _SZ, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, ctypes.c_float, _P, _U32,
                                    _P], _I),
     "ech_stde_sparse_batch_f64": ([_P, _P, _P, _SZ, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, ctypes.c_double, _P, _U32,

@@ -1722,7 +1722,7 @@ struct HostWelford {
 // [S][n] at one point x.
 template <class T>
 static ech_status jets_along(ech_ctx* ctx, ech_tape* t, const T* x, size_t n, const T* dirs, uint32_t S,
-                             std::vector<T>& c0, std::vector<T>& c2) {
+                             std::vector<T>& c0, std::vector<T>& c2, int kk = 2) {
   c0.assign(S, T(0));
   c2.assign(S, T(0));
   if (S == 0) return ECH_OK;
@@ -1735,7 +1735,7 @@ static ech_status jets_along(ech_ctx* ctx, ech_tape* t, const T* x, size_t n, co
   CU(cudaMemcpyAsync(ctx->io_in.p, x, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
   CU(cudaMemcpyAsync(ctx->io_in2.p, dirs, (size_t)S * n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
   CHECK(stde_run<T>(ctx, t, (const T*)ctx->io_in.p, true, 1, S, (const T*)ctx->io_in2.p, 1, 0, false, nullptr, 0.0,
-                    0, nullptr, (T*)ctx->io_out.p, (T*)ctx->io_out2.p));
+                    0, nullptr, (T*)ctx->io_out.p, (T*)ctx->io_out2.p, 3, kk));
   CU(cudaMemcpyAsync(c0.data(), ctx->io_out.p, (size_t)S * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
   CU(cudaMemcpyAsync(c2.data(), ctx->io_out2.p, (size_t)S * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
   CU(cudaStreamSynchronize(ctx->stream));
@@ -1879,6 +1879,79 @@ static ech_status do_parabolic_stoch(ech_ctx* ctx, const ech_tape* tc, const T* 
   put_result(out, (double)value, (double)(mean * scale), (double)(var * scale * scale), (double)(se * scale),
              acc.count);
   return ECH_OK;
+}
+
+// stde::estimate / estimate_weighted (src/stde/pipeline.rs:20-142) with the
+// reference's two estimators (src/stde/estimator.rs): Laplacian samples 2 c2,
+// GradientSquaredNorm c1^2.  The order-3 jets along the S host directions run on
+// the GPU; the statistics follow the reference's host loop in the sample type:
+// Welford without weights, West's weighted update with them (zero weights are
+// skipped but counted, non-finite samples skipped and not counted, standard error
+// over the effective n = (sum w)^2 / sum w^2).
+template <class T>
+static ech_status do_estimate(ech_ctx* ctx, const ech_tape* tc, const T* x, size_t n, int estimator, const T* dirs,
+                              uint32_t S, const T* weights, ech_estimator_result* out) {
+  CHECK(common_checks(ctx, tc, sizeof(T) == 8));
+  ech_tape* t = const_cast<ech_tape*>(tc);
+  CHECK(stde_checks(t, n, "estimate", "estimator"));
+  if (estimator != 0 && estimator != 1) return fail(ECH_ERR_INVALID_ARG, "estimator must be 0 (Laplacian) or 1 (GradientSquaredNorm)");
+  if (S == 0) return fail(ECH_ERR_OTHER, "directions must not be empty");
+  if (!x || !dirs || !out) return fail(ECH_ERR_INVALID_ARG, "null buffer");
+  if (weights)
+    for (uint32_t s = 0; s < S; ++s)
+      if (!(weights[s] >= T(0))) return fail(ECH_ERR_OTHER, "estimate_weighted: weights must be non-negative and non-NaN");
+  std::vector<T> c0, ck;
+  CHECK(jets_along<T>(ctx, t, x, n, dirs, S, c0, ck, estimator == 0 ? 2 : 1));
+  auto sample = [&](uint32_t s) { return estimator == 0 ? T(2) * ck[s] : ck[s] * ck[s]; };
+  T value = T(0);
+  if (!weights) {
+    HostWelford<T> acc;
+    for (uint32_t s = 0; s < S; ++s) {
+      value = c0[s];
+      acc.update(sample(s));
+    }
+    T mean, var, se;
+    acc.finalize(&mean, &var, &se);
+    put_result(out, (double)value, (double)mean, (double)var, (double)se, acc.count);
+    return ECH_OK;
+  }
+  T w_sum = T(0), w_sum2 = T(0), mean = T(0), m2 = T(0);
+  uint64_t skips = 0;
+  for (uint32_t s = 0; s < S; ++s) {
+    value = c0[s];
+    const T w = weights[s];
+    if (w == T(0)) continue;
+    const T v = sample(s);
+    if (!std::isfinite(v)) {
+      ++skips;
+      continue;
+    }
+    w_sum = w_sum + w;
+    w_sum2 = w_sum2 + w * w;
+    const T d = v - mean;
+    mean = mean + (w / w_sum) * d;
+    const T d2 = v - mean;
+    m2 = m2 + w * d * d2;
+  }
+  const T denom = w_sum > T(0) ? w_sum - w_sum2 / w_sum : T(0);
+  T var = T(0), se = T(0);
+  if (S > 1 && denom > T(0)) {
+    var = std::max(m2 / denom, T(0));
+    const T n_eff = w_sum * w_sum / w_sum2;
+    se = std::sqrt(var / n_eff);
+  }
+  const T est = (w_sum > T(0) || skips == 0) ? mean : std::numeric_limits<T>::quiet_NaN();
+  put_result(out, (double)value, (double)est, (double)var, (double)se, (uint64_t)S - skips);
+  return ECH_OK;
+}
+
+ECH_API ech_status ech_estimate_f32(ech_ctx* ctx, const ech_tape* t, const float* x, size_t n, int estimator,
+                                    const float* dirs, uint32_t S, const float* weights, ech_estimator_result* out) {
+  return do_estimate<float>(ctx, t, x, n, estimator, dirs, S, weights, out);
+}
+ECH_API ech_status ech_estimate_f64(ech_ctx* ctx, const ech_tape* t, const double* x, size_t n, int estimator,
+                                    const double* dirs, uint32_t S, const double* weights, ech_estimator_result* out) {
+  return do_estimate<double>(ctx, t, x, n, estimator, dirs, S, weights, out);
 }
 
 // dense_stde_2nd (src/stde/pde.rs:242-296): samples 2 c2 along v = L z, L lower

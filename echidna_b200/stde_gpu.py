@@ -155,6 +155,26 @@ def parabolic_diffusion_stochastic_gpu(backend: CudaContext, tape, x, sigma_colu
     return _result(r)
 
 
+LAPLACIAN, GRADIENT_SQUARED_NORM = 0, 1
+
+
+def estimate_gpu(backend: CudaContext, tape, x, directions, estimator: int = LAPLACIAN,
+                 weights=None) -> EstimatorResult:
+    """``stde::estimate`` / ``stde::estimate_weighted`` (``src/stde/pipeline.rs:20-142``) with the
+    ``Laplacian`` (2 c2) or ``GradientSquaredNorm`` (c1^2) estimator: jets on the GPU, the
+    reference's Welford or West's weighted statistics on the host."""
+    fn, dt = _fn(tape, "estimate")
+    xx = np.ascontiguousarray(x, dtype=dt).ravel()
+    V = np.ascontiguousarray(directions, dtype=dt).reshape(-1, xx.size)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=dt).ravel()
+    if w is not None and w.size != V.shape[0]:
+        raise ValueError("weights.len() must match directions.len()")
+    r = _lib.EstimatorResultC()
+    _check(fn(backend._h, tape._h, _lib.ptr(xx), xx.size, int(estimator), _lib.ptr(V), V.shape[0], _lib.ptr(w),
+              ctypes.byref(r)))
+    return _result(r)
+
+
 def dense_stde_2nd_gpu(backend: CudaContext, tape, x, cholesky, z_vectors) -> EstimatorResult:
     """``stde::dense_stde_2nd``: samples (L z)^T H (L z), L lower triangular [n, n]."""
     fn, dt = _fn(tape, "dense_stde_2nd")

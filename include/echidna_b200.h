@@ -347,6 +347,16 @@ ECH_API ech_status ech_parabolic_diffusion_stochastic_f64(ech_ctx* ctx, const ec
                                                           size_t n, const double* sigma_columns, uint32_t d,
                                                           const uint32_t* sampled_indices, uint32_t m,
                                                           ech_estimator_result* out);
+/* stde::estimate and stde::estimate_weighted (src/stde/pipeline.rs:20-142) with
+ * estimator 0 = Laplacian (samples 2 c2) or 1 = GradientSquaredNorm (c1^2),
+ * src/stde/estimator.rs: order-3 jets along dirs [S][n] at x on the GPU, then
+ * Welford (weights NULL) or West's weighted statistics (weights [S], >= 0) in
+ * the sample type.  Errors: "directions must not be empty", "estimate_weighted:
+ * weights must be non-negative and non-NaN"; scalar-output tapes only. */
+ECH_API ech_status ech_estimate_f32(ech_ctx* ctx, const ech_tape* tape, const float* x, size_t n, int estimator,
+                                    const float* dirs, uint32_t S, const float* weights, ech_estimator_result* out);
+ECH_API ech_status ech_estimate_f64(ech_ctx* ctx, const ech_tape* tape, const double* x, size_t n, int estimator,
+                                    const double* dirs, uint32_t S, const double* weights, ech_estimator_result* out);
 /* dense_stde_2nd (src/stde/pde.rs:242-296): samples 2 c2 along L z (L row-major n x n,
  * lower triangle used), z_vectors [m][n]. */
 ECH_API ech_status ech_dense_stde_2nd_f32(ech_ctx* ctx, const ech_tape* tape, const float* x, size_t n,

@@ -885,3 +885,73 @@ def test_gpu_diagonal_kth_order_vector_edges(ctx):
     two = record_multi(lambda v: [v[0] * v[1], v[0] + v[1]], [1.0, 2.0])[0]
     with pytest.raises(GpuError, match="scalar-output"):
         diagonal_kth_order_gpu(ctx, ctx.upload_tape_f64(two), [1.0, 2.0], 2)
+
+
+# stde_pipeline.rs:37-172: estimate / estimate_weighted with both estimators.
+_RADEMACHER4 = [[1.0, 1.0], [1.0, -1.0], [-1.0, 1.0], [-1.0, -1.0]]
+
+
+def _sum_sq(x0):
+    return record(lambda v: v[0] * v[0] + v[1] * v[1], x0)[0]
+
+
+@pytest.mark.gpu
+def test_gpu_estimate_pipeline(ctx):
+    from echidna_b200.stde_gpu import GRADIENT_SQUARED_NORM, LAPLACIAN, estimate_gpu, laplacian_gpu
+    # :37-54: the Laplacian estimator equals laplacian() (value 5, estimate 4, 4 samples)
+    gt = ctx.upload_tape_f64(_sum_sq([1.0, 2.0]))
+    r = estimate_gpu(ctx, gt, [1.0, 2.0], _RADEMACHER4, LAPLACIAN)
+    assert abs(r.value - 5.0) <= 1e-10 and abs(r.estimate - 4.0) <= 1e-10 and r.num_samples == 4
+    f32 = ctx.upload_tape(GpuTapeData.from_tape_f64_lossy(_sum_sq([1.0, 2.0])))
+    lap = laplacian_gpu(ctx, f32, [1.0, 2.0], _RADEMACHER4)
+    r32 = estimate_gpu(ctx, f32, [1.0, 2.0], _RADEMACHER4, LAPLACIAN)
+    assert r32.estimate == lap.estimate and r32.value == lap.value
+    # :56-76: GradientSquaredNorm at (3, 4): value 25, E[(g.v)^2] = |g|^2 = 100
+    gt = ctx.upload_tape_f64(_sum_sq([3.0, 4.0]))
+    r = estimate_gpu(ctx, gt, [3.0, 4.0], _RADEMACHER4, GRADIENT_SQUARED_NORM)
+    assert abs(r.value - 25.0) <= 1e-10 and abs(r.estimate - 100.0) <= 1e-10
+    # :78-101: unit weights reproduce the unweighted estimate
+    cm = ctx.upload_tape_f64(_cubic_mix())
+    dirs = [[1.0, 1.0, 1.0], [1.0, -1.0, 1.0], [-1.0, 1.0, -1.0], [1.0, 1.0, -1.0]]
+    a = estimate_gpu(ctx, cm, [1.0, 2.0, 3.0], dirs)
+    b = estimate_gpu(ctx, cm, [1.0, 2.0, 3.0], dirs, weights=[1.0] * 4)
+    assert abs(a.estimate - b.estimate) <= 1e-10 and a.num_samples == b.num_samples
+    # :103-124: weights (3, 1) on x^2 + y^2: both samples 4, so 4
+    gt = ctx.upload_tape_f64(_sum_sq([1.0, 2.0]))
+    r = estimate_gpu(ctx, gt, [1.0, 2.0], _RADEMACHER4[:2], weights=[3.0, 1.0])
+    assert abs(r.estimate - 4.0) <= 1e-10 and r.num_samples == 2
+    # :130-168: x^2 + 3 y^2, samples 2 and 6 with weights (3, 1): mean 3, SE over n_eff = 1.6
+    t = record(lambda v: v[0] * v[0] + (v[1] * v[1]) * constant(3.0), [1.0, 2.0])[0]
+    r = estimate_gpu(ctx, ctx.upload_tape_f64(t), [1.0, 2.0], [[1.0, 0.0], [0.0, 1.0]], weights=[3.0, 1.0])
+    assert abs(r.estimate - 3.0) <= 1e-10
+    assert abs(r.standard_error - math.sqrt(r.sample_variance / 1.6)) <= 1e-10
+    assert abs(r.standard_error - math.sqrt(r.sample_variance / 2.0)) > 1e-6
+
+
+@pytest.mark.gpu
+def test_gpu_estimate_weighted_matches_oracle_and_nonfinite(ctx):
+    from echidna_b200.gpu import GpuError
+    from echidna_b200.stde_gpu import estimate_gpu
+    from echidna_b200 import configs
+    # a random tape, random directions and weights with zeros: the oracle's West update
+    tape = configs.random_dag(6, 300, seed=77)
+    rng = np.random.default_rng(77)
+    x = rng.uniform(-0.7, 0.7, size=6)
+    dirs = rng.choice([-1.0, 1.0], size=(40, 6))
+    w = rng.uniform(0.0, 2.0, size=40)
+    w[::7] = 0.0
+    r = estimate_gpu(ctx, ctx.upload_tape_f64(tape), x, dirs, weights=w)
+    o = OracleTape(tape).estimate_weighted(x, dirs, w)
+    for got, want in zip((r.value, r.estimate, r.sample_variance, r.standard_error), o[:4]):
+        assert abs(got - float(want)) <= 1e-10 * max(1.0, abs(float(want)))
+    assert r.num_samples == int(o[4])
+    # stde_nonfinite_samples.rs:58-111 through the GPU jets
+    gt = ctx.upload_tape_f64(_exp_prod_tape())
+    r = estimate_gpu(ctx, gt, [1.0, 700.0], [LIVE, DEAD], weights=[1.0, 1.0])
+    assert r.num_samples == 1 and r.estimate == 0.0
+    r = estimate_gpu(ctx, gt, [1.0, 700.0], [LIVE], weights=[1.0])
+    assert r.num_samples == 0 and math.isnan(r.estimate)
+    with pytest.raises(GpuError, match="weights must be non-negative"):
+        estimate_gpu(ctx, gt, [1.0, 700.0], [LIVE], weights=[-1.0])
+    with pytest.raises(GpuError, match="directions must not be empty"):
+        estimate_gpu(ctx, gt, [1.0, 700.0], np.zeros((0, 2)))
