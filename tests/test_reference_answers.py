@@ -14,7 +14,13 @@ conventions on the bytecode tape in f64:
 * ``tests/hypot_leading_zero_parity.rs`` (jets built from polynomials);
 * ``tests/opcode_edge_cases.rs`` as forward values and gradients of one-op tapes;
 * ``tests/stde_nonfinite_samples.rs`` (the Welford accumulator);
-* the tape cases of ``tests/regressions.rs``.
+* the tape cases of ``tests/regressions.rs``;
+* ``tests/stde_higher_order.rs`` (k-th order diagonals, parabolic diffusion),
+  ``tests/stde_pipeline.rs`` (``estimate`` / ``estimate_weighted``),
+  ``tests/stde_core.rs`` and ``tests/stde_stats.rs`` (known Hessians, Welford
+  statistics, control variate);
+* the f32 jet tests of ``tests/gpu_stde.rs`` that the reference runs on its
+  CUDA backend.
 
 Dual-number cases become JVPs of the one-op tape (a ``Dual::new(x, 1)`` operand
 is a seeded input, a ``Dual::constant`` operand a tape constant).  The oracle
@@ -955,3 +961,86 @@ def test_gpu_estimate_weighted_matches_oracle_and_nonfinite(ctx):
         estimate_gpu(ctx, gt, [1.0, 700.0], [LIVE], weights=[-1.0])
     with pytest.raises(GpuError, match="directions must not be empty"):
         estimate_gpu(ctx, gt, [1.0, 700.0], np.zeros((0, 2)))
+
+
+# stde_core.rs:61-297 on the oracle (the GPU forms are checked against it in
+# test_gpu_taylor_stde.py and above): laplacian, hessian_diagonal and the
+# directional derivatives of the stde module's known Hessians.
+_R3 = [[a, b, c] for a in (1.0, -1.0) for b in (1.0, -1.0) for c in (1.0, -1.0)]
+STDE_CORE = {
+    # name: (tape maker, x, Rademacher dirs or None, value, laplacian or None, diagonal or None)
+    "sum_of_squares": (lambda: _sum_sq([1.0, 2.0]), [1.0, 2.0], _RADEMACHER4[:2], 5.0, 4.0, [2.0, 2.0]),
+    "product": (lambda: record(lambda v: v[0] * v[1], [3.0, 4.0])[0], [3.0, 4.0], _RADEMACHER4[:2], 12.0, 0.0,
+                [0.0, 0.0]),
+    "cubic_mix": (_cubic_mix, [1.0, 2.0, 3.0], _R3, 10.0, 16.0, [4.0, 12.0, 0.0]),
+    "cube_1d": (lambda: record(lambda v: v[0] * v[0] * v[0], [2.0])[0], [2.0], None, 8.0, None, [12.0]),
+    "linear": (lambda: record(lambda v: v[0] + v[1], [1.0, 2.0])[0], [1.0, 2.0], _RADEMACHER4[:2], 3.0, 0.0,
+               [0.0, 0.0]),
+}
+
+
+@pytest.mark.parametrize("name", sorted(STDE_CORE))
+def test_oracle_stde_core_known_hessians(name):
+    mk, x, dirs, value, lap, diag = STDE_CORE[name]
+    o = OracleTape(mk())
+    if dirs is not None:
+        v, got = o.laplacian(np.asarray(x), np.asarray(dirs))
+        assert abs(v - value) <= 1e-10 and abs(got - lap) <= 1e-10, (name, v, got)
+    v, d = o.hessian_diagonal(np.asarray(x))
+    assert abs(v - value) <= 1e-10 and np.allclose(d, diag, rtol=0, atol=1e-10), (name, v, d)
+    # :159-214: the diagonal and the trace agree with the full Hessian
+    _, _, H = o.hessian(np.asarray(x))
+    assert np.allclose(np.diag(H), d, rtol=0, atol=1e-10)
+
+
+def test_oracle_stde_core_directional_derivatives():
+    # :285-298: along e0 on x^2 + y^2 at (1, 2), c1 = 2 and c2 = e0^T H e0 / 2 = 1;
+    # :221-237: along each e_j, c1 is the gradient entry
+    o = OracleTape(_sum_sq([1.0, 2.0]))
+    c = o.taylor(np.asarray([[1.0, 2.0]]), np.asarray([[1.0, 0.0]]), 3)
+    assert abs(c[1][0] - 2.0) <= 1e-10 and abs(c[2][0] - 1.0) <= 1e-10
+    q = OracleTape(_cubic_mix())
+    _, g = q.gradient(np.asarray([[1.0, 2.0, 3.0]]))
+    for j in range(3):
+        e = np.zeros((1, 3))
+        e[0, j] = 1.0
+        cj = q.taylor(np.asarray([[1.0, 2.0, 3.0]]), e, 2)
+        assert abs(cj[1][0] - g[0][j]) <= 1e-10
+    assert np.allclose(g[0], [4.0, 13.0, 0.0], rtol=0, atol=1e-10)
+
+
+# stde_stats.rs:95-343 on the oracle: the Hessian diagonal of exp(x) + sin(y), the
+# Welford statistics of laplacian_with_stats and the control-variate estimate.
+_CM_DIRS = [[1.0, 1.0, 1.0], [1.0, -1.0, 1.0], [-1.0, 1.0, -1.0], [1.0, 1.0, -1.0]]
+
+
+def test_oracle_stde_stats_known_answers():
+    # :95-103
+    t = record(lambda v: v[0].exp() + v[1].sin(), [1.0, 2.0])[0]
+    _, d = OracleTape(t).hessian_diagonal(np.asarray([1.0, 2.0]))
+    assert abs(d[0] - math.exp(1.0)) <= 1e-10 and abs(d[1] + math.sin(2.0)) <= 1e-10
+    cm = OracleTape(_cubic_mix())
+    x3 = np.asarray([[1.0, 2.0, 3.0]])
+    # :146-163: off-diagonal Hessian entries give a positive variance
+    r = cm.laplacian_stats_batch(x3, np.asarray(_CM_DIRS))[0]
+    assert r[2] > 0.0 and r[3] > 0.0
+    # :178-189: SE = sqrt(var / n)
+    r = cm.laplacian_stats_batch(x3, np.asarray(_CM_DIRS[:3]))[0]
+    assert abs(r[3] - math.sqrt(r[2] / r[4])) <= 1e-14
+    ss = OracleTape(_sum_sq([1.0, 2.0]))
+    x2 = np.asarray([[1.0, 2.0]])
+    # :166-176: one sample has zero variance and SE
+    r = ss.laplacian_stats_batch(x2, np.asarray([[1.0, 1.0]]))[0]
+    assert int(r[4]) == 1 and r[2] == 0.0 and r[3] == 0.0
+    # :192-205: a diagonal Hessian gives 4 with zero variance; :128-143 it equals laplacian()
+    r = ss.laplacian_stats_batch(x2, np.asarray(_RADEMACHER4))[0]
+    v, lap = ss.laplacian(np.asarray([1.0, 2.0]), np.asarray(_RADEMACHER4))
+    assert abs(r[1] - 4.0) <= 1e-10 and abs(r[2]) <= 1e-10 and r[1] == lap and r[0] == v and int(r[4]) == 4
+    # :212-231: the control variate keeps the exact 16 over all 8 Rademacher vectors
+    _, diag = cm.hessian_diagonal(np.asarray([1.0, 2.0, 3.0]))
+    r = cm.laplacian_with_control(np.asarray([1.0, 2.0, 3.0]), np.asarray(_R3), diag)
+    assert abs(r[1] - 16.0) <= 1e-10
+    # :333-344: a linear function: value 3, estimate 0, variance 0
+    lin = OracleTape(record(lambda v: v[0] + v[1], [1.0, 2.0])[0])
+    r = lin.laplacian_stats_batch(x2, np.asarray(_RADEMACHER4))[0]
+    assert abs(r[0] - 3.0) <= 1e-10 and abs(r[1]) <= 1e-10 and abs(r[2]) <= 1e-10
