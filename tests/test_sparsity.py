@@ -55,6 +55,26 @@ def test_detected_jacobian_sparsity_coloring(engine_lib):
     assert rn == 1 and rc[0] == rc[1]
 
 
+# ── tests/sparse_jacobian.rs ──
+
+def test_jacobian_patterns_known_answers(engine_lib):
+    want = {
+        # :18-33: [2 x0 + x1, x1 + 3 x2]
+        "linear": (lambda v: [v[0] * 2.0 + v[1], v[1] + v[2] * 3.0], {(0, 0), (0, 1), (1, 1), (1, 2)}),
+        # :35-55: [x0 x1, x1 x2, x0^2]
+        "nonlinear": (lambda v: [v[0] * v[1], v[1] * v[2], v[0] * v[0]], {(0, 0), (0, 1), (1, 1), (1, 2), (2, 0)}),
+    }
+    for name, (fn, entries) in want.items():
+        tape, _ = record_multi(fn, [1.0, 2.0, 3.0])
+        p = detect_jacobian_sparsity(tape)
+        for i in range(tape.num_outputs()):
+            for j in range(3):
+                assert p.contains(i, j) == ((i, j) in entries), (name, i, j)
+    # :57-66: an identity map needs one column color
+    tape, _ = record_multi(lambda v: [v[0], v[1], v[2]], [1.0, 2.0, 3.0])
+    assert column_coloring(detect_jacobian_sparsity(tape))[1] == 1
+
+
 # ── tests/sparse_hessian.rs ──
 
 def test_hessian_patterns_known_answers(engine_lib):
