@@ -18,7 +18,8 @@ conventions on the bytecode tape in f64:
 * ``tests/stde_higher_order.rs`` (k-th order diagonals, parabolic diffusion),
   ``tests/stde_pipeline.rs`` (``estimate`` / ``estimate_weighted``),
   ``tests/stde_core.rs`` and ``tests/stde_stats.rs`` (known Hessians, Welford
-  statistics, control variate);
+  statistics, control variate) and ``tests/bytecode_tape.rs`` (gradients
+  through shared subexpressions);
 * the f32 jet tests of ``tests/gpu_stde.rs`` that the reference runs on its
   CUDA backend.
 
@@ -1044,3 +1045,26 @@ def test_oracle_stde_stats_known_answers():
     lin = OracleTape(record(lambda v: v[0] + v[1], [1.0, 2.0])[0])
     r = lin.laplacian_stats_batch(x2, np.asarray(_RADEMACHER4))[0]
     assert abs(r[0] - 3.0) <= 1e-10 and abs(r[1]) <= 1e-10 and abs(r[2]) <= 1e-10
+
+
+# bytecode_tape.rs:34-72 on the oracle: gradients through shared subexpressions.
+def _chain8(x):
+    a = x * x
+    b = a * a
+    return b * b
+
+
+BYTECODE_GRADS = {
+    "x_squared": (lambda v: v[0] * v[0], [3.0], [6.0]),
+    "x_times_y": (lambda v: v[0] * v[1], [3.0, 4.0], [4.0, 3.0]),
+    "diamond": (lambda v: v[0] * v[0] + v[0] * v[0] * v[0], [2.0], [16.0]),
+    "fan_out": (lambda v: v[0] + v[0] + v[0], [5.0], [3.0]),
+    "chain_depth": (lambda v: _chain8(v[0]), [2.0], [8.0 * 2.0 ** 7]),
+}
+
+
+@pytest.mark.parametrize("name", sorted(BYTECODE_GRADS))
+def test_oracle_bytecode_tape_gradients(name):
+    fn, x, want = BYTECODE_GRADS[name]
+    _, g = OracleTape(record(fn, x)[0]).gradient(np.asarray([x]))
+    assert all(abs(a - b) <= 1e-12 * abs(b) for a, b in zip(g[0], want)), (name, g[0], want)
